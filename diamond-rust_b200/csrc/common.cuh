@@ -1,0 +1,118 @@
+// Shared definitions of the drgpu CUDA library (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "drgpu.h"
+
+namespace drg {
+
+// An error carrying a DRG_ERR_* code; the C ABI turns it into a status.
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define DRG_CUDA(call)                                                                              \
+  do {                                                                                              \
+    cudaError_t e__ = (call);                                                                       \
+    if (e__ != cudaSuccess)                                                                         \
+      throw ::drg::Error(e__ == cudaErrorMemoryAllocation ? DRG_ERR_OOM : DRG_ERR_CUDA,             \
+                         std::string(#call) + ": " + cudaGetErrorString(e__));                      \
+  } while (0)
+
+// Residue codes (alphabet.rs:1-20): 0..19 canonical, 20..22 B/J/Z, 23 X, 24 '*'.
+constexpr int kAlpha = 25;
+// Code the kernels use for positions outside a sequence; it scores kSentinelScore
+// against everything so that cells there can never raise a score.
+constexpr int kSentinel = 25;
+constexpr int kSentinelScore = -64;
+
+// Grow-only device allocation owned by a context; contents are not preserved
+// on growth.
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+  void* ensure(size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (bytes > cap) {
+      release();
+      size_t want = bytes + bytes / 8;
+      DRG_CUDA(cudaMalloc(&p, want));
+      cap = want;
+    }
+    return p;
+  }
+  template <typename T>
+  T* as(size_t n) {
+    return static_cast<T*>(ensure(n * sizeof(T)));
+  }
+};
+
+// Pinned host staging buffer, grow-only.
+struct HostBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  ~HostBuf() {
+    if (p) cudaFreeHost(p);
+  }
+  void* ensure(size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (bytes > cap) {
+      if (p) cudaFreeHost(p);
+      p = nullptr;
+      size_t want = bytes + bytes / 8;
+      DRG_CUDA(cudaMallocHost(&p, want));
+      cap = want;
+    }
+    return p;
+  }
+  template <typename T>
+  T* as(size_t n) {
+    return static_cast<T*>(ensure(n * sizeof(T)));
+  }
+};
+
+// Number of kernels this library has launched in this process (all contexts).
+uint64_t kernel_launch_count();
+void count_launch();
+
+inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+inline int bits_for(uint64_t v) {  // bits needed to store values 0..v
+  int b = 0;
+  while (b < 64 && (v >> b) != 0) ++b;
+  return b;
+}
+
+// Seed shapes as the kernels see them (shape.rs:11-20).
+constexpr int kMaxShapes = 64;
+constexpr int kMaxWeight = 16;
+struct ShapeTable {
+  int n;
+  uint8_t weight[kMaxShapes];
+  uint8_t span[kMaxShapes];
+  uint8_t pos[kMaxShapes][kMaxWeight];
+};
+
+// Parameters of the seed stage for one search.
+struct SeedParams {
+  uint8_t bucket[32];      // residue -> reduced bucket, 255 = not seedable
+  uint64_t size;           // reduction size
+  double cut;              // complexity cut (natural log units)
+  double lnfact[33];       // ln n!, summed in the reference's order
+};
+
+}  // namespace drg

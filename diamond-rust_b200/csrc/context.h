@@ -1,0 +1,73 @@
+// Library objects behind the opaque C handles.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "drgpu.h"
+#include "host/presets.h"
+#include "host/scoring.h"
+
+struct drg_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  // seed stage
+  drg::DevBuf q_keys, q_vals, q_keys_s, q_vals_s, r_keys, r_vals, r_keys_s, r_vals_s, cub_tmp;
+  drg::DevBuf run_keys, run_counts, run_qstart, run_rlo, run_rcount, run_hits, run_hit_off, counters;
+  drg::DevBuf q_owner, r_owner;
+  // hits and ungapped stage
+  drg::DevBuf hits, hits_s, hits_u, flags, idx, segs, seg_keys, segs_c, keep;
+  // bands and DP
+  drg::DevBuf bands, bands_c, band_valid, pair_first, sw_keys, sw_keys_s, sw_order, sw_order_s, sw_tasks, scores,
+      state, sel_idx, sel_bands, exact_jobs, exact_out, exact_scratch, exact_ops;
+  drg::HostBuf h_stage;
+  cudaEvent_t ev[16] = {};
+  drg_run_stats last{};
+};
+
+struct drg_db {
+  drg_ctx* ctx = nullptr;
+  uint8_t* letters = nullptr;   // device, 16 bytes of slack after the end
+  uint64_t* offsets = nullptr;  // device, n + 1
+  uint32_t* owner = nullptr;    // device: letter -> sequence
+  std::vector<uint64_t> h_offsets;
+  uint64_t n = 0, total = 0;
+  uint32_t max_len = 0;
+};
+
+struct drg_batch {
+  drg_ctx* ctx = nullptr;
+  uint8_t* letters = nullptr;
+  uint64_t* offsets = nullptr;
+  uint32_t* owner = nullptr;
+  std::vector<uint64_t> h_offsets;
+  std::vector<uint8_t> h_letters;
+  std::vector<uint32_t> query;
+  std::vector<uint8_t> frame;
+  uint64_t n = 0, total = 0;
+  uint32_t max_len = 0;
+};
+
+namespace drg {
+struct Band;
+// Device sequences: letters + offsets (device) and the host copy of offsets.
+struct DevSeqs {
+  const uint8_t* letters;
+  const uint64_t* offsets;
+  const std::vector<uint64_t>* h_offsets;
+};
+void score_bands(drg_ctx* c, const Band* bands, uint64_t n_bands, const DevSeqs& q, const DevSeqs& s,
+                 const Scoring& sc, int32_t* scores, drg_run_stats& st, int64_t* d_count,
+                 unsigned long long* cells_gpu);
+// Whole-path search over resident inputs (pipeline.cu).
+void search(drg_ctx* ctx, const drg_db* db, const drg_batch* b, const drg_search_config* cfg, drg_result* out);
+// Device residency helpers.
+drg_db* make_db(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offsets, uint64_t n);
+drg_batch* make_batch(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offsets, const uint32_t* query,
+                      const uint8_t* frame, uint64_t n);
+void free_db(drg_db* db);
+void free_batch(drg_batch* b);
+}  // namespace drg

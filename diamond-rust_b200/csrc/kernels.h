@@ -1,0 +1,199 @@
+// Launch wrappers of the drgpu kernels (host-callable, stream-ordered).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "common.cuh"
+
+namespace drg {
+
+// ---- seeds (seed_kernels.cu) ----------------------------------------------
+void upload_seed_params(const ShapeTable& shapes, const SeedParams& p, cudaStream_t st);
+// seq index of every letter: out[g] = i with offsets[i] <= g < offsets[i+1].
+void launch_letter_owner(const uint64_t* offsets, uint64_t n_seqs, uint64_t letter_lo, uint64_t letter_hi,
+                         uint32_t* out, cudaStream_t st);
+// Enumerate seeds of letters [letter_lo, letter_hi) for shapes [0, n_shapes):
+// keys[(g - letter_lo) * n_shapes + s] = s << 42 | key, or ~0 when no seed.
+void launch_seed_enum(const uint8_t* letters, const uint64_t* offsets, const uint32_t* owner, uint64_t letter_lo,
+                      uint64_t letter_hi, int n_shapes, uint64_t* keys, uint32_t* vals, cudaStream_t st);
+constexpr uint64_t kNoSeed = ~0ull;
+constexpr int kShapeShift = 42;
+
+// For each query run u (unique key, count, start): the reference run [lo, hi)
+// with the same key and the number of hits it yields under the expansion cap.
+void launch_join_count(const uint64_t* run_keys, const uint32_t* run_counts, uint64_t n_runs,
+                       const uint64_t* ref_keys, uint64_t n_ref, uint64_t max_expand, uint32_t* run_rlo,
+                       uint32_t* run_rcount, uint64_t* run_hits, cudaStream_t st);
+
+// Layout of the packed 64-bit hit key (target, subject, diag + doff, spos).
+struct HitKeyLayout {
+  int tb, sb, db, pb;
+  int64_t doff;
+  int total() const { return tb + sb + db + pb; }
+};
+
+// Expand every counted run into hits.  Writes hit_keys[h] (packed) when
+// keys_mode, otherwise hits[h] = {query seq, qpos, subject seq, spos} taken
+// straight from the entries' (seq, pos).
+struct JoinExpandArgs {
+  const uint64_t* run_hit_off;  // exclusive scan of run_hits, n_runs + 1 entries
+  const uint32_t* run_qstart;
+  const uint32_t* run_rlo;
+  const uint32_t* run_rcount;
+  uint64_t n_runs;
+  const uint32_t* q_vals;  // query entry payloads
+  const uint32_t* r_vals;  // reference entry payloads
+  uint64_t n_hits;
+  // keys mode: payloads are global letter indices
+  const uint32_t* q_owner;      // letter -> target
+  const uint64_t* q_offsets;    // target offsets
+  const uint32_t* r_owner;      // letter -> subject
+  const uint64_t* r_offsets;    // subject offsets
+  HitKeyLayout layout;
+  uint64_t* hit_keys;
+  // entries mode: payloads index seq/pos arrays
+  const uint32_t* q_seq;
+  const uint32_t* q_pos;
+  const uint32_t* r_seq;
+  const uint32_t* r_pos;
+  uint32_t* hits4;  // 4 x u32 per hit
+};
+void launch_join_expand(const JoinExpandArgs& a, cudaStream_t st);
+
+// ---- ungapped (ungapped_kernels.cu) -----------------------------------------
+// Scores (25x25, int8) in constant memory for X-drop and the band stage.
+void upload_score_matrix(const int8_t* scores625, cudaStream_t st);
+
+struct SegmentOut {  // ungapped.rs:11-17 plus the hit key it came from
+  uint32_t q_start, s_start, len;
+  int32_t score;
+};
+
+// flags[i] = 1 when hit i starts a new (target, subject, diagonal) run.
+void launch_run_heads(const uint64_t* keys, uint64_t n, int shift, uint8_t* flags, cudaStream_t st);
+
+struct XdropArgs {
+  const uint64_t* hit_keys;
+  uint64_t n_hits;
+  const uint32_t* run_head_idx;  // compacted indices of run heads
+  uint64_t n_runs;
+  HitKeyLayout layout;
+  const uint8_t* q_letters;
+  const uint64_t* q_offsets;
+  const uint8_t* s_letters;
+  const uint64_t* s_offsets;
+  int xdrop;
+  int cutoff;
+  SegmentOut* seg;   // indexed like hits
+  uint8_t* keep;     // 1 when hit i produced a kept segment
+  unsigned long long* xdrop_count;
+};
+void launch_xdrop_runs(const XdropArgs& a, cudaStream_t st);
+
+// Plain ungapped::xdrop for explicit anchors (stage entry point).
+void launch_xdrop_jobs(const drg_xdrop_job* jobs, uint64_t n, const uint8_t* q_letters, const uint64_t* q_offsets,
+                       const uint8_t* s_letters, const uint64_t* s_offsets, int xdrop, drg_segment* out,
+                       cudaStream_t st);
+
+// Band record (search.rs:206-230 + gapped_hsp window, search.rs:303-312).
+struct Band {
+  uint32_t target, subject;
+  int32_t d0, d1;        // diagonal span in window coordinates
+  uint32_t q0, n;        // query window [q0, q0 + n)
+  int32_t best_score;    // best segment score (band order key)
+  uint32_t rank;         // position in the pair's band order
+  uint32_t pair;         // pair index
+  uint32_t pad;
+};
+
+struct BandArgs {
+  const uint64_t* seg_keys;  // kept segment keys, sorted
+  const SegmentOut* segs;
+  uint64_t n_segs;
+  const uint32_t* pair_head_idx;  // compacted indices of pair heads (n_pairs + 1, last = n_segs)
+  uint64_t n_pairs;
+  HitKeyLayout layout;
+  const uint64_t* q_offsets;
+  Band* bands;     // indexed like segments
+  uint8_t* valid;  // 1 where a band was written
+};
+void launch_build_bands(const BandArgs& a, cudaStream_t st);
+
+// ---- banded Smith-Waterman, score only (sw_score.cu) -----------------------
+struct SwTask {        // one warp: up to 32 bands sharing query window and width
+  uint32_t first;      // index of the first band in the sorted band order
+  uint32_t count;      // 1..32
+  uint32_t row_first;  // first DP row of the warp (1-based)
+  uint32_t n_strips;   // 16-row strips to run
+  uint32_t width;      // band width W = d1 - d0 + 1 of every band of the task
+  uint32_t pad;
+};
+struct SwScoreArgs {
+  const Band* bands;
+  const uint32_t* order;  // sorted band indices
+  const SwTask* tasks;
+  uint64_t n_tasks;
+  const uint8_t* q_letters;
+  const uint64_t* q_offsets;
+  const uint8_t* s_letters;
+  const uint64_t* s_offsets;
+  int gap_open, gap_extend;
+  int32_t* score;  // per band (indexed like bands)
+  int max_width;   // largest task width of the launch (sizes the shared ring)
+  int8_t scores625[628];  // substitution scores, row-major
+};
+// Returns the dynamic shared memory bytes per block used (for reporting).
+size_t launch_sw_score(const SwScoreArgs& a, cudaStream_t st);
+constexpr int kSwMinWidth = 17;   // narrower bands use the exact kernel
+constexpr int kSwMaxWidth = 264;  // wider bands use the exact kernel
+
+// ---- exact DP with traceback (sw_exact.cu) ----------------------------------
+struct ExactJob {
+  const uint8_t* q;  // query window
+  const uint8_t* s;  // subject
+  uint32_t n, m;
+  int32_t d0, d1;
+  uint64_t scratch_off;  // byte offset of this job's scratch (trace + rows)
+  uint64_t ops_off;      // index of this job's first op slot (n + m slots)
+};
+struct ExactOut {
+  int32_t score;
+  uint32_t q_begin, q_end, s_begin, s_end;
+  uint32_t identities, positives, mismatches, gap_openings, gaps, length;
+  uint32_t n_ops;
+  uint64_t cells;
+};
+// scratch bytes a job needs (trace bytes + four int32 rows of max width)
+uint64_t exact_scratch_bytes(uint32_t n, uint32_t m, int32_t d0, int32_t d1, bool trace);
+void set_exact_matrix(const int8_t* scores625);
+void launch_sw_exact(const ExactJob* jobs, uint64_t n_jobs, int gap_open, int gap_extend, bool trace,
+                     uint8_t* scratch, uint32_t* ops, ExactOut* out, cudaStream_t st);
+
+// ---- E-value gate (evalue.cu) ---------------------------------------------
+struct AlpDev {
+  double lambda, k, ln_k, a, b, alpha, beta, sigma, tau, v_thr, c_thr;
+};
+struct SelectArgs {
+  const Band* bands;     // pair-grouped, rank ordered
+  const int32_t* score;  // per band
+  uint64_t n_bands;
+  const uint32_t* pair_first;  // first band of each pair (n_pairs + 1)
+  uint64_t n_pairs;
+  const uint64_t* q_offsets;
+  const uint64_t* s_offsets;
+  uint64_t db_letters;
+  AlpDev alp;
+  double evalue;
+  uint32_t max_hsps;
+  uint8_t* state;  // per band: 0 skipped, 1 computed-failed, 2 selected, 3 undecided
+  unsigned long long* cells_ref;
+  unsigned long long* n_computed;
+};
+void upload_alp_tables(cudaStream_t st);
+void launch_select(const SelectArgs& a, cudaStream_t st);
+uint64_t band_cells_host(uint32_t n, uint32_t m, int32_t d0, int32_t d1);
+
+// ---- probe ---------------------------------------------------------------
+void run_int_probe(double* lane_ops_per_s, double* mhz, cudaStream_t st);
+
+}  // namespace drg

@@ -1,0 +1,891 @@
+// search::run (search.rs:95-146) on one GPU.
+//
+// Device stages per index chunk (seed.rs:146-164 chunking, search.rs:127-133):
+//   seeds   query seeds once, reference seeds per chunk: enumerate + radix sort
+//   join    query key runs x sorted reference keys, expansion cap, packed hits
+//   hits    radix sort by (target, subject, diagonal, spos), de-duplicate
+//   xdrop   one thread per (target, subject, diagonal) run, cutoff 19
+//   bands   one thread per pair: merge, order, window (search.rs:206-230, 303-312)
+//   sw      packed 16-bit banded SW scores (warp = 32 bands of one query)
+//   gate    ALP E-value and the max_hsps band walk per pair
+// Host: exact E-values of the kept bands, per-target culling (search.rs:256-270),
+// then the exact traceback kernel for the surviving HSPs only.
+#include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+#include "context.h"
+#include "kernels.h"
+
+namespace drg {
+
+namespace {
+
+constexpr double kLn2 = 0.693147180559945309417232121458176568;
+
+template <typename F>
+void cub_call(drg_ctx* c, F f) {
+  size_t bytes = 0;
+  DRG_CUDA(f(nullptr, bytes));
+  void* t = c->cub_tmp.ensure(bytes);
+  DRG_CUDA(f(t, bytes));
+}
+
+template <typename T>
+T fetch(drg_ctx* c, const T* d) {
+  T* h = c->h_stage.as<T>(1);
+  DRG_CUDA(cudaMemcpyAsync(h, d, sizeof(T), cudaMemcpyDeviceToHost, c->stream));
+  DRG_CUDA(cudaStreamSynchronize(c->stream));
+  return *h;
+}
+
+template <typename T>
+void fetch_n(drg_ctx* c, std::vector<T>& out, const T* d, size_t n) {
+  out.resize(n);
+  if (n == 0) return;
+  DRG_CUDA(cudaMemcpyAsync(out.data(), d, n * sizeof(T), cudaMemcpyDeviceToHost, c->stream));
+  DRG_CUDA(cudaStreamSynchronize(c->stream));
+}
+
+// Indices i < n with flags[i] != 0, in order.
+uint64_t select_indices(drg_ctx* c, const uint8_t* flags, uint64_t n, uint32_t* out, int64_t* d_count) {
+  if (n == 0) return 0;
+  thrust::counting_iterator<uint32_t> it(0);
+  cub_call(c, [&](void* t, size_t& b) {
+    return cub::DeviceSelect::Flagged(t, b, it, flags, out, d_count, (int64_t)n, c->stream);
+  });
+  return (uint64_t)fetch(c, d_count);
+}
+
+struct Timer {
+  drg_ctx* c;
+  cudaEvent_t a, b;
+  explicit Timer(drg_ctx* ctx) : c(ctx) {
+    DRG_CUDA(cudaEventCreate(&a));
+    DRG_CUDA(cudaEventCreate(&b));
+  }
+  ~Timer() {
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  }
+  void start() { DRG_CUDA(cudaEventRecord(a, c->stream)); }
+  double stop() {
+    DRG_CUDA(cudaEventRecord(b, c->stream));
+    DRG_CUDA(cudaEventSynchronize(b));
+    float ms = 0;
+    DRG_CUDA(cudaEventElapsedTime(&ms, a, b));
+    return ms;
+  }
+};
+
+__global__ void k_count_valid(const uint64_t* keys, uint64_t n, int64_t* out) {
+  // number of keys before the first kNoSeed (keys sorted ascending)
+  uint64_t lo = 0, hi = n;
+  while (lo < hi) {
+    uint64_t m = (lo + hi) >> 1;
+    if (keys[m] < kNoSeed) lo = m + 1;
+    else hi = m;
+  }
+  *out = (int64_t)lo;
+}
+
+int64_t count_valid(drg_ctx* c, const uint64_t* keys, uint64_t n, int64_t* d_tmp) {
+  if (n == 0) return 0;
+  count_launch();
+  k_count_valid<<<1, 1, 0, c->stream>>>(keys, n, d_tmp);
+  DRG_CUDA(cudaGetLastError());
+  return fetch(c, d_tmp);
+}
+
+__global__ void k_set_u64(uint64_t* p, uint64_t v) { *p = v; }
+__global__ void k_set_u32(uint32_t* p, uint32_t v) { *p = v; }
+
+__global__ void k_rank0_flags(const Band* b, uint64_t n, uint8_t* f) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i < n) f[i] = b[i].rank == 0;
+}
+
+// Classify bands for the packed kernel and build its sort keys:
+// (width, target, window start, first real row); others get ~0.
+__global__ void k_sw_keys(const Band* bands, uint64_t n, const uint64_t* s_offsets, int max_score,
+                          uint64_t* keys, uint32_t* order) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Band b = bands[i];
+  int64_t W = (int64_t)b.d1 - b.d0 + 1;
+  int64_t m = (int64_t)(s_offsets[b.subject + 1] - s_offsets[b.subject]);
+  int64_t rs = b.d0 + 1 > 1 ? b.d0 + 1 : 1;
+  int64_t re = m + b.d1 < (int64_t)b.n ? m + b.d1 : (int64_t)b.n;
+  int64_t mn = m < (int64_t)b.n ? m : (int64_t)b.n;
+  bool fast = W >= kSwMinWidth && W <= kSwMaxWidth && (int64_t)max_score * mn <= 32000 && rs <= re &&
+              b.target < (1u << 21) && b.q0 < 65536 && re < 65536;
+  keys[i] = fast ? ((uint64_t)W << 53) | ((uint64_t)b.target << 32) | ((uint64_t)b.q0 << 16) | (uint64_t)rs
+                 : ~0ull;
+  order[i] = (uint32_t)i;
+}
+
+// Task heads: first band of each (width, target, window) group and every 32nd after.
+__global__ void k_sw_group_start(const uint64_t* keys, uint64_t n, uint32_t* gstart) {
+  uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  gstart[s] = (s == 0 || (keys[s] >> 16) != (keys[s - 1] >> 16)) ? (uint32_t)s : 0u;
+}
+__global__ void k_sw_task_flags(const uint32_t* gstart, uint64_t n, uint8_t* f) {
+  uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (s < n) f[s] = ((s - gstart[s]) % 32) == 0;
+}
+__global__ void k_sw_fill_tasks(const uint32_t* starts, uint64_t n_tasks, const uint64_t* keys, uint64_t n_fast,
+                                const uint32_t* order, const Band* bands, const uint64_t* s_offsets, SwTask* tasks,
+                                unsigned long long* cells_gpu) {
+  uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (t >= n_tasks) return;
+  uint32_t s = starts[t];
+  uint64_t grp = keys[s] >> 16;
+  uint32_t cnt = 0;
+  int64_t row_first = (int64_t)(keys[s] & 0xFFFF), row_last = 0;
+  while (cnt < 32 && s + cnt < n_fast && (keys[s + cnt] >> 16) == grp) {
+    Band b = bands[order[s + cnt]];
+    int64_t m = (int64_t)(s_offsets[b.subject + 1] - s_offsets[b.subject]);
+    int64_t re = m + b.d1 < (int64_t)b.n ? m + b.d1 : (int64_t)b.n;
+    if (re > row_last) row_last = re;
+    ++cnt;
+  }
+  SwTask k;
+  k.first = s;
+  k.count = cnt;
+  k.row_first = (uint32_t)row_first;
+  k.n_strips = (uint32_t)((row_last - row_first + 16) / 16);
+  k.width = (uint32_t)(keys[s] >> 53);
+  k.pad = 0;
+  tasks[t] = k;
+  atomicAdd(cells_gpu, (unsigned long long)k.n_strips * 16ull * (k.width + 16ull) * cnt);
+}
+
+// Bands the packed kernel did not take, or whose score is below 12.
+__global__ void k_exact_flags(const uint64_t* sw_keys_sorted, const uint32_t* order, uint64_t n_fast, uint64_t n,
+                              const int32_t* score, uint8_t* f) {
+  uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  uint32_t i = order[s];
+  f[s] = (s >= n_fast || score[i] < 12) ? 1 : 0;
+}
+
+__global__ void k_gather_positions(const uint32_t* pos, const uint32_t* order, uint64_t n, const Band* bands,
+                                   uint32_t* idx, Band* out) {
+  uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  uint32_t i = order[pos[k]];
+  idx[k] = i;
+  out[k] = bands[i];
+}
+
+__global__ void k_scatter_scores(const uint32_t* idx, const ExactOut* out, uint64_t n, int32_t* score) {
+  uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (k < n) score[idx[k]] = out[k].score;
+}
+
+__global__ void k_state_flags(const uint8_t* state, uint64_t n, uint8_t* f) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i < n) f[i] = state[i] >= 2;
+}
+
+__global__ void k_gather_bands(const uint32_t* idx, uint64_t n, const Band* bands, const int32_t* score,
+                               const uint8_t* state, Band* out_b, int32_t* out_s, uint8_t* out_st) {
+  uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  uint32_t i = idx[k];
+  out_b[k] = bands[i];
+  out_s[k] = score[i];
+  out_st[k] = state[i];
+}
+
+}  // namespace
+
+// Scores of n_bands bands (any order): the packed kernel for the bands it
+// takes, the exact kernel for the rest and for packed results below 12.
+void score_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, const DevSeqs& s,
+                 const Scoring& scr, int32_t* scores, drg_run_stats& st, int64_t* d_count,
+                 unsigned long long* cells_gpu) {
+  if (n_bands == 0) return;
+  uint8_t* flags = c->flags.as<uint8_t>(n_bands + 1);
+  uint64_t* swk = c->sw_keys.as<uint64_t>(n_bands);
+  uint64_t* swks = c->sw_keys_s.as<uint64_t>(n_bands);
+  uint32_t* swo = c->sw_order.as<uint32_t>(n_bands);
+  uint32_t* swos = c->sw_order_s.as<uint32_t>(n_bands);
+  count_launch();
+  k_sw_keys<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(bc, n_bands, s.offsets, scr.max_score, swk, swo);
+  cub_call(c, [&](void* t, size_t& b) {
+    return cub::DeviceRadixSort::SortPairs(t, b, swk, swks, swo, swos, (int64_t)n_bands, 0, 64, c->stream);
+  });
+  const uint64_t n_fast = (uint64_t)count_valid(c, swks, n_bands, d_count);
+  uint64_t n_tasks = 0;
+  if (n_fast > 0) {
+    uint32_t* gstart = c->idx.as<uint32_t>(n_fast + 1);  // reuse (pair heads no longer needed)
+    count_launch();
+    k_sw_group_start<<<ceil_div(n_fast, 256), 256, 0, c->stream>>>(swks, n_fast, gstart);
+    cub_call(c, [&](void* t, size_t& b) {
+      return cub::DeviceScan::InclusiveScan(t, b, gstart, gstart, cub::Max(), (int64_t)n_fast, c->stream);
+    });
+    count_launch();
+    k_sw_task_flags<<<ceil_div(n_fast, 256), 256, 0, c->stream>>>(gstart, n_fast, flags);
+    uint32_t* tstart = c->sel_idx.as<uint32_t>(n_fast + 1);
+    n_tasks = select_indices(c, flags, n_fast, tstart, d_count);
+    SwTask* tasks = c->sw_tasks.as<SwTask>(n_tasks);
+    count_launch();
+    k_sw_fill_tasks<<<ceil_div(n_tasks, 128), 128, 0, c->stream>>>(tstart, n_tasks, swks, n_fast, swos, bc,
+                                                                    s.offsets, tasks, cells_gpu);
+    SwScoreArgs sa{};
+    sa.bands = bc;
+    sa.order = swos;
+    sa.tasks = tasks;
+    sa.n_tasks = n_tasks;
+    sa.q_letters = qs.letters;
+    sa.q_offsets = qs.offsets;
+    sa.s_letters = s.letters;
+    sa.s_offsets = s.offsets;
+    sa.gap_open = scr.gap_open;
+    sa.gap_extend = scr.gap_extend;
+    sa.score = scores;
+    sa.max_width = kSwMaxWidth;
+    std::memcpy(sa.scores625, scr.scores, 625);
+    Timer kt(c);
+    kt.start();
+    launch_sw_score(sa, c->stream);
+    st.ms_sw_kernel += kt.stop();
+    st.sw_launches += 1;
+  }
+  // exact scores for the bands the packed kernel did not settle
+  count_launch();
+  k_exact_flags<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(swks, swos, n_fast, n_bands, scores, flags);
+  uint32_t* ex_pos = c->sel_idx.as<uint32_t>(n_bands + 1);
+  const uint64_t n_ex = select_indices(c, flags, n_bands, ex_pos, d_count);
+  if (n_ex > 0) {
+    uint32_t* ex_idx = c->idx.as<uint32_t>(n_ex);
+    Band* ex_b = c->sel_bands.as<Band>(n_ex);
+    count_launch();
+    k_gather_positions<<<ceil_div(n_ex, 256), 256, 0, c->stream>>>(ex_pos, swos, n_ex, bc, ex_idx, ex_b);
+    std::vector<uint32_t> bidx;
+    std::vector<Band> all_b;
+    fetch_n(c, bidx, ex_idx, n_ex);
+    fetch_n(c, all_b, ex_b, n_ex);
+    std::vector<ExactJob> jobs(n_ex);
+    uint64_t soff = 0;
+    for (uint64_t k = 0; k < n_ex; ++k) {
+      const Band& b = all_b[k];
+      ExactJob& j = jobs[k];
+      j.q = qs.letters + (*qs.h_offsets)[b.target] + b.q0;
+      j.s = s.letters + (*s.h_offsets)[b.subject];
+      j.n = b.n;
+      j.m = (uint32_t)((*s.h_offsets)[b.subject + 1] - (*s.h_offsets)[b.subject]);
+      j.d0 = b.d0;
+      j.d1 = b.d1;
+      j.scratch_off = soff;
+      j.ops_off = 0;
+      soff += exact_scratch_bytes(j.n, j.m, j.d0, j.d1, false);
+    }
+    ExactJob* dj = c->exact_jobs.as<ExactJob>(n_ex);
+    ExactOut* dout = c->exact_out.as<ExactOut>(n_ex);
+    uint8_t* scratch = c->exact_scratch.as<uint8_t>(soff);
+    DRG_CUDA(cudaMemcpyAsync(dj, jobs.data(), n_ex * sizeof(ExactJob), cudaMemcpyHostToDevice, c->stream));
+    launch_sw_exact(dj, n_ex, scr.gap_open, scr.gap_extend, false, scratch, nullptr, dout, c->stream);
+    count_launch();
+    k_scatter_scores<<<ceil_div(n_ex, 256), 256, 0, c->stream>>>(ex_idx, dout, n_ex, scores);
+    DRG_CUDA(cudaGetLastError());
+  }
+}
+
+namespace {
+
+struct Candidate {
+  Band band;
+  int32_t score;
+  uint8_t state;
+  uint64_t pair_key;  // chunk << 32 | pair: identifies the (target, subject) pair
+  double evalue, bits;
+};
+
+struct Search {
+  drg_ctx* c;
+  const drg_db* db;
+  const drg_batch* q;
+  Scoring sc;
+  std::vector<ShapeCode> shapes;
+  ReducedAlphabet red;
+  double complexity_cut = 0;
+  uint64_t index_chunks = 1;
+  double evalue = 1e-3;
+  uint64_t max_hsps = 1, max_targets = 25;
+  drg_run_stats st{};
+  std::vector<Candidate> cands;
+  // device scratch for counters
+  int64_t* d_count = nullptr;
+  unsigned long long* d_counters = nullptr;  // [0] xdrops [1] cells_ref [2] computed [3] cells_gpu
+
+  void configure(const drg_search_config* cfg) {
+    std::string err;
+    if (!make_scoring(cfg->matrix ? cfg->matrix : "BLOSUM62", cfg->gap_open, cfg->gap_extend, &sc, &err))
+      throw Error(DRG_ERR_INVALID, err);
+    std::string sens = cfg->sensitivity ? cfg->sensitivity : "default";
+    shapes = preset_shapes(sens);
+    red = preset_reduction(sens);
+    double cut = cfg->has_seed_cut ? cfg->seed_cut : preset_seed_cut(sens);
+    complexity_cut = cut * kLn2 * (double)shapes[0].weight;
+    index_chunks = cfg->index_chunks >= 0 ? std::max<int64_t>(cfg->index_chunks, 1) : preset_index_chunks(sens);
+    evalue = cfg->evalue;
+    max_hsps = std::max<uint32_t>(cfg->max_hsps, 1);
+    max_targets = std::max<uint32_t>(cfg->max_target_seqs, 1);
+    if ((int)shapes.size() > kMaxShapes) throw Error(DRG_ERR_INVALID, "too many seed shapes");
+    ShapeTable t{};
+    t.n = (int)shapes.size();
+    for (int s = 0; s < t.n; ++s) {
+      if (shapes[s].weight > kMaxWeight) throw Error(DRG_ERR_INVALID, "seed shape weight above 16");
+      t.weight[s] = (uint8_t)shapes[s].weight;
+      t.span[s] = (uint8_t)shapes[s].span;
+      for (int k = 0; k < shapes[s].weight; ++k) t.pos[s][k] = (uint8_t)shapes[s].positions[k];
+    }
+    SeedParams p{};
+    for (int i = 0; i < 32; ++i) p.bucket[i] = 255;
+    for (int i = 0; i < 25; ++i) p.bucket[i] = red.bucket[i];
+    p.size = (uint64_t)red.size;
+    p.cut = complexity_cut;
+    ln_factorial_table(p.lnfact);
+    upload_seed_params(t, p, c->stream);
+    upload_score_matrix(sc.scores, c->stream);
+    set_exact_matrix(sc.scores);
+    upload_alp_tables(c->stream);
+  }
+
+  HitKeyLayout layout() const {
+    HitKeyLayout L;
+    L.tb = bits_for(q->n > 0 ? q->n - 1 : 0);
+    L.sb = bits_for(db->n > 0 ? db->n - 1 : 0);
+    L.doff = (int64_t)db->max_len;
+    L.db = bits_for((uint64_t)q->max_len + db->max_len);
+    L.pb = bits_for(db->max_len);
+    if (L.tb < 1) L.tb = 1;
+    if (L.sb < 1) L.sb = 1;
+    if (L.total() > 64)
+      throw Error(DRG_ERR_INVALID, "batch too large: hit key needs " + std::to_string(L.total()) + " bits");
+    return L;
+  }
+
+  void run(drg_result* out);
+  void query_seeds(uint64_t* n_runs);
+  void chunk(uint64_t chunk_id, uint64_t c0, uint64_t c1, uint64_t n_runs);
+  void finish(drg_result* out);
+};
+
+void Search::query_seeds(uint64_t* n_runs_out) {
+  const int S = (int)shapes.size();
+  const uint64_t N = q->total * (uint64_t)S;
+  uint64_t* keys = c->q_keys.as<uint64_t>(N);
+  uint32_t* vals = c->q_vals.as<uint32_t>(N);
+  uint64_t* keys_s = c->q_keys_s.as<uint64_t>(N);
+  uint32_t* vals_s = c->q_vals_s.as<uint32_t>(N);
+  launch_seed_enum(q->letters, q->offsets, q->owner, 0, q->total, S, keys, vals, c->stream);
+  cub_call(c, [&](void* t, size_t& b) {
+    return cub::DeviceRadixSort::SortPairs(t, b, keys, keys_s, vals, vals_s, (int64_t)N, 0, 48, c->stream);
+  });
+  int64_t nv = count_valid(c, keys_s, N, d_count);
+  st.query_seeds = (uint64_t)nv;
+  uint64_t* rk = c->run_keys.as<uint64_t>(nv + 1);
+  uint32_t* rc = c->run_counts.as<uint32_t>(nv + 1);
+  uint64_t n_runs = 0;
+  if (nv > 0) {
+    cub_call(c, [&](void* t, size_t& b) {
+      return cub::DeviceRunLengthEncode::Encode(t, b, keys_s, rk, rc, d_count, (int64_t)nv, c->stream);
+    });
+    n_runs = (uint64_t)fetch(c, d_count);
+  }
+  uint32_t* qs = c->run_qstart.as<uint32_t>(n_runs + 1);
+  if (n_runs > 0)
+    cub_call(c, [&](void* t, size_t& b) {
+      return cub::DeviceScan::ExclusiveSum(t, b, rc, qs, (int64_t)n_runs, c->stream);
+    });
+  *n_runs_out = n_runs;
+}
+
+void Search::chunk(uint64_t chunk_id, uint64_t c0, uint64_t c1, uint64_t n_runs) {
+  Timer tm(c);
+  const int S = (int)shapes.size();
+  const uint64_t lo = db->h_offsets[c0], hi = db->h_offsets[c1];
+  const uint64_t N = (hi - lo) * (uint64_t)S;
+  // ---- reference seeds + join
+  tm.start();
+  uint64_t* keys = c->r_keys.as<uint64_t>(N);
+  uint32_t* vals = c->r_vals.as<uint32_t>(N);
+  uint64_t* keys_s = c->r_keys_s.as<uint64_t>(N);
+  uint32_t* vals_s = c->r_vals_s.as<uint32_t>(N);
+  launch_seed_enum(db->letters, db->offsets, db->owner + lo, lo, hi, S, keys, vals, c->stream);
+  cub_call(c, [&](void* t, size_t& b) {
+    return cub::DeviceRadixSort::SortPairs(t, b, keys, keys_s, vals, vals_s, (int64_t)N, 0, 48, c->stream);
+  });
+  int64_t nr = count_valid(c, keys_s, N, d_count);
+  st.ref_seeds += (uint64_t)nr;
+  uint32_t* rlo = c->run_rlo.as<uint32_t>(n_runs + 1);
+  uint32_t* rcnt = c->run_rcount.as<uint32_t>(n_runs + 1);
+  uint64_t* rhits = c->run_hits.as<uint64_t>(n_runs + 1);
+  uint64_t* roff = c->run_hit_off.as<uint64_t>(n_runs + 1);
+  launch_join_count(c->run_keys.as<uint64_t>(0), c->run_counts.as<uint32_t>(0), n_runs, keys_s, (uint64_t)nr, 4096,
+                    rlo, rcnt, rhits, c->stream);
+  count_launch();
+  k_set_u64<<<1, 1, 0, c->stream>>>(rhits + n_runs, 0);
+  cub_call(c, [&](void* t, size_t& b) {
+    return cub::DeviceScan::ExclusiveSum(t, b, rhits, roff, (int64_t)n_runs + 1, c->stream);
+  });
+  const uint64_t n_hits = fetch(c, roff + n_runs);
+  st.hits += n_hits;
+  const HitKeyLayout L = layout();
+  uint64_t* hk = c->hits.as<uint64_t>(n_hits);
+  if (n_hits > 0) {
+    JoinExpandArgs ja{};
+    ja.run_hit_off = roff;
+    ja.run_qstart = c->run_qstart.as<uint32_t>(0);
+    ja.run_rlo = rlo;
+    ja.run_rcount = rcnt;
+    ja.n_runs = n_runs;
+    ja.q_vals = c->q_vals_s.as<uint32_t>(0);
+    ja.r_vals = vals_s;
+    ja.n_hits = n_hits;
+    ja.q_owner = q->owner;
+    ja.q_offsets = q->offsets;
+    ja.r_owner = db->owner;
+    ja.r_offsets = db->offsets;
+    ja.layout = L;
+    ja.hit_keys = hk;
+    launch_join_expand(ja, c->stream);
+  }
+  st.ms_join += tm.stop();
+  if (n_hits == 0) return;
+  // ---- sort + unique hits
+  tm.start();
+  uint64_t* hs = c->hits_s.as<uint64_t>(n_hits);
+  uint64_t* hu = c->hits_u.as<uint64_t>(n_hits);
+  cub_call(c, [&](void* t, size_t& b) {
+    return cub::DeviceRadixSort::SortKeys(t, b, hk, hs, (int64_t)n_hits, 0, L.total(), c->stream);
+  });
+  cub_call(c, [&](void* t, size_t& b) {
+    return cub::DeviceSelect::Unique(t, b, hs, hu, d_count, (int64_t)n_hits, c->stream);
+  });
+  const uint64_t n_u = (uint64_t)fetch(c, d_count);
+  st.unique_hits += n_u;
+  st.ms_sort += tm.stop();
+  // ---- ungapped
+  tm.start();
+  uint8_t* flags = c->flags.as<uint8_t>(n_u + 1);
+  uint32_t* idx = c->idx.as<uint32_t>(n_u + 1);
+  launch_run_heads(hu, n_u, L.pb, flags, c->stream);
+  const uint64_t n_runs_d = select_indices(c, flags, n_u, idx, d_count);
+  SegmentOut* segs = c->segs.as<SegmentOut>(n_u);
+  uint8_t* keep = c->keep.as<uint8_t>(n_u);
+  XdropArgs xa{};
+  xa.hit_keys = hu;
+  xa.n_hits = n_u;
+  xa.run_head_idx = idx;
+  xa.n_runs = n_runs_d;
+  xa.layout = L;
+  xa.q_letters = q->letters;
+  xa.q_offsets = q->offsets;
+  xa.s_letters = db->letters;
+  xa.s_offsets = db->offsets;
+  xa.xdrop = sc.raw_score(12.3);
+  xa.cutoff = 19;
+  xa.seg = segs;
+  xa.keep = keep;
+  xa.xdrop_count = d_counters + 0;
+  launch_xdrop_runs(xa, c->stream);
+  uint64_t* sk = c->seg_keys.as<uint64_t>(n_u);
+  SegmentOut* sc_ = c->segs_c.as<SegmentOut>(n_u);
+  cub_call(c, [&](void* t, size_t& b) {
+    return cub::DeviceSelect::Flagged(t, b, hu, keep, sk, d_count, (int64_t)n_u, c->stream);
+  });
+  const uint64_t n_segs = (uint64_t)fetch(c, d_count);
+  cub_call(c, [&](void* t, size_t& b) {
+    return cub::DeviceSelect::Flagged(t, b, segs, keep, sc_, d_count, (int64_t)n_u, c->stream);
+  });
+  st.segments += n_segs;
+  st.ms_ungapped += tm.stop();
+  if (n_segs == 0) return;
+  // ---- bands
+  tm.start();
+  launch_run_heads(sk, n_segs, L.pb + L.db, flags, c->stream);
+  const uint64_t n_pairs = select_indices(c, flags, n_segs, idx, d_count);
+  count_launch();
+  k_set_u32<<<1, 1, 0, c->stream>>>(idx + n_pairs, (uint32_t)n_segs);
+  Band* bands = c->bands.as<Band>(n_segs);
+  uint8_t* bvalid = c->band_valid.as<uint8_t>(n_segs);
+  BandArgs ba{};
+  ba.seg_keys = sk;
+  ba.segs = sc_;
+  ba.n_segs = n_segs;
+  ba.pair_head_idx = idx;
+  ba.n_pairs = n_pairs;
+  ba.layout = L;
+  ba.q_offsets = q->offsets;
+  ba.bands = bands;
+  ba.valid = bvalid;
+  launch_build_bands(ba, c->stream);
+  Band* bc = c->bands_c.as<Band>(n_segs);
+  cub_call(c, [&](void* t, size_t& b) {
+    return cub::DeviceSelect::Flagged(t, b, bands, bvalid, bc, d_count, (int64_t)n_segs, c->stream);
+  });
+  const uint64_t n_bands = (uint64_t)fetch(c, d_count);
+  st.bands += n_bands;
+  uint32_t* pfirst = c->pair_first.as<uint32_t>(n_pairs + 1);
+  count_launch();
+  k_rank0_flags<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(bc, n_bands, flags);
+  select_indices(c, flags, n_bands, pfirst, d_count);
+  count_launch();
+  k_set_u32<<<1, 1, 0, c->stream>>>(pfirst + n_pairs, (uint32_t)n_bands);
+  st.ms_bands += tm.stop();
+  // ---- banded SW scores
+  tm.start();
+  int32_t* scores = c->scores.as<int32_t>(n_bands);
+  DevSeqs qs{q->letters, q->offsets, &q->h_offsets};
+  DevSeqs ss{db->letters, db->offsets, &db->h_offsets};
+  score_bands(c, bc, n_bands, qs, ss, sc, scores, st, d_count, d_counters + 3);
+  st.ms_sw += tm.stop();
+  flags = c->flags.as<uint8_t>(n_bands + 1);  // scratch buffers may have been regrown
+  // ---- E-value gate and band walk
+  tm.start();
+  uint8_t* state = c->state.as<uint8_t>(n_bands);
+  SelectArgs ga{};
+  ga.bands = bc;
+  ga.score = scores;
+  ga.n_bands = n_bands;
+  ga.pair_first = pfirst;
+  ga.n_pairs = n_pairs;
+  ga.q_offsets = q->offsets;
+  ga.s_offsets = db->offsets;
+  ga.db_letters = db->total;
+  const Alp& A = sc.alp;
+  ga.alp = AlpDev{A.lambda, A.k, A.ln_k, A.a, A.b, A.alpha, A.beta, A.sigma, A.tau, A.v_thr, A.c_thr};
+  ga.evalue = evalue;
+  ga.max_hsps = (uint32_t)std::min<uint64_t>(max_hsps, 0xFFFFFFFFu);
+  ga.state = state;
+  ga.cells_ref = d_counters + 1;
+  ga.n_computed = d_counters + 2;
+  launch_select(ga, c->stream);
+  count_launch();
+  k_state_flags<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(state, n_bands, flags);
+  uint32_t* sel = c->sel_idx.as<uint32_t>(n_bands + 1);
+  const uint64_t n_sel = select_indices(c, flags, n_bands, sel, d_count);
+  if (n_sel > 0) {
+    Band* gb = c->sel_bands.as<Band>(n_sel);
+    int32_t* gs = reinterpret_cast<int32_t*>(c->exact_out.as<uint8_t>(n_sel * 5 + 16));
+    uint8_t* gst = reinterpret_cast<uint8_t*>(gs + n_sel);
+    count_launch();
+    k_gather_bands<<<ceil_div(n_sel, 256), 256, 0, c->stream>>>(sel, n_sel, bc, scores, state, gb, gs, gst);
+    std::vector<Band> hb;
+    std::vector<int32_t> hs_;
+    std::vector<uint8_t> hst;
+    fetch_n(c, hb, gb, n_sel);
+    fetch_n(c, hs_, gs, n_sel);
+    fetch_n(c, hst, gst, n_sel);
+    for (uint64_t k = 0; k < n_sel; ++k) {
+      Candidate cd;
+      cd.band = hb[k];
+      cd.score = hs_[k];
+      cd.state = hst[k];
+      cd.pair_key = (chunk_id << 32) | hb[k].pair;
+      cd.evalue = 0;
+      cd.bits = 0;
+      cands.push_back(cd);
+    }
+  }
+  st.ms_select += tm.stop();
+}
+
+int cmp_cand(const Candidate& a, const Candidate& b) {  // cmp_hsp, search.rs:273-282
+  if (a.score != b.score) return b.score < a.score ? -1 : 1;
+  if (a.evalue < b.evalue) return -1;
+  if (a.evalue > b.evalue) return 1;
+  if (a.band.subject != b.band.subject) return a.band.subject < b.band.subject ? -1 : 1;
+  return 0;
+}
+
+void Search::finish(drg_result* out) {
+  auto t0 = std::chrono::steady_clock::now();
+  // exact statistics and the walk of undecided pairs
+  std::vector<Candidate> kept;
+  kept.reserve(cands.size());
+  for (size_t i = 0; i < cands.size();) {
+    size_t j = i;
+    while (j < cands.size() && cands[j].pair_key == cands[i].pair_key) ++j;
+    uint64_t nkept = 0;
+    for (size_t k = i; k < j; ++k) {
+      Candidate cd = cands[k];
+      const uint64_t qlen = q->h_offsets[cd.band.target + 1] - q->h_offsets[cd.band.target];
+      const uint64_t slen = db->h_offsets[cd.band.subject + 1] - db->h_offsets[cd.band.subject];
+      if (cd.state == 2) {
+        cd.evalue = sc.evalue(cd.score, qlen, slen, db->total);
+        cd.bits = sc.bit_score(cd.score);
+        kept.push_back(cd);
+        ++nkept;
+      } else {  // undecided: continue the reference's walk exactly
+        if (nkept >= max_hsps) continue;
+        if (cd.score <= 0) continue;
+        double e = sc.evalue(cd.score, qlen, slen, db->total);
+        if (e <= evalue) {
+          cd.evalue = e;
+          cd.bits = sc.bit_score(cd.score);
+          cd.state = 2;
+          kept.push_back(cd);
+          ++nkept;
+        }
+      }
+    }
+    i = j;
+  }
+  // per target: pairs in subject order, HSPs of a pair by cmp_hsp, pairs by
+  // their best HSP, then --max-target-seqs and --max-hsps (search.rs:256-270)
+  std::vector<std::vector<size_t>> by_target(q->n);
+  for (size_t k = 0; k < kept.size(); ++k) by_target[kept[k].band.target].push_back(k);
+  std::vector<std::vector<size_t>> final_lists(q->n);
+  for (uint64_t t = 0; t < q->n; ++t) {
+    auto& v = by_target[t];
+    std::stable_sort(v.begin(), v.end(), [&](size_t a, size_t b) { return kept[a].band.subject < kept[b].band.subject; });
+    std::vector<std::vector<size_t>> found;
+    for (size_t i = 0; i < v.size();) {
+      size_t j = i;
+      while (j < v.size() && kept[v[j]].band.subject == kept[v[i]].band.subject) ++j;
+      std::vector<size_t> hs(v.begin() + i, v.begin() + j);
+      std::stable_sort(hs.begin(), hs.end(), [&](size_t a, size_t b) { return cmp_cand(kept[a], kept[b]) < 0; });
+      found.push_back(hs);
+      i = j;
+    }
+    std::stable_sort(found.begin(), found.end(), [&](const std::vector<size_t>& a, const std::vector<size_t>& b) {
+      return cmp_cand(kept[a[0]], kept[b[0]]) < 0;
+    });
+    if (found.size() > max_targets) found.resize(max_targets);
+    for (auto& hs : found) {
+      if (hs.size() > max_hsps) hs.resize(max_hsps);
+      for (size_t k : hs) final_lists[t].push_back(k);
+    }
+  }
+  // traceback for the survivors
+  std::vector<size_t> order;
+  for (uint64_t t = 0; t < q->n; ++t)
+    for (size_t k : final_lists[t]) order.push_back(k);
+  const uint64_t nj = order.size();
+  std::vector<ExactJob> jobs(nj);
+  uint64_t soff = 0, ooff = 0;
+  for (uint64_t k = 0; k < nj; ++k) {
+    const Band& b = kept[order[k]].band;
+    ExactJob& j = jobs[k];
+    j.q = q->letters + q->h_offsets[b.target] + b.q0;
+    j.s = db->letters + db->h_offsets[b.subject];
+    j.n = b.n;
+    j.m = (uint32_t)(db->h_offsets[b.subject + 1] - db->h_offsets[b.subject]);
+    j.d0 = b.d0;
+    j.d1 = b.d1;
+    j.scratch_off = soff;
+    j.ops_off = ooff;
+    soff += exact_scratch_bytes(j.n, j.m, j.d0, j.d1, true);
+    ooff += (uint64_t)j.n + j.m;
+  }
+  st.ms_host += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  std::vector<ExactOut> eo;
+  std::vector<uint32_t> ops_all;
+  if (nj > 0) {
+    Timer tm(c);
+    tm.start();
+    ExactJob* dj = c->exact_jobs.as<ExactJob>(nj);
+    ExactOut* dout = c->exact_out.as<ExactOut>(nj);
+    uint8_t* scr = c->exact_scratch.as<uint8_t>(soff);
+    uint32_t* dops = c->exact_ops.as<uint32_t>(ooff);
+    DRG_CUDA(cudaMemcpyAsync(dj, jobs.data(), nj * sizeof(ExactJob), cudaMemcpyHostToDevice, c->stream));
+    launch_sw_exact(dj, nj, sc.gap_open, sc.gap_extend, true, scr, dops, dout, c->stream);
+    fetch_n(c, eo, dout, nj);
+    fetch_n(c, ops_all, dops, ooff);
+    st.ms_trace += tm.stop();
+  }
+  auto t1 = std::chrono::steady_clock::now();
+  // assemble per-target lists
+  out->n_targets = q->n;
+  out->target_offsets = (uint64_t*)std::malloc(sizeof(uint64_t) * (q->n + 1));
+  out->hsps = (drg_hsp*)std::malloc(sizeof(drg_hsp) * (nj + 1));
+  uint64_t total_ops = 0;
+  for (uint64_t k = 0; k < nj; ++k) total_ops += eo[k].n_ops;
+  out->ops = (uint32_t*)std::malloc(sizeof(uint32_t) * (total_ops + 1));
+  if (!out->target_offsets || !out->hsps || !out->ops) throw Error(DRG_ERR_OOM, "host allocation failed");
+  uint64_t h = 0, ko = 0, k = 0;
+  out->target_offsets[0] = 0;
+  for (uint64_t t = 0; t < q->n; ++t) {
+    for (size_t kk = 0; kk < final_lists[t].size(); ++kk, ++k) {
+      const Candidate& cd = kept[order[k]];
+      const ExactOut& r = eo[k];
+      if (r.score != cd.score)
+        throw Error(DRG_ERR_CUDA, "internal: traceback score " + std::to_string(r.score) + " != band score " +
+                                      std::to_string(cd.score));
+      drg_hsp& o = out->hsps[h++];
+      o.query = q->query[t];
+      o.subject = cd.band.subject;
+      o.frame = q->frame[t];
+      o.score = r.score;
+      o.q_begin = cd.band.q0 + r.q_begin;
+      o.q_end = cd.band.q0 + r.q_end;
+      o.s_begin = r.s_begin;
+      o.s_end = r.s_end;
+      o.bits = cd.bits;
+      o.evalue = cd.evalue;
+      o.identities = r.identities;
+      o.positives = r.positives;
+      o.mismatches = r.mismatches;
+      o.gap_openings = r.gap_openings;
+      o.gaps = r.gaps;
+      o.length = r.length;
+      o.ops_offset = ko;
+      o.n_ops = r.n_ops;
+      o.pad = 0;
+      std::memcpy(out->ops + ko, ops_all.data() + jobs[k].ops_off, r.n_ops * sizeof(uint32_t));
+      ko += r.n_ops;
+    }
+    out->target_offsets[t + 1] = h;
+  }
+  out->n_hsps = h;
+  out->n_ops = ko;
+  st.traced_bands = nj;
+  st.hsps = h;
+  st.ms_host += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t1).count();
+}
+
+void Search::run(drg_result* out) {
+  const uint64_t launches0 = kernel_launch_count();
+  Timer total(c);
+  total.start();
+  std::memset(out, 0, sizeof(*out));
+  d_count = c->counters.as<int64_t>(8);
+  d_counters = reinterpret_cast<unsigned long long*>(d_count + 2);
+  DRG_CUDA(cudaMemsetAsync(d_count, 0, 8 * sizeof(int64_t), c->stream));
+  if (q->n == 0 || db->n == 0) {
+    out->n_targets = q->n;
+    out->target_offsets = (uint64_t*)std::calloc(q->n + 1, sizeof(uint64_t));
+    out->hsps = (drg_hsp*)std::malloc(sizeof(drg_hsp));
+    out->ops = (uint32_t*)std::malloc(sizeof(uint32_t));
+    st.ms_total = total.stop();
+    out->stats = st;
+    return;
+  }
+  Timer tm(c);
+  tm.start();
+  uint64_t n_runs = 0;
+  query_seeds(&n_runs);
+  st.ms_seed = tm.stop();
+  if (n_runs > 0) {
+    uint64_t cid = 0;
+    for (auto [c0, c1] : split_chunks(db->n, index_chunks)) chunk(cid++, c0, c1, n_runs);
+  }
+  finish(out);
+  unsigned long long cnt[4];
+  DRG_CUDA(cudaMemcpyAsync(cnt, d_counters, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
+  DRG_CUDA(cudaStreamSynchronize(c->stream));
+  st.xdrops = cnt[0];
+  st.dp_cells_ref = cnt[1];
+  st.bands_computed = cnt[2];
+  st.dp_cells_gpu = cnt[3];
+  st.ms_total = total.stop();
+  st.kernel_launches = kernel_launch_count() - launches0;
+  out->stats = st;
+}
+
+}  // namespace
+
+void search(drg_ctx* ctx, const drg_db* db, const drg_batch* b, const drg_search_config* cfg, drg_result* out) {
+  Search s;
+  s.c = ctx;
+  s.db = db;
+  s.q = b;
+  s.configure(cfg);
+  s.run(out);
+  ctx->last = out->stats;
+}
+
+drg_db* make_db(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offsets, uint64_t n) {
+  drg_db* d = new drg_db();
+  d->ctx = ctx;
+  d->n = n;
+  d->h_offsets.assign(offsets, offsets + n + 1);
+  d->total = offsets[n];
+  for (uint64_t i = 0; i < n; ++i) {
+    if (offsets[i + 1] < offsets[i]) {
+      delete d;
+      throw Error(DRG_ERR_INVALID, "database offsets must be non-decreasing");
+    }
+    d->max_len = std::max<uint32_t>(d->max_len, (uint32_t)(offsets[i + 1] - offsets[i]));
+  }
+  try {
+    DRG_CUDA(cudaMalloc(&d->letters, d->total + 64));
+    DRG_CUDA(cudaMalloc(&d->offsets, (n + 1) * sizeof(uint64_t)));
+    DRG_CUDA(cudaMalloc(&d->owner, (d->total + 1) * sizeof(uint32_t)));
+    DRG_CUDA(cudaMemsetAsync(d->letters + d->total, 25, 64, ctx->stream));
+    if (d->total)
+      DRG_CUDA(cudaMemcpyAsync(d->letters, letters, d->total, cudaMemcpyHostToDevice, ctx->stream));
+    DRG_CUDA(cudaMemcpyAsync(d->offsets, offsets, (n + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, ctx->stream));
+    launch_letter_owner(d->offsets, n, 0, d->total, d->owner, ctx->stream);
+    DRG_CUDA(cudaStreamSynchronize(ctx->stream));
+  } catch (...) {
+    free_db(d);
+    throw;
+  }
+  return d;
+}
+
+drg_batch* make_batch(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offsets, const uint32_t* query,
+                      const uint8_t* frame, uint64_t n) {
+  drg_batch* b = new drg_batch();
+  b->ctx = ctx;
+  b->n = n;
+  b->h_offsets.assign(offsets, offsets + n + 1);
+  b->total = offsets[n];
+  b->h_letters.assign(letters, letters + b->total);
+  b->query.resize(n);
+  b->frame.resize(n);
+  for (uint64_t i = 0; i < n; ++i) {
+    b->query[i] = query ? query[i] : (uint32_t)i;
+    b->frame[i] = frame ? frame[i] : 0;
+    if (offsets[i + 1] < offsets[i]) {
+      delete b;
+      throw Error(DRG_ERR_INVALID, "target offsets must be non-decreasing");
+    }
+    b->max_len = std::max<uint32_t>(b->max_len, (uint32_t)(offsets[i + 1] - offsets[i]));
+  }
+  try {
+    DRG_CUDA(cudaMalloc(&b->letters, b->total + 64));
+    DRG_CUDA(cudaMalloc(&b->offsets, (n + 1) * sizeof(uint64_t)));
+    DRG_CUDA(cudaMalloc(&b->owner, (b->total + 1) * sizeof(uint32_t)));
+    DRG_CUDA(cudaMemsetAsync(b->letters + b->total, 25, 64, ctx->stream));
+    if (b->total)
+      DRG_CUDA(cudaMemcpyAsync(b->letters, letters, b->total, cudaMemcpyHostToDevice, ctx->stream));
+    DRG_CUDA(cudaMemcpyAsync(b->offsets, offsets, (n + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, ctx->stream));
+    launch_letter_owner(b->offsets, n, 0, b->total, b->owner, ctx->stream);
+    DRG_CUDA(cudaStreamSynchronize(ctx->stream));
+  } catch (...) {
+    free_batch(b);
+    throw;
+  }
+  return b;
+}
+
+void free_db(drg_db* d) {
+  if (!d) return;
+  cudaFree(d->letters);
+  cudaFree(d->offsets);
+  cudaFree(d->owner);
+  delete d;
+}
+
+void free_batch(drg_batch* b) {
+  if (!b) return;
+  cudaFree(b->letters);
+  cudaFree(b->offsets);
+  cudaFree(b->owner);
+  delete b;
+}
+
+}  // namespace drg

@@ -1,0 +1,183 @@
+// Seed enumeration (shape.rs:60-75, seed.rs:46-104) and the sort-merge
+// double-index join (seed.rs:110-143) on the device.
+//
+// Layout: one thread per (letter, shape).  Letters of a sequence batch are
+// contiguous in HBM, so the w reads of a seed hit one or two 32-byte sectors
+// shared by neighbouring threads (L1 absorbs the reuse across shapes).  Seeds
+// are written as 64-bit keys (shape << 42 | key) with a 32-bit payload (the
+// global letter index) and radix-sorted by CUB; the join walks query key runs
+// and binary-searches the sorted reference keys (they stay L2-resident).
+#include "kernels.h"
+
+namespace drg {
+
+__constant__ ShapeTable c_shapes;
+__constant__ SeedParams c_seed;
+
+void upload_seed_params(const ShapeTable& shapes, const SeedParams& p, cudaStream_t st) {
+  DRG_CUDA(cudaMemcpyToSymbolAsync(c_shapes, &shapes, sizeof(ShapeTable), 0, cudaMemcpyHostToDevice, st));
+  DRG_CUDA(cudaMemcpyToSymbolAsync(c_seed, &p, sizeof(SeedParams), 0, cudaMemcpyHostToDevice, st));
+}
+
+__global__ void k_letter_owner(const uint64_t* __restrict__ offsets, uint64_t n_seqs, uint64_t lo, uint64_t hi,
+                               uint32_t* __restrict__ out) {
+  uint64_t g = lo + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (g >= hi) return;
+  // largest i with offsets[i] <= g (sequences may be empty)
+  uint64_t a = 0, b = n_seqs;  // answer in [a, b)
+  while (b - a > 1) {
+    uint64_t m = (a + b) >> 1;
+    if (offsets[m] <= g) a = m;
+    else b = m;
+  }
+  out[g - lo] = (uint32_t)a;
+}
+
+void launch_letter_owner(const uint64_t* offsets, uint64_t n_seqs, uint64_t lo, uint64_t hi, uint32_t* out,
+                         cudaStream_t st) {
+  if (hi <= lo || n_seqs == 0) return;
+  count_launch();
+  k_letter_owner<<<ceil_div(hi - lo, 256), 256, 0, st>>>(offsets, n_seqs, lo, hi, out);
+  DRG_CUDA(cudaGetLastError());
+}
+
+// One seed: the reduced key and the log-multinomial complexity test.  The
+// counts live in three 64-bit words (8 buckets x 8 bits each); the entropy is
+// lnfact[w] minus lnfact[c_b] for b = 0, 1, ... in bucket order, the order the
+// reference subtracts in, so the double result is identical.
+__device__ __forceinline__ bool seed_at(const uint8_t* __restrict__ p, int s, uint64_t* key_out) {
+  const int w = c_shapes.weight[s];
+  const uint64_t size = c_seed.size;
+  uint64_t key = 0, c0 = 0, c1 = 0, c2 = 0;
+  for (int k = 0; k < w; ++k) {
+    uint32_t l = p[c_shapes.pos[s][k]];
+    if (l >= 20) return false;
+    uint32_t b = c_seed.bucket[l];
+    if (b >= 24) return false;
+    key = key * size + b;
+    uint64_t inc = 1ull << (8 * (b & 7));
+    if (b < 8) c0 += inc;
+    else if (b < 16) c1 += inc;
+    else c2 += inc;
+  }
+  const double cut = c_seed.cut;
+  if (cut > 0.0) {
+    double e = c_seed.lnfact[w];
+    for (int b = 0; b < (int)size; ++b) {
+      uint64_t word = b < 8 ? c0 : (b < 16 ? c1 : c2);
+      uint32_t c = (uint32_t)(word >> (8 * (b & 7))) & 0xffu;
+      if (c > 0) e = __dsub_rn(e, c_seed.lnfact[c]);
+    }
+    if (!(e >= cut)) return false;
+  }
+  *key_out = key;
+  return true;
+}
+
+__global__ void k_seed_enum(const uint8_t* __restrict__ letters, const uint64_t* __restrict__ offsets,
+                            const uint32_t* __restrict__ owner, uint64_t lo, uint64_t hi, int n_shapes,
+                            uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  uint64_t n = (hi - lo) * (uint64_t)n_shapes;
+  if (t >= n) return;
+  uint64_t g = lo + t / n_shapes;
+  int s = (int)(t % n_shapes);
+  uint32_t seq = owner[g - lo];
+  uint64_t end = offsets[seq + 1];
+  uint64_t key = 0;
+  bool ok = g + c_shapes.span[s] <= end && seed_at(letters + g, s, &key);
+  keys[t] = ok ? ((uint64_t)s << kShapeShift) | key : kNoSeed;
+  vals[t] = (uint32_t)g;
+}
+
+void launch_seed_enum(const uint8_t* letters, const uint64_t* offsets, const uint32_t* owner, uint64_t lo,
+                      uint64_t hi, int n_shapes, uint64_t* keys, uint32_t* vals, cudaStream_t st) {
+  uint64_t n = (hi - lo) * (uint64_t)n_shapes;
+  if (n == 0) return;
+  count_launch();
+  k_seed_enum<<<ceil_div(n, 256), 256, 0, st>>>(letters, offsets, owner, lo, hi, n_shapes, keys, vals);
+  DRG_CUDA(cudaGetLastError());
+}
+
+__global__ void k_join_count(const uint64_t* __restrict__ run_keys, const uint32_t* __restrict__ run_counts,
+                             uint64_t n_runs, const uint64_t* __restrict__ ref_keys, uint64_t n_ref,
+                             uint64_t max_expand, uint32_t* __restrict__ run_rlo, uint32_t* __restrict__ run_rcount,
+                             uint64_t* __restrict__ run_hits) {
+  uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (u >= n_runs) return;
+  uint64_t key = run_keys[u];
+  uint64_t a = 0, b = n_ref;
+  while (a < b) {  // lower bound
+    uint64_t m = (a + b) >> 1;
+    if (ref_keys[m] < key) a = m + 1;
+    else b = m;
+  }
+  uint64_t lo = a;
+  b = n_ref;
+  while (a < b) {  // upper bound
+    uint64_t m = (a + b) >> 1;
+    if (ref_keys[m] <= key) a = m + 1;
+    else b = m;
+  }
+  uint64_t rc = a - lo;
+  uint64_t qc = run_counts[u];
+  run_rlo[u] = (uint32_t)lo;
+  run_rcount[u] = (uint32_t)rc;
+  run_hits[u] = (rc > 0 && qc * rc <= max_expand) ? qc * rc : 0;
+}
+
+void launch_join_count(const uint64_t* run_keys, const uint32_t* run_counts, uint64_t n_runs,
+                       const uint64_t* ref_keys, uint64_t n_ref, uint64_t max_expand, uint32_t* run_rlo,
+                       uint32_t* run_rcount, uint64_t* run_hits, cudaStream_t st) {
+  if (n_runs == 0) return;
+  count_launch();
+  k_join_count<<<ceil_div(n_runs, 256), 256, 0, st>>>(run_keys, run_counts, n_runs, ref_keys, n_ref, max_expand,
+                                                      run_rlo, run_rcount, run_hits);
+  DRG_CUDA(cudaGetLastError());
+}
+
+__global__ void k_join_expand(JoinExpandArgs a) {
+  uint64_t h = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (h >= a.n_hits) return;
+  // run u: largest with run_hit_off[u] <= h
+  uint64_t lo = 0, hi = a.n_runs;
+  while (hi - lo > 1) {
+    uint64_t m = (lo + hi) >> 1;
+    if (a.run_hit_off[m] <= h) lo = m;
+    else hi = m;
+  }
+  uint64_t u = lo;
+  uint64_t k = h - a.run_hit_off[u];
+  uint32_t rc = a.run_rcount[u];
+  uint64_t qi = a.run_qstart[u] + k / rc;
+  uint64_t ri = a.run_rlo[u] + k % rc;
+  if (a.hit_keys) {
+    uint32_t qg = a.q_vals[qi], rg = a.r_vals[ri];
+    uint32_t t = a.q_owner[qg];
+    uint32_t s = a.r_owner[rg];
+    int64_t qpos = (int64_t)qg - (int64_t)a.q_offsets[t];
+    int64_t spos = (int64_t)rg - (int64_t)a.r_offsets[s];
+    const HitKeyLayout& L = a.layout;
+    uint64_t key = (uint64_t)t;
+    key = (key << L.sb) | (uint64_t)s;
+    key = (key << L.db) | (uint64_t)(qpos - spos + L.doff);
+    key = (key << L.pb) | (uint64_t)spos;
+    a.hit_keys[h] = key;
+  } else {
+    uint32_t qe = a.q_vals[qi], re = a.r_vals[ri];
+    uint32_t* o = a.hits4 + 4 * h;
+    o[0] = a.q_seq[qe];
+    o[1] = a.q_pos[qe];
+    o[2] = a.r_seq[re];
+    o[3] = a.r_pos[re];
+  }
+}
+
+void launch_join_expand(const JoinExpandArgs& a, cudaStream_t st) {
+  if (a.n_hits == 0) return;
+  count_launch();
+  k_join_expand<<<ceil_div(a.n_hits, 256), 256, 0, st>>>(a);
+  DRG_CUDA(cudaGetLastError());
+}
+
+}  // namespace drg

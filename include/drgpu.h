@@ -1,0 +1,199 @@
+/*
+ * drgpu -- B200 (sm_100a) protein-search hot path behind a C ABI.
+ *
+ * The entry points mirror the public functions of the diamond-rust crate on
+ * the seed -> join -> ungapped X-drop -> banded Smith-Waterman path, on flat
+ * buffers (plain pointers and sizes, no framework types).  Each declaration
+ * names the reference function it replaces (file:line in diamond-rust).
+ *
+ * Conventions
+ *  - Every call returns DRG_OK (0) or a DRG_ERR_* code; drg_last_error(ctx)
+ *    holds the message (the reference's Error(String), error.rs:11-52).
+ *  - Inputs are borrowed for the duration of the call; host pointers unless
+ *    the name says "device".
+ *  - Outputs allocated by the library are released with drg_free() /
+ *    drg_result_free().
+ *  - Letters are diamond-rust residue codes 0..24 (alphabet.rs:1-20):
+ *    A R N D C Q E G H I L K M F P S T W Y V B J Z X *.
+ *  - A context is used by one host thread at a time.
+ */
+#ifndef DRGPU_H
+#define DRGPU_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DRG_OK 0
+#define DRG_ERR_INVALID 1   /* bad argument (unknown matrix, shape, preset, size) */
+#define DRG_ERR_OOM 2       /* device or host allocation failed */
+#define DRG_ERR_CUDA 3      /* CUDA runtime error */
+#define DRG_ERR_IO 4        /* file could not be read or written */
+#define DRG_ERR_TIMEOUT 5   /* a bounded device-side wait gave up */
+#define DRG_ERR_NODEVICE 6  /* no usable CUDA device: there is no CPU fallback */
+
+typedef struct drg_ctx drg_ctx;
+typedef struct drg_db drg_db;       /* database resident in device memory */
+typedef struct drg_batch drg_batch; /* query batch resident in device memory */
+
+/* seed.rs:14-19 SeedEntry */
+typedef struct { uint64_t key; uint32_t seq; uint32_t pos; } drg_seed_entry;
+/* seed.rs:21-27 SeedHit */
+typedef struct { uint32_t query, qpos, subject, spos; } drg_seed_hit;
+/* ungapped.rs:11-17 Segment */
+typedef struct { uint64_t q_start, s_start, len; int32_t score; int32_t pad; } drg_segment;
+/* ungapped::xdrop arguments: query/subject index into the batch, anchor */
+typedef struct { uint32_t query, subject; uint64_t qa, sa; } drg_xdrop_job;
+/* gapped::extend_span arguments: query/subject index, diagonal range d0..=d1 */
+typedef struct { uint32_t query, subject; int64_t d0, d1; } drg_span_job;
+/* gapped.rs:35-43 Aligned (+ hsp.rs:29-57 HspStats); found == 0 is None.
+ * ops are run-length encoded as (count << 2 | op), op 0=M 1=I 2=D. */
+typedef struct {
+  int32_t found, score;
+  uint64_t q_begin, q_end, s_begin, s_end;
+  uint32_t identities, positives, mismatches, gap_openings, gaps, length;
+  uint64_t cells;      /* DP cells of the reference's row ranges */
+  uint32_t n_ops, pad; /* ops of this job start at ops_offset */
+  uint64_t ops_offset;
+} drg_aligned;
+
+/* hsp.rs:65-82 Hsp */
+typedef struct {
+  uint32_t query, subject;
+  uint32_t frame;
+  int32_t score;
+  uint32_t q_begin, q_end, s_begin, s_end;
+  double bits, evalue;
+  uint32_t identities, positives, mismatches, gap_openings, gaps, length;
+  uint64_t ops_offset;
+  uint32_t n_ops, pad;
+} drg_hsp;
+
+/* search.rs:19-48 SearchConfig.  Strings are NUL-terminated.
+ * index_chunks < 0 and has_seed_cut == 0 keep the preset's values. */
+typedef struct {
+  const char* matrix;       /* "BLOSUM62" ... ; NULL = BLOSUM62 */
+  int32_t gap_open, gap_extend; /* -1 = matrix default */
+  double evalue;
+  uint32_t max_target_seqs, max_hsps;
+  const char* sensitivity;  /* "fast", "default", "sensitive", ... */
+  int32_t index_chunks;
+  int32_t has_seed_cut;
+  double seed_cut;
+  uint32_t threads;         /* host threads for the CPU-side steps (0 = all) */
+  uint32_t flags;           /* reserved, 0 */
+} drg_search_config;
+
+/* Counters and device times of the last search (milliseconds, CUDA events). */
+typedef struct {
+  uint64_t query_seeds, ref_seeds, hits, unique_hits, xdrops, segments, bands, bands_computed;
+  uint64_t dp_cells_ref;    /* cells of the extend_span calls the reference makes */
+  uint64_t dp_cells_gpu;    /* cells the score kernel evaluated (incl. padding) */
+  uint64_t traced_bands, hsps;
+  double ms_total, ms_seed, ms_join, ms_sort, ms_ungapped, ms_bands, ms_sw, ms_select, ms_trace, ms_host;
+  double ms_h2d, ms_d2h;
+  double ms_sw_kernel;      /* device time of the packed score kernel launches alone */
+  uint64_t sw_launches, kernel_launches;
+} drg_run_stats;
+
+/* search::run result: per-target HSP lists, target_offsets[n_targets+1]. */
+typedef struct {
+  drg_hsp* hsps;
+  uint64_t n_hsps;
+  uint64_t* target_offsets;
+  uint64_t n_targets;
+  uint32_t* ops;
+  uint64_t n_ops;
+  drg_run_stats stats;
+} drg_result;
+
+/* ---- context --------------------------------------------------------- */
+int drg_ctx_create(int device, drg_ctx** out);
+void drg_ctx_destroy(drg_ctx* ctx);
+const char* drg_last_error(const drg_ctx* ctx);
+const char* drg_version(void);
+void drg_free(void* p);
+
+/* ---- stage entry points (seed.rs / ungapped.rs / gapped.rs) ------------ */
+
+/* seed::build (seed.rs:76-104): every seed of every sequence, sorted by key.
+ * reduction: 0 = murphy10, 1 = diamond9, 2 = none (reduction.rs:48-67).
+ * The order of entries that share a key is unspecified, as in the reference. */
+int drg_seed_build(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offsets, uint64_t n_seqs,
+                   const char* shape_code, int32_t reduction, uint32_t base, double complexity_cut,
+                   drg_seed_entry** out, uint64_t* n_out);
+
+/* seed::join_into (seed.rs:110-143) into n_targets hit maps, returned flat and
+ * ordered by (query, subject, qpos - spos, spos); hits are kept with their
+ * multiplicity, as the reference pushes them. */
+int drg_seed_join(drg_ctx* ctx, const drg_seed_entry* query, uint64_t n_query, const drg_seed_entry* ref,
+                  uint64_t n_ref, uint64_t n_targets, uint64_t max_expand, drg_seed_hit** out, uint64_t* n_out);
+
+/* seed::chunks (seed.rs:146-164): up to `parts` (start, end) pairs. */
+int drg_seed_chunks(uint64_t n, uint64_t parts, uint64_t* out_pairs, uint64_t* n_out);
+
+/* ungapped::xdrop (ungapped.rs:38-88) for a batch of anchors. */
+int drg_xdrop_batch(drg_ctx* ctx, const uint8_t* q_letters, const uint64_t* q_offsets, uint64_t n_q,
+                    const uint8_t* s_letters, const uint64_t* s_offsets, uint64_t n_s, const drg_xdrop_job* jobs,
+                    uint64_t n_jobs, const char* matrix, int32_t xdrop, drg_segment* out);
+
+/* gapped::extend_span (gapped.rs:67-280) for a batch of (query, subject, d0, d1).
+ * out[n_jobs]; *ops is allocated by the library. */
+int drg_extend_span_batch(drg_ctx* ctx, const uint8_t* q_letters, const uint64_t* q_offsets, uint64_t n_q,
+                          const uint8_t* s_letters, const uint64_t* s_offsets, uint64_t n_s,
+                          const drg_span_job* jobs, uint64_t n_jobs, const char* matrix, int32_t gap_open,
+                          int32_t gap_extend, drg_aligned* out, uint32_t** ops, uint64_t* n_ops);
+
+/* gapped::extend_span, score only (gapped.rs:67-203): the band score the
+ * search's E-value gate uses, computed by the same packed 16-bit kernel
+ * (exact kernel where that one does not apply).  scores[i] = 0 is None. */
+int drg_extend_span_scores(drg_ctx* ctx, const uint8_t* q_letters, const uint64_t* q_offsets, uint64_t n_q,
+                           const uint8_t* s_letters, const uint64_t* s_offsets, uint64_t n_s,
+                           const drg_span_job* jobs, uint64_t n_jobs, const char* matrix, int32_t gap_open,
+                           int32_t gap_extend, int32_t* scores, drg_run_stats* stats);
+
+/* ---- whole path: search::run (search.rs:95-146) ------------------------ */
+
+/* Database resident in device memory: letters[offsets[i]..offsets[i+1]]. */
+int drg_db_create(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offsets, uint64_t n_seqs, drg_db** out);
+void drg_db_destroy(drg_db* db);
+
+/* Query batch (search::Target list, search.rs:82-88) resident in device memory. */
+int drg_batch_create(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offsets, const uint32_t* query_index,
+                     const uint8_t* frame, uint64_t n_targets, drg_batch** out);
+void drg_batch_destroy(drg_batch* b);
+
+/* search::run over resident inputs.  Results are per-target HSP lists, each
+ * in the reference's order (best target first, search.rs:262-270). */
+int drg_search_batch(drg_ctx* ctx, const drg_db* db, const drg_batch* batch, const drg_search_config* cfg,
+                     drg_result* out);
+
+/* search::run from host buffers: uploads the database and the targets,
+ * searches, downloads the HSPs (the end-to-end drop-in call). */
+int drg_search_run(drg_ctx* ctx, const uint8_t* db_letters, const uint64_t* db_offsets, uint64_t n_db,
+                   const uint8_t* t_letters, const uint64_t* t_offsets, const uint32_t* t_query,
+                   const uint8_t* t_frame, uint64_t n_targets, const drg_search_config* cfg, drg_result* out);
+
+/* search::merge_frames (search.rs:357-396) applied to a result, in place:
+ * target_offsets becomes per-query offsets (n_queries + 1 entries). */
+int drg_merge_frames(drg_result* res, uint64_t n_queries, const uint32_t* t_query, uint64_t max_hsps,
+                     uint64_t max_target_seqs);
+
+void drg_result_free(drg_result* res);
+
+/* ---- statistics (matrix.rs:164-200, alp.rs:108-163) ------------------- */
+int drg_matrix_evalue(const char* matrix, int32_t gap_open, int32_t gap_extend, int32_t raw, uint64_t qlen,
+                      uint64_t slen, uint64_t db_letters, double* evalue, double* bits);
+
+/* ---- measurement ------------------------------------------------------- */
+/* Issue rate of the integer pipe on this device (16x2 DPX max/add-max lane
+ * operations per second), measured by a short calibrated kernel. */
+int drg_probe_int_peak(drg_ctx* ctx, double* lane_ops_per_s, double* sm_mhz);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DRGPU_H */

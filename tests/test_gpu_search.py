@@ -1,0 +1,99 @@
+"""search::run parity on the GPU: every HSP field, bit for bit, against the
+CPU oracle on seeded synthetic workloads, for every sensitivity preset."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+import drgpu  # noqa: E402
+from drgpu import synth  # noqa: E402
+
+
+def as_tuples(lists):
+    return [[h.key() for h in lst] for lst in lists]
+
+
+def run_both(ctx, orc, w, **kw):
+    dl, do = drgpu.concat(w.db)
+    tl, to = drgpu.concat(w.queries)
+    cfg = drgpu.make_config(**kw)
+    got, stats = ctx.search(dl, do, tl, to, cfg)
+    okw = dict(kw)
+    exp, ostats = orc.search(w.db, w.queries, threads=8, **{k: v for k, v in okw.items()})
+    return as_tuples(got), exp, stats, ostats
+
+
+def small(config_id, n_queries, n_db, seed=0):
+    return synth.workload(config_id, n_queries=n_queries, n_db=n_db, seed_offset=seed)
+
+
+@pytest.mark.parametrize("sens", ["fast", "default", "mid-sensitive", "sensitive", "more-sensitive",
+                                  "very-sensitive"])
+def test_search_matches_oracle_all_presets(ctx, orc, sens):
+    w = small(2, 24, 400, seed=1)
+    got, exp, stats, ostats = run_both(ctx, orc, w, sensitivity=sens)
+    assert got == exp
+    assert stats["hits"] == ostats["hits"]
+    assert sum(len(x) for x in exp) > 0
+
+
+def test_search_ultra_sensitive(ctx, orc):
+    w = small(2, 6, 150, seed=2)
+    got, exp, _, _ = run_both(ctx, orc, w, sensitivity="ultra-sensitive")
+    assert got == exp
+
+
+@pytest.mark.parametrize("kw", [
+    dict(sensitivity="sensitive", index_chunks=1),
+    dict(sensitivity="sensitive", index_chunks=7),
+    dict(sensitivity="default", max_hsps=3, max_target_seqs=4),
+    dict(sensitivity="default", evalue=10.0),
+    dict(sensitivity="sensitive", seed_cut=0.5),
+    dict(sensitivity="default", matrix="BLOSUM80"),
+    dict(sensitivity="default", matrix="PAM70", gap_open=10, gap_extend=1),
+])
+def test_search_options_match_oracle(ctx, orc, kw):
+    w = small(2, 16, 300, seed=3)
+    got, exp, _, _ = run_both(ctx, orc, w, **kw)
+    assert got == exp
+
+
+def test_search_config1_shape(ctx, orc):
+    w = synth.workload(1, n_db=1200)
+    got, exp, stats, _ = run_both(ctx, orc, w, sensitivity="default")
+    assert got == exp
+    assert len(exp[0]) >= 1
+
+
+def test_search_empty_inputs(ctx):
+    dl, do = drgpu.concat([np.zeros(10, np.uint8)])
+    tl, to = drgpu.concat([])
+    lists, _ = ctx.search(dl, do, tl, to, drgpu.make_config())
+    assert lists == []
+    tl, to = drgpu.concat([np.zeros(0, np.uint8), np.arange(20, dtype=np.uint8)])
+    lists, _ = ctx.search(dl, do, tl, to, drgpu.make_config())
+    assert len(lists) == 2 and lists[0] == []
+
+
+def test_search_rejects_unknown_matrix(ctx):
+    dl, do = drgpu.concat([np.zeros(10, np.uint8)])
+    with pytest.raises(drgpu.DrgError) as ei:
+        ctx.search(dl, do, dl, do, drgpu.make_config(matrix="NOPE"))
+    assert ei.value.code == 1
+
+
+def test_resident_search_equals_host_search(ctx):
+    w = small(2, 12, 250, seed=4)
+    dl, do = drgpu.concat(w.db)
+    tl, to = drgpu.concat(w.queries)
+    cfg = drgpu.make_config(sensitivity="sensitive")
+    host, _ = ctx.search(dl, do, tl, to, cfg)
+    db = drgpu.ResidentDb(ctx, dl, do)
+    b = drgpu.ResidentBatch(ctx, tl, to)
+    try:
+        for _ in range(2):  # the resident objects can be searched repeatedly
+            res, _, _ = drgpu.search_resident(ctx, db, b, cfg)
+            assert as_tuples(res) == as_tuples(host)
+    finally:
+        b.close()
+        db.close()
