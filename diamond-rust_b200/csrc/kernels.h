@@ -166,6 +166,10 @@ struct ExactOut {
 // scratch bytes a job needs (trace bytes + four int32 rows of max width)
 uint64_t exact_scratch_bytes(uint32_t n, uint32_t m, int32_t d0, int32_t d1, bool trace);
 void set_exact_matrix(const int8_t* scores625);
+// Same kernel with the substitution scores passed per launch (no shared host state).
+void launch_sw_exact_with_matrix(const ExactJob* jobs, uint64_t n_jobs, int gap_open, int gap_extend, bool trace,
+                                 uint8_t* scratch, uint32_t* ops, ExactOut* out, const int8_t* scores625,
+                                 cudaStream_t st);
 void launch_sw_exact(const ExactJob* jobs, uint64_t n_jobs, int gap_open, int gap_extend, bool trace,
                      uint8_t* scratch, uint32_t* ops, ExactOut* out, cudaStream_t st);
 

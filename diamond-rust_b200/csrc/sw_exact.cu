@@ -237,6 +237,17 @@ uint64_t exact_scratch_bytes(uint32_t n, uint32_t m, int32_t d0, int32_t d1, boo
   return (bytes + 255) & ~255ull;
 }
 
+void launch_sw_exact_with_matrix(const ExactJob* jobs, uint64_t n_jobs, int go, int ge, bool trace,
+                                 uint8_t* scratch, uint32_t* ops, ExactOut* out, const int8_t* scores625,
+                                 cudaStream_t st) {
+  if (n_jobs == 0) return;
+  MatArg m;
+  for (int i = 0; i < 625; ++i) m.s[i] = scores625[i];
+  count_launch();
+  k_sw_exact<<<ceil_div(n_jobs, 64), 64, 0, st>>>(jobs, n_jobs, go, ge, trace, scratch, ops, out, m);
+  DRG_CUDA(cudaGetLastError());
+}
+
 static MatArg g_mat_arg;
 void set_exact_matrix(const int8_t* s625) {
   for (int i = 0; i < 625; ++i) g_mat_arg.s[i] = s625[i];
