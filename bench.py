@@ -48,7 +48,8 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="drgpu", choices=["drgpu", "reference"])
     p.add_argument("--cpu-sample", type=int, default=100, help="queries in the CPU baseline sample")
-    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (development only)")
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
+    p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     return p.parse_args()
 
 
@@ -235,11 +236,11 @@ def main():
     launches = sum(s["kernel_launches"] for s in steps)
 
     # ---- end to end through the host-buffer C-ABI call --------------------
-    for _ in range(min(args.warmup, 2)):
+    for _ in range(0 if args.no_e2e else min(args.warmup, 2)):
         ctx.search(dl, do, tl, to, cfg)
-    e2e_s = 0.0
+    e2e_s = 1e-9
     d2h = 0
-    for _ in range(args.steps):
+    for _ in range(0 if args.no_e2e else args.steps):
         flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -285,9 +286,14 @@ def main():
                          "cells_evaluated_per_launch": cells_gpu / max(sw_launches, 1),
                          "ms_per_launch": sw_ms / max(sw_launches, 1)},
             "stages_ms": {k: round(s0[k], 3) for k in ("ms_seed", "ms_join", "ms_sort", "ms_ungapped", "ms_bands",
-                                                         "ms_sw", "ms_select", "ms_trace", "ms_host")},
+                                                         "ms_sw", "ms_sw_kernel", "ms_select", "ms_trace",
+                                                         "ms_trace_kernel", "ms_host")},
+            "sw_classes": {"width_max": [136, 272, 544, 1700], "warps": s0["sw_class_tasks"],
+                           "longest_warp_steps": s0["sw_class_max_steps"],
+                           "ms": [round(x, 3) for x in s0["ms_sw_class"]]},
             "counts": {k: int(s0[k]) for k in ("query_seeds", "ref_seeds", "hits", "unique_hits", "xdrops",
-                                                "segments", "bands", "bands_computed", "traced_bands", "hsps")},
+                                                "segments", "bands", "bands_computed", "exact_bands", "traced_bands",
+                                                "hsps")},
             "e2e": e2e,
             "gpu_launches": int(launches),
             "cpu_baseline": cpu,

@@ -121,7 +121,9 @@ int drg_ctx_create(int device, drg_ctx** out) {
   drg_ctx* c = new (std::nothrow) drg_ctx();
   if (!c) return DRG_ERR_OOM;
   c->device = device;
-  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess) {
+    if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return DRG_ERR_CUDA;
   }
@@ -133,7 +135,9 @@ void drg_ctx_destroy(drg_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
+  cudaStreamSynchronize(c->side);
   cudaStreamDestroy(c->stream);
+  cudaStreamDestroy(c->side);
   delete c;
 }
 
@@ -435,7 +439,8 @@ int drg_extend_span_scores(drg_ctx* c, const uint8_t* ql, const uint64_t* qo, ui
   DRG_CUDA(cudaMemsetAsync(cells.p, 0, 8, c->stream));
   if (n) DRG_CUDA(cudaMemcpyAsync(db_.p, hb.data(), n * sizeof(Band), cudaMemcpyHostToDevice, c->stream));
   drg_run_stats st{};
-  score_bands(c, db_.p, n, qs.view(), ss.view(), sc, ds.p, st, cnt.p, cells.p);
+  run_bands(c, db_.p, n, qs.view(), ss.view(), sc, false, ds.p, nullptr, nullptr, nullptr, nullptr, nullptr, st, cnt.p,
+            cells.p);
   if (n) DRG_CUDA(cudaMemcpyAsync(scores, ds.p, n * 4, cudaMemcpyDeviceToHost, c->stream));
   unsigned long long cg = 0;
   DRG_CUDA(cudaMemcpyAsync(&cg, cells.p, 8, cudaMemcpyDeviceToHost, c->stream));

@@ -13,6 +13,7 @@
 struct drg_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t side = nullptr;  // concurrent launches (wide-band classes)
   std::string err;
   // seed stage
   drg::DevBuf q_keys, q_vals, q_keys_s, q_vals_s, r_keys, r_vals, r_keys_s, r_vals_s, cub_tmp;
@@ -23,6 +24,8 @@ struct drg_ctx {
   // bands and DP
   drg::DevBuf bands, bands_c, band_valid, pair_first, sw_keys, sw_keys_s, sw_order, sw_order_s, sw_tasks, scores,
       state, sel_idx, sel_bands, exact_jobs, exact_out, exact_scratch, exact_ops;
+  drg::DevBuf tband, task_size, task_off, trace, rev, ex_bands, ops_off, trace_out, task_max;
+  drg::DevBuf sw_tasks_u, task_key, task_key_s, task_val, task_val_s, best_row;
   drg::HostBuf h_stage;
   cudaEvent_t ev[16] = {};
   drg_run_stats last{};
@@ -59,9 +62,11 @@ struct DevSeqs {
   const uint64_t* offsets;
   const std::vector<uint64_t>* h_offsets;
 };
-void score_bands(drg_ctx* c, const Band* bands, uint64_t n_bands, const DevSeqs& q, const DevSeqs& s,
-                 const Scoring& sc, int32_t* scores, drg_run_stats& st, int64_t* d_count,
-                 unsigned long long* cells_gpu);
+struct ExactOut;
+void run_bands(drg_ctx* c, const Band* bands, uint64_t n_bands, const DevSeqs& q, const DevSeqs& s,
+               const Scoring& sc, bool trace, int32_t* scores, int32_t* best_row, ExactOut* out, uint32_t* ops,
+               const uint64_t* d_ops_off, const std::vector<uint64_t>* h_ops_off, drg_run_stats& st,
+               int64_t* d_count, unsigned long long* cells_gpu);
 // Whole-path search over resident inputs (pipeline.cu).
 void search(drg_ctx* ctx, const drg_db* db, const drg_batch* b, const drg_search_config* cfg, drg_result* out);
 // Device residency helpers.

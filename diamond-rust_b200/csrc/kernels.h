@@ -120,32 +120,63 @@ struct BandArgs {
 void launch_build_bands(const BandArgs& a, cudaStream_t st);
 
 // ---- banded Smith-Waterman, score only (sw_score.cu) -----------------------
-struct SwTask {        // one warp: up to 32 bands sharing query window and width
+struct SwTask {        // one warp: up to 32 bands sharing a query window
   uint32_t first;      // index of the first band in the sorted band order
   uint32_t count;      // 1..32
   uint32_t row_first;  // first DP row of the warp (1-based)
   uint32_t n_strips;   // 16-row strips to run
-  uint32_t width;      // band width W = d1 - d0 + 1 of every band of the task
-  uint32_t pad;
+  uint32_t width;      // widest band of the task, W_max = d1 - d0 + 1
+  uint32_t w_min;      // narrowest band of the task
+  uint64_t trace_off;  // trace mode: first uint2 of the task's trace
+};
+// Trace-pass result of one band: where its nibbles are and its first maximum.
+struct TraceBand {
+  uint64_t trace_off;  // task trace_off + lane
+  uint32_t row_first, width;
+  int32_t score, best_i, best_j, pad;
 };
 struct SwScoreArgs {
   const Band* bands;
   const uint32_t* order;  // sorted band indices
   const SwTask* tasks;
-  uint64_t n_tasks;
+  uint64_t task_lo, task_hi;  // tasks of this launch
   const uint8_t* q_letters;
   const uint64_t* q_offsets;
   const uint8_t* s_letters;
   const uint64_t* s_offsets;
   int gap_open, gap_extend;
-  int32_t* score;  // per band (indexed like bands)
-  int max_width;   // largest task width of the launch (sizes the shared ring)
+  int32_t* score;     // score mode: per band (indexed like bands)
+  int32_t* best_row;  // score mode: first DP row holding the best (0 if none)
+  uint2* trace;       // trace mode: nibble buffer
+  TraceBand* tband;   // trace mode: per band (indexed like bands)
   int8_t scores625[628];  // substitution scores, row-major
 };
-// Returns the dynamic shared memory bytes per block used (for reporting).
-size_t launch_sw_score(const SwScoreArgs& a, cudaStream_t st);
+struct ExactOut;
+struct SwWalkArgs {
+  const Band* bands;
+  const TraceBand* tband;
+  uint64_t n_bands;
+  const uint2* trace;
+  const uint8_t* q_letters;
+  const uint64_t* q_offsets;
+  const uint8_t* s_letters;
+  const uint64_t* s_offsets;
+  const uint64_t* ops_off;  // per band: first op slot (n + m slots each)
+  uint8_t* rev;             // per band: n + m bytes at ops_off
+  uint32_t* ops;
+  ExactOut* out;
+  int8_t scores625[628];
+};
+// Width classes of the packed kernel by the widest band of a warp (the shared
+// ring holds W + 1 words per thread); each fits 3 blocks per SM but the last.
 constexpr int kSwMinWidth = 17;   // narrower bands use the exact kernel
-constexpr int kSwMaxWidth = 264;  // wider bands use the exact kernel
+constexpr int kSwC0 = 136, kSwC1 = 272, kSwC2 = 544, kSwC3 = 1700;
+constexpr int kSwClassMax[4] = {kSwC0, kSwC1, kSwC2, kSwC3};  // 4, 2, 1, 1 warps per block
+constexpr int kSwMaxWidth = 1700;                       // wider bands use the exact kernel
+constexpr int kSwClasses = 4;
+int sw_width_class(int width);  // 0..3, or -1 for the exact kernel
+void launch_sw_class(const SwScoreArgs& a, int cls, bool trace, cudaStream_t st);
+void launch_sw_walk(const SwWalkArgs& a, cudaStream_t st);
 
 // ---- exact DP with traceback (sw_exact.cu) ----------------------------------
 struct ExactJob {

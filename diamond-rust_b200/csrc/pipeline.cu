@@ -110,8 +110,12 @@ __global__ void k_rank0_flags(const Band* b, uint64_t n, uint8_t* f) {
   if (i < n) f[i] = b[i].rank == 0;
 }
 
+__host__ __device__ __forceinline__ int sw_class_of(uint32_t w) {
+  return w <= (uint32_t)kSwC0 ? 0 : (w <= (uint32_t)kSwC1 ? 1 : (w <= (uint32_t)kSwC2 ? 2 : 3));
+}
+
 // Classify bands for the packed kernel and build its sort keys:
-// (width, target, window start, first real row); others get ~0.
+// (target, window start, width, first real row); others get ~0.
 __global__ void k_sw_keys(const Band* bands, uint64_t n, const uint64_t* s_offsets, int max_score,
                           uint64_t* keys, uint32_t* order) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
@@ -124,55 +128,110 @@ __global__ void k_sw_keys(const Band* bands, uint64_t n, const uint64_t* s_offse
   int64_t mn = m < (int64_t)b.n ? m : (int64_t)b.n;
   bool fast = W >= kSwMinWidth && W <= kSwMaxWidth && (int64_t)max_score * mn <= 32000 && rs <= re &&
               b.target < (1u << 21) && b.q0 < 65536 && re < 65536;
-  keys[i] = fast ? ((uint64_t)W << 53) | ((uint64_t)b.target << 32) | ((uint64_t)b.q0 << 16) | (uint64_t)rs
+  keys[i] = fast ? ((uint64_t)b.target << 43) | ((uint64_t)b.q0 << 27) | ((uint64_t)W << 16) | (uint64_t)rs
                  : ~0ull;
   order[i] = (uint32_t)i;
 }
 
-// Task heads: first band of each (width, target, window) group and every 32nd after.
+// Task heads: first band of each (target, window) group and every 32nd after
+// (a group's bands are in width order, so a warp's widths are close).
 __global__ void k_sw_group_start(const uint64_t* keys, uint64_t n, uint32_t* gstart) {
   uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (s >= n) return;
-  gstart[s] = (s == 0 || (keys[s] >> 16) != (keys[s - 1] >> 16)) ? (uint32_t)s : 0u;
+  gstart[s] = (s == 0 || (keys[s] >> 27) != (keys[s - 1] >> 27)) ? (uint32_t)s : 0u;
 }
 __global__ void k_sw_task_flags(const uint32_t* gstart, uint64_t n, uint8_t* f) {
   uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (s < n) f[s] = ((s - gstart[s]) % 32) == 0;
 }
 __global__ void k_sw_fill_tasks(const uint32_t* starts, uint64_t n_tasks, const uint64_t* keys, uint64_t n_fast,
-                                const uint32_t* order, const Band* bands, const uint64_t* s_offsets, SwTask* tasks,
+                                const uint32_t* order, const Band* bands, const uint64_t* s_offsets, bool row_limit,
+                                SwTask* tasks, uint64_t* sort_key, uint32_t* sort_val, uint64_t* trace_size,
                                 unsigned long long* cells_gpu) {
   uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (t >= n_tasks) return;
   uint32_t s = starts[t];
-  uint64_t grp = keys[s] >> 16;
+  uint64_t grp = keys[s] >> 27;
   uint32_t cnt = 0;
-  int64_t row_first = (int64_t)(keys[s] & 0xFFFF), row_last = 0;
-  while (cnt < 32 && s + cnt < n_fast && (keys[s + cnt] >> 16) == grp) {
-    Band b = bands[order[s + cnt]];
+  int64_t row_first = INT64_MAX, row_last = 0;
+  uint32_t wmin = 0xFFFFFFFFu, wmax = 0;
+  while (cnt < 32 && s + cnt < n_fast && (keys[s + cnt] >> 27) == grp) {
+    const uint64_t key = keys[s + cnt];
+    const Band b = bands[order[s + cnt]];
     int64_t m = (int64_t)(s_offsets[b.subject + 1] - s_offsets[b.subject]);
     int64_t re = m + b.d1 < (int64_t)b.n ? m + b.d1 : (int64_t)b.n;
+    if (row_limit && b.pad > 0 && (int64_t)b.pad < re) re = b.pad;  // traceback: rows up to the best
+    const int64_t rs = (int64_t)(key & 0xFFFF);
+    const uint32_t w = (uint32_t)((key >> 16) & 0x7FF);
     if (re > row_last) row_last = re;
+    if (rs < row_first) row_first = rs;
+    if (w < wmin) wmin = w;
+    if (w > wmax) wmax = w;
     ++cnt;
   }
+  if (row_last < row_first) row_last = row_first;
   SwTask k;
   k.first = s;
   k.count = cnt;
   k.row_first = (uint32_t)row_first;
   k.n_strips = (uint32_t)((row_last - row_first + 16) / 16);
-  k.width = (uint32_t)(keys[s] >> 53);
-  k.pad = 0;
+  k.width = wmax;
+  k.w_min = wmin;
+  k.trace_off = 0;
   tasks[t] = k;
-  atomicAdd(cells_gpu, (unsigned long long)k.n_strips * 16ull * (k.width + 16ull) * cnt);
+  const uint64_t steps = (uint64_t)k.n_strips * (wmax + 16ull);
+  const int cls = sw_class_of(wmax);
+  sort_key[t] = ((uint64_t)cls << 60) | ((~steps) & ((1ull << 60) - 1));  // class, then longest first
+  sort_val[t] = (uint32_t)t;
+  if (trace_size) trace_size[t] = steps * 32ull;
+  atomicAdd(cells_gpu, (unsigned long long)k.n_strips * 16ull * (wmax + 16ull) * cnt);
 }
 
-// Bands the packed kernel did not take, or whose score is below 12.
-__global__ void k_exact_flags(const uint64_t* sw_keys_sorted, const uint32_t* order, uint64_t n_fast, uint64_t n,
-                              const int32_t* score, uint8_t* f) {
+__global__ void k_task_trace_size(const SwTask* tasks, uint64_t n, uint64_t* size) {
+  uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (t < n) size[t] = (uint64_t)tasks[t].n_strips * (tasks[t].width + 16ull) * 32ull;
+  else if (t == n) size[t] = 0;
+}
+
+__global__ void k_gather_tasks(const SwTask* in, const uint32_t* idx, uint64_t n, SwTask* out) {
+  uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (t < n) out[t] = in[idx[t]];
+}
+
+// First task of classes 1, 2 and 3 (tasks are sorted by class).
+__global__ void k_task_bounds(const SwTask* tasks, uint64_t n, int64_t* out) {
+  for (int c = 0; c < kSwClasses - 1; ++c) {
+    uint64_t lo = 0, hi = n;
+    while (lo < hi) {
+      uint64_t m = (lo + hi) >> 1;
+      if (sw_class_of(tasks[m].width) <= c) lo = m + 1;
+      else hi = m;
+    }
+    out[c] = (int64_t)lo;
+  }
+}
+
+// Longest warp of each width class, in column steps (strips x (W + 16)).
+__global__ void k_task_steps(const SwTask* tasks, uint64_t n, unsigned long long* mx) {
+  uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const SwTask k = tasks[t];
+  atomicMax(mx + sw_class_of(k.width), (unsigned long long)k.n_strips * (k.width + 16ull));
+}
+
+__global__ void k_set_trace_off(SwTask* tasks, const uint64_t* off, uint64_t n) {
+  uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (t < n) tasks[t].trace_off = off[t];
+}
+
+// Bands the packed kernel did not take, or whose best is below 12.
+__global__ void k_exact_flags(const uint32_t* order, uint64_t n_fast, uint64_t n, const int32_t* score,
+                              const TraceBand* tband, uint8_t* f) {
   uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (s >= n) return;
   uint32_t i = order[s];
-  f[s] = (s >= n_fast || score[i] < 12) ? 1 : 0;
+  int v = tband ? tband[i].score : score[i];
+  f[s] = (s >= n_fast || v < 12) ? 1 : 0;
 }
 
 __global__ void k_gather_positions(const uint32_t* pos, const uint32_t* order, uint64_t n, const Band* bands,
@@ -189,28 +248,42 @@ __global__ void k_scatter_scores(const uint32_t* idx, const ExactOut* out, uint6
   if (k < n) score[idx[k]] = out[k].score;
 }
 
+__global__ void k_scatter_exact(const uint32_t* idx, const ExactOut* src, uint64_t n, ExactOut* dst) {
+  uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (k < n) dst[idx[k]] = src[k];
+}
+
 __global__ void k_state_flags(const uint8_t* state, uint64_t n, uint8_t* f) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i < n) f[i] = state[i] >= 2;
 }
 
 __global__ void k_gather_bands(const uint32_t* idx, uint64_t n, const Band* bands, const int32_t* score,
-                               const uint8_t* state, Band* out_b, int32_t* out_s, uint8_t* out_st) {
+                               const int32_t* best_row, const uint8_t* state, Band* out_b, int32_t* out_s,
+                               uint8_t* out_st) {
   uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (k >= n) return;
   uint32_t i = idx[k];
-  out_b[k] = bands[i];
+  Band b = bands[i];
+  b.pad = best_row ? (uint32_t)best_row[i] : 0u;  // first row of the best: the traceback needs no row below
+  out_b[k] = b;
   out_s[k] = score[i];
   out_st[k] = state[i];
 }
 
 }  // namespace
 
-// Scores of n_bands bands (any order): the packed kernel for the bands it
-// takes, the exact kernel for the rest and for packed results below 12.
-void score_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, const DevSeqs& s,
-                 const Scoring& scr, int32_t* scores, drg_run_stats& st, int64_t* d_count,
-                 unsigned long long* cells_gpu) {
+// The banded DP of n_bands bands (any order).  The packed kernel takes the
+// bands whose width it supports (by width class) and whose best cannot
+// overflow 16 bits; the exact kernel takes the rest and every band whose
+// packed best is below 12.
+//  score mode (trace == false): scores[i] = best score (0 = None).
+//  trace mode: out[i] and the band's ops at h_ops_off[i] in ops (n + m slots
+//  per band), the same records the exact kernel produces.
+void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, const DevSeqs& s,
+               const Scoring& scr, bool trace, int32_t* scores, int32_t* best_row, ExactOut* out, uint32_t* ops,
+               const uint64_t* d_ops_off, const std::vector<uint64_t>* h_ops_off, drg_run_stats& st,
+               int64_t* d_count, unsigned long long* cells_gpu) {
   if (n_bands == 0) return;
   uint8_t* flags = c->flags.as<uint8_t>(n_bands + 1);
   uint64_t* swk = c->sw_keys.as<uint64_t>(n_bands);
@@ -223,9 +296,13 @@ void score_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs
     return cub::DeviceRadixSort::SortPairs(t, b, swk, swks, swo, swos, (int64_t)n_bands, 0, 64, c->stream);
   });
   const uint64_t n_fast = (uint64_t)count_valid(c, swks, n_bands, d_count);
-  uint64_t n_tasks = 0;
+  TraceBand* tb = nullptr;
+  if (trace) {
+    tb = c->tband.as<TraceBand>(n_bands);
+    DRG_CUDA(cudaMemsetAsync(tb, 0xFF, n_bands * sizeof(TraceBand), c->stream));  // score -1: not traced
+  }
   if (n_fast > 0) {
-    uint32_t* gstart = c->idx.as<uint32_t>(n_fast + 1);  // reuse (pair heads no longer needed)
+    uint32_t* gstart = c->idx.as<uint32_t>(n_fast + 1);
     count_launch();
     k_sw_group_start<<<ceil_div(n_fast, 256), 256, 0, c->stream>>>(swks, n_fast, gstart);
     cub_call(c, [&](void* t, size_t& b) {
@@ -234,16 +311,34 @@ void score_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs
     count_launch();
     k_sw_task_flags<<<ceil_div(n_fast, 256), 256, 0, c->stream>>>(gstart, n_fast, flags);
     uint32_t* tstart = c->sel_idx.as<uint32_t>(n_fast + 1);
-    n_tasks = select_indices(c, flags, n_fast, tstart, d_count);
+    const uint64_t n_tasks = select_indices(c, flags, n_fast, tstart, d_count);
+    SwTask* tasks_u = c->sw_tasks_u.as<SwTask>(n_tasks);
     SwTask* tasks = c->sw_tasks.as<SwTask>(n_tasks);
+    uint64_t* tkey = c->task_key.as<uint64_t>(n_tasks);
+    uint64_t* tkey_s = c->task_key_s.as<uint64_t>(n_tasks);
+    uint32_t* tval = c->task_val.as<uint32_t>(n_tasks);
+    uint32_t* tval_s = c->task_val_s.as<uint32_t>(n_tasks);
     count_launch();
     k_sw_fill_tasks<<<ceil_div(n_tasks, 128), 128, 0, c->stream>>>(tstart, n_tasks, swks, n_fast, swos, bc,
-                                                                    s.offsets, tasks, cells_gpu);
+                                                                    s.offsets, trace, tasks_u, tkey, tval, nullptr,
+                                                                    cells_gpu);
+    // by width class, longest warps first within a class
+    cub_call(c, [&](void* t, size_t& b) {
+      return cub::DeviceRadixSort::SortPairs(t, b, tkey, tkey_s, tval, tval_s, (int64_t)n_tasks, 0, 64, c->stream);
+    });
+    count_launch();
+    k_gather_tasks<<<ceil_div(n_tasks, 256), 256, 0, c->stream>>>(tasks_u, tval_s, n_tasks, tasks);
+    count_launch();
+    // task_max holds the per-class step maxima, then the class bounds
+    int64_t* dbounds = reinterpret_cast<int64_t*>(c->task_max.as<unsigned long long>(2 * kSwClasses)) + kSwClasses;
+    k_task_bounds<<<1, 1, 0, c->stream>>>(tasks, n_tasks, dbounds);
+    int64_t bounds[kSwClasses - 1];
+    DRG_CUDA(cudaMemcpyAsync(bounds, dbounds, sizeof(bounds), cudaMemcpyDeviceToHost, c->stream));
+    DRG_CUDA(cudaStreamSynchronize(c->stream));
     SwScoreArgs sa{};
     sa.bands = bc;
     sa.order = swos;
     sa.tasks = tasks;
-    sa.n_tasks = n_tasks;
     sa.q_letters = qs.letters;
     sa.q_offsets = qs.offsets;
     sa.s_letters = s.letters;
@@ -251,22 +346,97 @@ void score_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs
     sa.gap_open = scr.gap_open;
     sa.gap_extend = scr.gap_extend;
     sa.score = scores;
-    sa.max_width = kSwMaxWidth;
+    sa.best_row = best_row;
+    sa.tband = tb;
     std::memcpy(sa.scores625, scr.scores, 625);
-    Timer kt(c);
-    kt.start();
-    launch_sw_score(sa, c->stream);
-    st.ms_sw_kernel += kt.stop();
-    st.sw_launches += 1;
+    if (trace) {
+      uint64_t* tsize = c->task_size.as<uint64_t>(n_tasks + 1);
+      uint64_t* toff = c->task_off.as<uint64_t>(n_tasks + 1);
+      count_launch();
+      k_task_trace_size<<<ceil_div(n_tasks + 1, 256), 256, 0, c->stream>>>(tasks, n_tasks, tsize);
+      cub_call(c, [&](void* t, size_t& b) {
+        return cub::DeviceScan::ExclusiveSum(t, b, tsize, toff, (int64_t)n_tasks + 1, c->stream);
+      });
+      count_launch();
+      k_set_trace_off<<<ceil_div(n_tasks, 256), 256, 0, c->stream>>>(tasks, toff, n_tasks);
+      const uint64_t total = fetch(c, toff + n_tasks);
+      sa.trace = c->trace.as<uint2>(total);
+    }
+    uint64_t lo[kSwClasses], hi[kSwClasses];
+    for (int k = 0; k < kSwClasses; ++k) {
+      lo[k] = k == 0 ? 0 : (uint64_t)bounds[k - 1];
+      hi[k] = k == kSwClasses - 1 ? n_tasks : (uint64_t)bounds[k];
+    }
+    unsigned long long* dmax = c->task_max.as<unsigned long long>(2 * kSwClasses);
+    DRG_CUDA(cudaMemsetAsync(dmax, 0, kSwClasses * sizeof(unsigned long long), c->stream));
+    count_launch();
+    k_task_steps<<<ceil_div(n_tasks, 256), 256, 0, c->stream>>>(tasks, n_tasks, dmax);
+    unsigned long long hmax[kSwClasses];
+    DRG_CUDA(cudaMemcpyAsync(hmax, dmax, sizeof(hmax), cudaMemcpyDeviceToHost, c->stream));
+    // The bulk class runs on the main stream while the wide classes run on the
+    // side stream, so a few long wide-band warps do not serialise behind it.
+    cudaEvent_t ev[2 * kSwClasses + 1];
+    for (auto& e : ev) DRG_CUDA(cudaEventCreate(&e));
+    const int fork = 2 * kSwClasses;
+    DRG_CUDA(cudaEventRecord(ev[fork], c->stream));
+    DRG_CUDA(cudaStreamWaitEvent(c->side, ev[fork], 0));
+    for (int cls = 0; cls < kSwClasses; ++cls) {
+      cudaStream_t sc = cls == 0 ? c->stream : c->side;
+      sa.task_lo = lo[cls];
+      sa.task_hi = hi[cls];
+      DRG_CUDA(cudaEventRecord(ev[2 * cls], sc));
+      if (hi[cls] > lo[cls]) {
+        launch_sw_class(sa, cls, trace, sc);
+        if (!trace) st.sw_launches += 1;
+      }
+      DRG_CUDA(cudaEventRecord(ev[2 * cls + 1], sc));
+    }
+    const int side_end = 2 * kSwClasses - 1;
+    DRG_CUDA(cudaStreamWaitEvent(c->stream, ev[side_end], 0));
+    DRG_CUDA(cudaEventSynchronize(ev[1]));
+    DRG_CUDA(cudaEventSynchronize(ev[side_end]));
+    float cls_ms[kSwClasses], side_span = 0;
+    for (int k = 0; k < kSwClasses; ++k) DRG_CUDA(cudaEventElapsedTime(&cls_ms[k], ev[2 * k], ev[2 * k + 1]));
+    DRG_CUDA(cudaEventElapsedTime(&side_span, ev[fork], ev[side_end]));
+    for (auto& e : ev) cudaEventDestroy(e);
+    const double kms = cls_ms[0] > side_span ? cls_ms[0] : side_span;  // wall of the concurrent launches
+    if (!trace) {
+      st.ms_sw_kernel += kms;
+      for (int k = 0; k < kSwClasses; ++k) {
+        st.ms_sw_class[k] += cls_ms[k];
+        st.sw_class_tasks[k] += hi[k] - lo[k];
+        if (hmax[k] > st.sw_class_max_steps[k]) st.sw_class_max_steps[k] = hmax[k];
+      }
+    } else {
+      st.ms_trace_kernel += kms;
+    }
+    if (trace) {
+      SwWalkArgs wa{};
+      wa.bands = bc;
+      wa.tband = tb;
+      wa.n_bands = n_bands;
+      wa.trace = sa.trace;
+      wa.q_letters = qs.letters;
+      wa.q_offsets = qs.offsets;
+      wa.s_letters = s.letters;
+      wa.s_offsets = s.offsets;
+      wa.ops_off = d_ops_off;
+      wa.rev = c->rev.as<uint8_t>((*h_ops_off)[n_bands] + 16);
+      wa.ops = ops;
+      wa.out = out;
+      std::memcpy(wa.scores625, scr.scores, 625);
+      launch_sw_walk(wa, c->stream);
+    }
   }
-  // exact scores for the bands the packed kernel did not settle
+  // the exact kernel for the bands the packed kernel did not settle
   count_launch();
-  k_exact_flags<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(swks, swos, n_fast, n_bands, scores, flags);
+  k_exact_flags<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(swos, n_fast, n_bands, scores, tb, flags);
   uint32_t* ex_pos = c->sel_idx.as<uint32_t>(n_bands + 1);
   const uint64_t n_ex = select_indices(c, flags, n_bands, ex_pos, d_count);
+  st.exact_bands += n_ex;
   if (n_ex > 0) {
     uint32_t* ex_idx = c->idx.as<uint32_t>(n_ex);
-    Band* ex_b = c->sel_bands.as<Band>(n_ex);
+    Band* ex_b = c->ex_bands.as<Band>(n_ex);
     count_launch();
     k_gather_positions<<<ceil_div(n_ex, 256), 256, 0, c->stream>>>(ex_pos, swos, n_ex, bc, ex_idx, ex_b);
     std::vector<uint32_t> bidx;
@@ -285,16 +455,18 @@ void score_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs
       j.d0 = b.d0;
       j.d1 = b.d1;
       j.scratch_off = soff;
-      j.ops_off = 0;
-      soff += exact_scratch_bytes(j.n, j.m, j.d0, j.d1, false);
+      j.ops_off = trace ? (*h_ops_off)[bidx[k]] : 0;
+      soff += exact_scratch_bytes(j.n, j.m, j.d0, j.d1, trace);
     }
     ExactJob* dj = c->exact_jobs.as<ExactJob>(n_ex);
     ExactOut* dout = c->exact_out.as<ExactOut>(n_ex);
     uint8_t* scratch = c->exact_scratch.as<uint8_t>(soff);
     DRG_CUDA(cudaMemcpyAsync(dj, jobs.data(), n_ex * sizeof(ExactJob), cudaMemcpyHostToDevice, c->stream));
-    launch_sw_exact(dj, n_ex, scr.gap_open, scr.gap_extend, false, scratch, nullptr, dout, c->stream);
+    launch_sw_exact_with_matrix(dj, n_ex, scr.gap_open, scr.gap_extend, trace, scratch, trace ? ops : nullptr, dout,
+                                scr.scores, c->stream);
     count_launch();
-    k_scatter_scores<<<ceil_div(n_ex, 256), 256, 0, c->stream>>>(ex_idx, dout, n_ex, scores);
+    if (trace) k_scatter_exact<<<ceil_div(n_ex, 256), 256, 0, c->stream>>>(ex_idx, dout, n_ex, out);
+    else k_scatter_scores<<<ceil_div(n_ex, 256), 256, 0, c->stream>>>(ex_idx, dout, n_ex, scores);
     DRG_CUDA(cudaGetLastError());
   }
 }
@@ -548,7 +720,9 @@ void Search::chunk(uint64_t chunk_id, uint64_t c0, uint64_t c1, uint64_t n_runs)
   int32_t* scores = c->scores.as<int32_t>(n_bands);
   DevSeqs qs{q->letters, q->offsets, &q->h_offsets};
   DevSeqs ss{db->letters, db->offsets, &db->h_offsets};
-  score_bands(c, bc, n_bands, qs, ss, sc, scores, st, d_count, d_counters + 3);
+  int32_t* best_row = c->best_row.as<int32_t>(n_bands);
+  run_bands(c, bc, n_bands, qs, ss, sc, false, scores, best_row, nullptr, nullptr, nullptr, nullptr, st, d_count,
+            d_counters + 3);
   st.ms_sw += tm.stop();
   flags = c->flags.as<uint8_t>(n_bands + 1);  // scratch buffers may have been regrown
   // ---- E-value gate and band walk
@@ -580,7 +754,8 @@ void Search::chunk(uint64_t chunk_id, uint64_t c0, uint64_t c1, uint64_t n_runs)
     int32_t* gs = reinterpret_cast<int32_t*>(c->exact_out.as<uint8_t>(n_sel * 5 + 16));
     uint8_t* gst = reinterpret_cast<uint8_t*>(gs + n_sel);
     count_launch();
-    k_gather_bands<<<ceil_div(n_sel, 256), 256, 0, c->stream>>>(sel, n_sel, bc, scores, state, gb, gs, gst);
+    k_gather_bands<<<ceil_div(n_sel, 256), 256, 0, c->stream>>>(sel, n_sel, bc, scores, best_row, state, gb, gs,
+                                                                  gst);
     std::vector<Band> hb;
     std::vector<int32_t> hs_;
     std::vector<uint8_t> hst;
@@ -673,21 +848,12 @@ void Search::finish(drg_result* out) {
   for (uint64_t t = 0; t < q->n; ++t)
     for (size_t k : final_lists[t]) order.push_back(k);
   const uint64_t nj = order.size();
-  std::vector<ExactJob> jobs(nj);
-  uint64_t soff = 0, ooff = 0;
+  std::vector<Band> sb(nj);
+  std::vector<uint64_t> ops_off(nj + 1, 0);
   for (uint64_t k = 0; k < nj; ++k) {
-    const Band& b = kept[order[k]].band;
-    ExactJob& j = jobs[k];
-    j.q = q->letters + q->h_offsets[b.target] + b.q0;
-    j.s = db->letters + db->h_offsets[b.subject];
-    j.n = b.n;
-    j.m = (uint32_t)(db->h_offsets[b.subject + 1] - db->h_offsets[b.subject]);
-    j.d0 = b.d0;
-    j.d1 = b.d1;
-    j.scratch_off = soff;
-    j.ops_off = ooff;
-    soff += exact_scratch_bytes(j.n, j.m, j.d0, j.d1, true);
-    ooff += (uint64_t)j.n + j.m;
+    sb[k] = kept[order[k]].band;
+    const uint64_t m = db->h_offsets[sb[k].subject + 1] - db->h_offsets[sb[k].subject];
+    ops_off[k + 1] = ops_off[k] + sb[k].n + m;
   }
   st.ms_host += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   std::vector<ExactOut> eo;
@@ -695,14 +861,18 @@ void Search::finish(drg_result* out) {
   if (nj > 0) {
     Timer tm(c);
     tm.start();
-    ExactJob* dj = c->exact_jobs.as<ExactJob>(nj);
-    ExactOut* dout = c->exact_out.as<ExactOut>(nj);
-    uint8_t* scr = c->exact_scratch.as<uint8_t>(soff);
-    uint32_t* dops = c->exact_ops.as<uint32_t>(ooff);
-    DRG_CUDA(cudaMemcpyAsync(dj, jobs.data(), nj * sizeof(ExactJob), cudaMemcpyHostToDevice, c->stream));
-    launch_sw_exact(dj, nj, sc.gap_open, sc.gap_extend, true, scr, dops, dout, c->stream);
+    Band* db_ = c->sel_bands.as<Band>(nj);
+    uint64_t* doff = c->ops_off.as<uint64_t>(nj + 1);
+    ExactOut* dout = c->trace_out.as<ExactOut>(nj);
+    uint32_t* dops = c->exact_ops.as<uint32_t>(ops_off[nj] + 1);
+    DRG_CUDA(cudaMemcpyAsync(db_, sb.data(), nj * sizeof(Band), cudaMemcpyHostToDevice, c->stream));
+    DRG_CUDA(cudaMemcpyAsync(doff, ops_off.data(), (nj + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
+    DevSeqs qs{q->letters, q->offsets, &q->h_offsets};
+    DevSeqs ss{db->letters, db->offsets, &db->h_offsets};
+    run_bands(c, db_, nj, qs, ss, sc, true, nullptr, nullptr, dout, dops, doff, &ops_off, st, d_count,
+              d_counters + 4);
     fetch_n(c, eo, dout, nj);
-    fetch_n(c, ops_all, dops, ooff);
+    fetch_n(c, ops_all, dops, ops_off[nj]);
     st.ms_trace += tm.stop();
   }
   auto t1 = std::chrono::steady_clock::now();
@@ -743,7 +913,7 @@ void Search::finish(drg_result* out) {
       o.ops_offset = ko;
       o.n_ops = r.n_ops;
       o.pad = 0;
-      std::memcpy(out->ops + ko, ops_all.data() + jobs[k].ops_off, r.n_ops * sizeof(uint32_t));
+      std::memcpy(out->ops + ko, ops_all.data() + ops_off[k], r.n_ops * sizeof(uint32_t));
       ko += r.n_ops;
     }
     out->target_offsets[t + 1] = h;

@@ -12,16 +12,23 @@ __global__ void k_probe(uint32_t seed, uint32_t* sink, long long* cycles) {
 #pragma unroll
   for (int k = 0; k < kChains; ++k) a[k] = seed * (threadIdx.x + 1) + k * 0x9E37u;
   long long t0 = clock64();
+  unsigned long long g0;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(g0));
   for (int it = 0; it < kIters; ++it) {
 #pragma unroll
     for (int k = 0; k < kChains; ++k) a[k] = __viaddmax_s16x2(a[k], a[(k + 1) & (kChains - 1)], seed + k);
   }
   long long t1 = clock64();
+  unsigned long long g1;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(g1));
   uint32_t s = 0;
 #pragma unroll
   for (int k = 0; k < kChains; ++k) s ^= a[k];
   if (s == 0x2468ACE1u) sink[0] = s;
-  if (blockIdx.x == 0 && threadIdx.x == 0) cycles[0] = t1 - t0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    cycles[0] = t1 - t0;
+    cycles[1] = (long long)(g1 - g0);  // nanoseconds
+  }
 }
 }  // namespace
 
@@ -48,11 +55,11 @@ void run_int_probe(double* lane_ops_per_s, double* mhz, cudaStream_t st) {
   DRG_CUDA(cudaEventSynchronize(e1));
   float ms = 0;
   DRG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-  long long c = 0;
-  DRG_CUDA(cudaMemcpy(&c, cyc, 8, cudaMemcpyDeviceToHost));
+  long long c[2] = {0, 0};
+  DRG_CUDA(cudaMemcpy(c, cyc, 16, cudaMemcpyDeviceToHost));
   double ops = (double)kIters * kChains * threads * (double)blocks * reps;
   *lane_ops_per_s = ops / (ms * 1e-3);
-  *mhz = (double)c / ((ms / reps) * 1e3);
+  *mhz = c[1] > 0 ? (double)c[0] / ((double)c[1] * 1e-3) : 0.0;  // cycles per microsecond
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   cudaFree(sink);

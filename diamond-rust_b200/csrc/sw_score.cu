@@ -1,28 +1,37 @@
-// Banded affine Smith-Waterman, score only (gapped.rs:67-203), for bands of
-// equal width W that share a query window.
+// Banded affine Smith-Waterman (gapped.rs:67-280) for many bands that share a
+// query window: the score pass of the E-value gate and the traceback of the
+// HSPs that survive it.
 //
 // Mapping (inter-task): one thread = one band; one warp = up to 32 bands of
-// the same query window, so the query profile is shared per warp.  The band is
-// swept in strips of 16 DP rows.  Inside a strip, relative column c covers
-// absolute subject column j = i0 - d1 + c, and row r of the strip is in the
-// band for r <= c <= r + W - 1.  The 16 rows are held as 8 pairs of signed
-// 16-bit lanes (DPX s16x2 instructions): pair p holds row p at column c in
-// its low half and row p + 8 at column c - 1 in its high half.  With that
+// the same query window and width W, so the query profile is shared per warp.
+// The band is swept in strips of 16 DP rows.  Inside a strip, relative column
+// c covers absolute subject column j = i0 - d1 + c, and row r of the strip is
+// in the band for r <= c <= r + W - 1.  The 16 rows are held as 8 pairs of
+// signed 16-bit lanes (DPX s16x2 instructions): pair p holds row p at column c
+// in its low half and row p + 8 at column c - 1 in its high half.  With that
 // one-column skew every dependency of a pair is already computed:
-//   D(i,j) = H(i-1,j-1) + S     previous step of the pair above
-//   E(i,j) = max(E(i-1,j) - ge, H(i-1,j) - oc)    this step, pair above
-//   F(i,j) = max(F(i,j-1) - ge, H(i,j-1) - oc)    previous step, same pair
+//   D(i,j) = H(i-1,j-1) + S                        previous step, pair above
+//   E(i,j) = max(E(i-1,j) - ge, H(i-1,j) - oc)      this step, pair above
+//   F(i,j) = max(F(i,j-1) - ge, H(i,j-1) - oc)      previous step, same pair
 //   H      = max(0, D, E, F)
 // Row 8's "pair above" is row 7, taken from the previous step; row 0's is the
-// previous strip's last row, kept in a per-thread ring in shared memory.
+// previous strip's last row, kept in a per-thread ring in shared memory.  The
+// ring holds W + 1 words (H | E << 16): a strip reads the previous strip's
+// word for column c and then overwrites the slot of column c - 1, which is
+// the word the next strip needs at its column c - 17.
 //
 // Exactness: values equal the reference's int32 DP while the band's best is
-// below 2^15 (bands that could exceed it go to the exact kernel).  Cells with
-// j < 0, j > m or rows past the query read a sentinel residue scoring -64;
-// they can neither raise the maximum above the true band maximum (when that is
-// >= 12; smaller results are recomputed exactly) nor feed an in-band cell.
-// Cells left or right of the band in the first/last 16 steps of a strip are
-// masked: their H does not count and they pass -inf-like E/F to the band.
+// below 2^15 (bands that could exceed it are not given to this kernel).
+// Cells with j < 0, j > m or rows past the query read a sentinel residue
+// scoring -64; they can neither raise the maximum above the true band maximum
+// (when that is >= 12; smaller results are recomputed exactly) nor feed an
+// in-band cell.  Cells left or right of the band in the first/last 16 steps of
+// a strip are masked: their H does not count and they pass -inf-like E/F.
+//
+// Trace mode also writes, per cell, the reference's trace nibble
+// (choice | e_ext << 2 | f_ext << 3, gapped.rs:171-188) into a lane-interleaved
+// buffer and tracks the first row-major maximum; a walk kernel then follows
+// the reference's traceback (gapped.rs:205-279) through those nibbles.
 #include "kernels.h"
 
 namespace drg {
@@ -34,7 +43,6 @@ constexpr int kPairs = kRows / 2;  // s16x2 pairs
 constexpr int kProfStride = 24;    // bytes per residue row of the strip profile
 constexpr int kProfBytes = 26 * kProfStride;
 constexpr uint32_t kNeg2 = 0xC000C000u;  // (-16384, -16384)
-constexpr int kWarpsPerBlock = 4;
 
 __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
   uint32_t r;
@@ -51,6 +59,11 @@ __device__ __forceinline__ uint32_t max2(uint32_t a, uint32_t b) {
   asm("max.s16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
   return r;
 }
+__device__ __forceinline__ uint32_t max2_relu(uint32_t a, uint32_t b) {
+  uint32_t r;
+  asm("max.s16x2.relu %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+  return r;
+}
 // keep halves selected by k (0xFFFF per kept half), replace the others with v
 __device__ __forceinline__ uint32_t sel2(uint32_t x, uint32_t k, uint32_t v) { return (x & k) | (v & ~k); }
 
@@ -65,44 +78,72 @@ struct Lane {
   int jbase;         // absolute column of relative column 0 in this strip
 };
 
+template <bool TR>
 struct Regs {
   uint32_t H[kPairs], Hm[kPairs], F[kPairs];
-  uint32_t E7;       // E of pair 7 at the previous step
-  uint32_t htop_old; // top H of the previous step (D operand of pair 0)
-  uint32_t best;
-  uint32_t res_prev; // subject residue of the previous column
+  uint32_t E7;        // E of pair 7 at the previous step
+  uint32_t htop_old;  // top H of the previous step (D operand of pair 0)
+  uint32_t res_prev;  // subject residue of the previous column
+  uint32_t rowmax[kPairs];            // per row of the strip: max H so far
+  uint32_t rowcol[TR ? kPairs : 1];   // trace mode: first column of that max
 };
 
 // One column step.  MODE 0: middle (all rows in band), 1: prologue step
-// C (= c), 2: epilogue step C (= c - W).  Masks are compile-time constants.
-template <int MODE, int C>
-__device__ __forceinline__ void sw_step(Regs& R, const Lane& L, int c, const uint8_t* __restrict__ prof,
+// C (= c), 2: epilogue step C (= c - W) of a warp whose bands share one
+// width, 3: step past the narrowest band of a warp with mixed widths
+// (cw = c - this lane's W, masks computed at run time).
+template <int MODE, int C, bool TR>
+__device__ __forceinline__ void sw_step(Regs<TR>& R, const Lane& L, int c, const uint8_t* __restrict__ prof,
                                         uint32_t* __restrict__ ring_r, uint32_t* __restrict__ ring_w, uint32_t noc2,
-                                        uint32_t nge2) {
+                                        uint32_t nge2, uint2* __restrict__ trace, int cw = 0) {
   const int jm1 = L.jbase + c - 1;  // subject index j - 1 of this column
   const uint32_t res = ((unsigned)jm1 < (unsigned)L.m) ? (uint32_t)__ldg(L.s + jm1) : 25u;
   const uint2 lo8 = *reinterpret_cast<const uint2*>(prof + res * kProfStride);
   const uint2 hi8 = *reinterpret_cast<const uint2*>(prof + R.res_prev * kProfStride + 8);
   R.res_prev = res;
-  const uint32_t rw = *ring_r;                      // (H, E) of the row above row 0, column c
+  const uint32_t rw = *ring_r;  // (H, E) of the row above row 0, column c
   const uint32_t htop = prmt(rw, R.H[kPairs - 1], 0x5410);
   uint32_t e_up = prmt(rw, R.E7, 0x5432);
   uint32_t hm_up = add2(htop, noc2);
   uint32_t hd = R.htop_old;
+  uint32_t tr_lo = 0, tr_hi = 0;
+  const uint32_t colpair = TR ? ((uint32_t)c | ((uint32_t)(c - 1) << 16)) : 0u;
 #pragma unroll
   for (int p = 0; p < kPairs; ++p) {
     const uint32_t sc = prmt(p < 4 ? lo8.x : lo8.y, p < 4 ? hi8.x : hi8.y, pick_sel(p & 3));
     const uint32_t d = add2(hd, sc);
-    uint32_t e = __viaddmax_s16x2(e_up, nge2, hm_up);
-    uint32_t f = __viaddmax_s16x2(R.F[p], nge2, R.Hm[p]);
-    uint32_t h = __vimax3_s16x2_relu(d, e, f);
+    uint32_t e, f, h;
+    if (!TR) {
+      e = __viaddmax_s16x2(e_up, nge2, hm_up);
+      f = __viaddmax_s16x2(R.F[p], nge2, R.Hm[p]);
+      h = __vimax3_s16x2_relu(d, e, f);
+    } else {
+      const uint32_t te = add2(e_up, nge2);
+      const uint32_t tf = add2(R.F[p], nge2);
+      e = max2(te, hm_up);
+      f = max2(tf, R.Hm[p]);
+      const uint32_t m1 = max2_relu(d, 0u);
+      const uint32_t ce = __vcmpgts2(e, m1);
+      const uint32_t m2 = max2(e, m1);
+      const uint32_t cf = __vcmpgts2(f, m2);
+      h = max2(f, m2);
+      const uint32_t cd = __vcmpgts2(d, 0u);
+      const uint32_t ee = __vcmpgts2(te, hm_up);
+      const uint32_t fe = __vcmpgts2(tf, R.Hm[p]);
+      // nibble per half: choice (bit0, bit1), e_ext (bit2), f_ext (bit3)
+      uint32_t bits = ((cf | (cd & ~ce)) & 0x00010001u) | ((cf | ce) & 0x00020002u) | (ee & 0x00040004u) |
+                      (fe & 0x00080008u);
+      const uint32_t byte = (bits & 0xFu) | ((bits >> 12) & 0xF0u);  // low row in the low nibble
+      if (p < 4) tr_lo |= byte << (8 * (p & 3));
+      else tr_hi |= byte << (8 * (p & 3));
+    }
     if (MODE == 1) {
       // left of the band: row p at column C (low), row p+8 at column C-1 (high)
       const bool lo_left = C < p;
       const bool hi_left = C <= p + 8;
       const uint32_t k = (lo_left ? 0u : 0x0000FFFFu) | (hi_left ? 0u : 0xFFFF0000u);
       if (k != 0xFFFFFFFFu) {
-        h = h & k;            // no score, H - oc = -oc toward the entry cell
+        h = h & k;  // no score; H - oc = -oc toward the entry cell
         f = sel2(f, k, kNeg2);
       }
     } else if (MODE == 2) {
@@ -113,9 +154,20 @@ __device__ __forceinline__ void sw_step(Regs& R, const Lane& L, int c, const uin
         h = h & k;
         e = sel2(e, k, kNeg2);
       }
+    } else if (MODE == 3) {
+      // right of this lane's band: row p at column c (low), row p+8 at column c-1 (high)
+      const uint32_t k = (cw >= p ? 0u : 0x0000FFFFu) | (cw >= p + 9 ? 0u : 0xFFFF0000u);
+      h = h & k;
+      e = sel2(e, k, kNeg2);
     }
     const uint32_t hm = add2(h, noc2);
-    R.best = max2(R.best, h);
+    if (!TR) {
+      R.rowmax[p] = max2(R.rowmax[p], h);
+    } else {
+      const uint32_t gt = __vcmpgts2(h, R.rowmax[p]);
+      R.rowmax[p] = max2(R.rowmax[p], h);
+      R.rowcol[p] = (R.rowcol[p] & ~gt) | (colpair & gt);
+    }
     hd = R.H[p];
     R.H[p] = h;
     R.Hm[p] = hm;
@@ -126,41 +178,50 @@ __device__ __forceinline__ void sw_step(Regs& R, const Lane& L, int c, const uin
   R.E7 = e_up;
   *ring_w = prmt(R.H[kPairs - 1], R.E7, 0x7632);  // (H, E) of row 15 at column c - 1
   R.htop_old = htop;
+  if (TR) *trace = make_uint2(tr_lo, tr_hi);
 }
 
-template <int MODE, int C>
+template <int MODE, int C, bool TR>
 struct Unroll {
-  static __device__ __forceinline__ void run(Regs& R, const Lane& L, int c0, const uint8_t* prof, uint32_t* ring,
-                                             int buf, int stride, int& slot, uint32_t noc2, uint32_t nge2) {
+  static __device__ __forceinline__ void run(Regs<TR>& R, const Lane& L, int c0, const uint8_t* prof, uint32_t* ring,
+                                             int buf, int stride, int& slot, uint32_t noc2, uint32_t nge2,
+                                             uint2* trace) {
     int wslot = slot == 0 ? buf - 1 : slot - 1;
-    sw_step<MODE, C>(R, L, c0 + C, prof, ring + slot * stride, ring + wslot * stride, noc2, nge2);
+    sw_step<MODE, C, TR>(R, L, c0 + C, prof, ring + slot * stride, ring + wslot * stride, noc2, nge2,
+                         TR ? trace + (c0 + C) * 32 : nullptr);
     slot = slot + 1 == buf ? 0 : slot + 1;
-    Unroll<MODE, C + 1>::run(R, L, c0, prof, ring, buf, stride, slot, noc2, nge2);
+    Unroll<MODE, C + 1, TR>::run(R, L, c0, prof, ring, buf, stride, slot, noc2, nge2, trace);
   }
 };
-template <int MODE>
-struct Unroll<MODE, kRows> {
-  static __device__ __forceinline__ void run(Regs&, const Lane&, int, const uint8_t*, uint32_t*, int, int, int&,
-                                             uint32_t, uint32_t) {}
+template <int MODE, bool TR>
+struct Unroll<MODE, kRows, TR> {
+  static __device__ __forceinline__ void run(Regs<TR>&, const Lane&, int, const uint8_t*, uint32_t*, int, int, int&,
+                                             uint32_t, uint32_t, uint2*) {}
 };
 
-__global__ void __launch_bounds__(kWarpsPerBlock * 32) k_sw_score(SwScoreArgs a) {
+__device__ __forceinline__ int lo16(uint32_t x) { return (int)(int16_t)(x & 0xFFFFu); }
+__device__ __forceinline__ int hi16(uint32_t x) { return (int)(int16_t)(x >> 16); }
+
+template <int WARPS, bool TR>
+__global__ void __launch_bounds__(WARPS * 32) k_sw(SwScoreArgs a) {
   extern __shared__ __align__(16) uint8_t smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint64_t task_id = (uint64_t)blockIdx.x * kWarpsPerBlock + warp;
-  const int stride = blockDim.x;
-  int8_t* mat = reinterpret_cast<int8_t*>(smem);                        // 25 x 25 scores
-  uint8_t* prof = smem + 640 + warp * kProfBytes;                        // strip profile
-  uint32_t* ring = reinterpret_cast<uint32_t*>(smem + 640 + kWarpsPerBlock * kProfBytes) + threadIdx.x;
+  const uint64_t task_id = a.task_lo + (uint64_t)blockIdx.x * WARPS + warp;
+  const int stride = WARPS * 32;
+  int8_t* mat = reinterpret_cast<int8_t*>(smem);  // 25 x 25 scores
+  uint8_t* prof = smem + 640 + warp * kProfBytes;  // strip profile
+  uint32_t* ring = reinterpret_cast<uint32_t*>(smem + 640 + WARPS * kProfBytes) + threadIdx.x;
   for (int i = threadIdx.x; i < 625; i += blockDim.x) mat[i] = a.scores625[i];
   __syncthreads();
-  if (task_id >= a.n_tasks) return;
+  if (task_id >= a.task_hi) return;
   const SwTask task = a.tasks[task_id];
-  const int W = (int)task.width;
-  const int buf = W + kRows + 1;
+  const int W = (int)task.width;   // widest band of the warp
+  const int Wmin = (int)task.w_min;
+  const int buf = W + 1;
   const bool active = lane < (int)task.count;
   const uint32_t bidx = a.order[task.first + (active ? lane : 0)];
   const Band band = a.bands[bidx];
+  const int Wl = band.d1 - band.d0 + 1;  // this lane's width
   const uint8_t* q = a.q_letters + a.q_offsets[band.target] + band.q0;
   const int n = (int)band.n;
   Lane L;
@@ -168,12 +229,14 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_sw_score(SwScoreArgs a)
   L.m = (int)(a.s_offsets[band.subject + 1] - a.s_offsets[band.subject]);
   const uint32_t noc2 = (uint32_t)(uint16_t)(-(a.gap_open + a.gap_extend)) * 0x10001u;
   const uint32_t nge2 = (uint32_t)(uint16_t)(-a.gap_extend) * 0x10001u;
-  // ring: boundary row above the first strip is row 0 of the reference (H = 0)
-  for (int g = 0; g < buf; ++g) ring[g * stride] = 0xC0000000u;  // H = 0, E = -inf
+  // the row above the first strip is row 0 of the reference: H = 0, and its
+  // E is -inf; column Wl - 1 is outside row 0's band on the right.
+  for (int g = 0; g < buf; ++g) ring[g * stride] = 0xC0000000u;
+  ring[(Wl - 1) * stride] = kNeg2;
   int base = 0;  // ring slot of relative column 0 of the current strip
-  ring[(W - 1) * stride] = kNeg2;
-  Regs R;
-  R.best = 0;
+  Regs<TR> R;
+  int best = 0, best_i = 0, best_j = 0;
+  uint2* tr = TR ? a.trace + task.trace_off + lane : nullptr;
   for (uint32_t k = 0; k < task.n_strips; ++k) {
     const int i0 = (int)task.row_first + (int)(k * kRows);
     // strip profile: prof[res * stride + r] = S(q[i0 + r - 1], res)
@@ -193,53 +256,211 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_sw_score(SwScoreArgs a)
       R.H[p] = 0;
       R.Hm[p] = kNeg2;
       R.F[p] = kNeg2;
+      R.rowmax[p] = 0;
+      if (TR) R.rowcol[p] = 0;
     }
     R.E7 = kNeg2;
-    int slot_m1 = base == 0 ? buf - 1 : base - 1;
+    const int slot_m1 = base == 0 ? buf - 1 : base - 1;
     R.htop_old = ring[slot_m1 * stride] & 0xFFFFu;
-    R.res_prev = 25u;
     {
       const int jm1 = L.jbase - 2;  // column -1
       R.res_prev = ((unsigned)jm1 < (unsigned)L.m) ? (uint32_t)L.s[jm1] : 25u;
     }
+    uint2* trs = TR ? tr + (uint64_t)k * (W + kRows) * 32 : nullptr;
     int slot = base;
-    Unroll<1, 0>::run(R, L, 0, prof, ring, buf, stride, slot, noc2, nge2);
-    for (int c = kRows; c < W; ++c) {
-      int wslot = slot == 0 ? buf - 1 : slot - 1;
-      sw_step<0, 0>(R, L, c, prof, ring + slot * stride, ring + wslot * stride, noc2, nge2);
+    Unroll<1, 0, TR>::run(R, L, 0, prof, ring, buf, stride, slot, noc2, nge2, trs);
+    for (int c = kRows; c < Wmin; ++c) {
+      const int wslot = slot == 0 ? buf - 1 : slot - 1;
+      sw_step<0, 0, TR>(R, L, c, prof, ring + slot * stride, ring + wslot * stride, noc2, nge2,
+                        TR ? trs + c * 32 : nullptr);
       slot = slot + 1 == buf ? 0 : slot + 1;
     }
-    Unroll<2, 0>::run(R, L, W, prof, ring, buf, stride, slot, noc2, nge2);
-    // slot now indexes column W + 16 - 1 + 1; column W + 15 of this strip is the
-    // next strip's column W - 1: its E/H must read as outside the band.
-    int last = slot == 0 ? buf - 1 : slot - 1;
-    ring[last * stride] = kNeg2;
+    if (Wmin == W) {  // one width in the warp: compile-time masks
+      Unroll<2, 0, TR>::run(R, L, W, prof, ring, buf, stride, slot, noc2, nge2, trs);
+    } else {          // mixed widths: each lane masks past its own right edge
+      for (int c = Wmin; c < W + kRows; ++c) {
+        const int wslot = slot == 0 ? buf - 1 : slot - 1;
+        sw_step<3, 0, TR>(R, L, c, prof, ring + slot * stride, ring + wslot * stride, noc2, nge2,
+                          TR ? trs + c * 32 : nullptr, c - Wl);
+        slot = slot + 1 == buf ? 0 : slot + 1;
+      }
+    }
+    // this lane's column Wl + 15 is the next strip's column Wl - 1: outside
+    // the band on the right, its E/H must read as -inf.
+    {
+      int ls = base + Wl + kRows - 1;
+      ls = ls >= buf ? ls - buf : ls;
+      ls = ls >= buf ? ls - buf : ls;
+      ring[ls * stride] = kNeg2;
+    }
     base += kRows;
     if (base >= buf) base -= buf;
+    // first row-major maximum: rows in order, strictly greater wins
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) {
+      const int v = r < kPairs ? lo16(R.rowmax[r]) : hi16(R.rowmax[r - kPairs]);
+      if (v > best) {
+        best = v;
+        best_i = i0 + r;
+        if (TR) best_j = L.jbase + (r < kPairs ? lo16(R.rowcol[r]) : hi16(R.rowcol[r - kPairs]));
+      }
+    }
   }
-  if (active) {
-    int lo = (int)(int16_t)(R.best & 0xFFFFu), hi = (int)(int16_t)(R.best >> 16);
-    a.score[bidx] = lo > hi ? lo : hi;
+  if (!active) return;
+  if (!TR) {
+    a.score[bidx] = best;
+    if (a.best_row) a.best_row[bidx] = best_i;
+  } else {
+    TraceBand t;
+    t.trace_off = task.trace_off + lane;
+    t.row_first = task.row_first;
+    t.width = (uint32_t)W;
+    t.score = best;
+    t.best_i = best_i;
+    t.best_j = best_j;
+    t.pad = 0;
+    a.tband[bidx] = t;
   }
+}
+
+// Traceback of one band through the nibbles of the trace pass, in the
+// reference's order and with its stopping rules (gapped.rs:205-279).
+__global__ void k_sw_walk(SwWalkArgs a) {
+  const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (t >= a.n_bands) return;
+  const Band b = a.bands[t];
+  const TraceBand tb = a.tband[t];
+  ExactOut R;
+  R.score = 0;
+  R.q_begin = R.q_end = R.s_begin = R.s_end = 0;
+  R.identities = R.positives = R.mismatches = R.gap_openings = R.gaps = R.length = 0;
+  R.n_ops = 0;
+  R.cells = 0;
+  if (tb.score < 12) return;  // not traced here: the exact kernel writes this band
+  const uint8_t* q = a.q_letters + a.q_offsets[b.target] + b.q0;
+  const uint8_t* s = a.s_letters + a.s_offsets[b.subject];
+  const int64_t m = (int64_t)(a.s_offsets[b.subject + 1] - a.s_offsets[b.subject]);
+  const int64_t d0 = b.d0, d1 = b.d1, W = tb.width, rf = tb.row_first;
+  if (tb.best_i < 1 || tb.best_i > (int64_t)b.n || tb.best_j < 1 || tb.best_j > m) {
+    R.score = -1;  // cannot happen for a best >= 12; reported to the host as an internal error
+    a.out[t] = R;
+    return;
+  }
+  R.score = tb.score;
+  R.q_end = (uint32_t)tb.best_i;
+  R.s_end = (uint32_t)tb.best_j;
+  uint8_t* rev = a.rev + a.ops_off[t];
+  uint32_t nrev = 0;
+  int state = 0;
+  int64_t i = tb.best_i, j = tb.best_j;
+  bool in_gap = false;
+  while (i > 0 && j > 0) {
+    int64_t lo = i - d1, hi = i - d0;
+    lo = lo < 0 ? 0 : (lo > m ? m : lo);
+    hi = hi < 0 ? 0 : (hi > m ? m : hi);
+    if (j < lo || j > hi || i < rf) break;
+    const int64_t k = (i - rf) >> 4, r = (i - rf) & 15;
+    const int64_t c = j - (rf + 16 * k - d1);
+    const int64_t it = c + (r >= 8 ? 1 : 0);
+    const uint2 w = a.trace[tb.trace_off + (uint64_t)(k * (W + 16) + it) * 32];
+    const uint32_t p = (uint32_t)(r & 7);
+    const uint32_t byte = ((p < 4 ? w.x : w.y) >> (8 * (p & 3))) & 0xFFu;
+    const uint32_t nib = r >= 8 ? byte >> 4 : byte & 0xFu;
+    if (state == 0) {
+      const uint32_t ch = nib & 3;
+      if (ch == 0) break;
+      if (ch == 1) {
+        const uint32_t x = q[i - 1], y = s[j - 1];
+        R.length++;
+        if (x == y) R.identities++;
+        else R.mismatches++;
+        if (a.scores625[(x < 24 ? x : 24) * 25 + (y < 24 ? y : 24)] > 0) R.positives++;
+        rev[nrev++] = 0;
+        in_gap = false;
+        --i;
+        --j;
+      } else {
+        state = ch == 2 ? 1 : 2;
+      }
+    } else if (state == 1) {
+      R.length++;
+      R.gaps++;
+      if (!in_gap) {
+        R.gap_openings++;
+        in_gap = true;
+      }
+      rev[nrev++] = 1;
+      if (((nib >> 2) & 1) == 0) state = 0;
+      --i;
+    } else {
+      R.length++;
+      R.gaps++;
+      if (!in_gap) {
+        R.gap_openings++;
+        in_gap = true;
+      }
+      rev[nrev++] = 2;
+      if (((nib >> 3) & 1) == 0) state = 0;
+      --j;
+    }
+  }
+  R.q_begin = (uint32_t)i;
+  R.s_begin = (uint32_t)j;
+  uint32_t* o = a.ops + a.ops_off[t];
+  uint32_t nops = 0;
+  int64_t x = (int64_t)nrev - 1;
+  while (x >= 0) {
+    const uint32_t op = rev[x];
+    uint32_t cnt = 0;
+    while (x >= 0 && rev[x] == op) {
+      ++cnt;
+      --x;
+    }
+    o[nops++] = (cnt << 2) | op;
+  }
+  R.n_ops = nops;
+  a.out[t] = R;
+}
+
+template <int WARPS, bool TR>
+void launch_class(const SwScoreArgs& a, int max_width, cudaStream_t st) {
+  if (a.task_hi <= a.task_lo) return;
+  const int threads = WARPS * 32;
+  const size_t smem = 640 + WARPS * kProfBytes + (size_t)threads * (max_width + 1) * 4;
+  static int configured = 0;  // per template instance
+  if ((int)smem > configured) {
+    DRG_CUDA(cudaFuncSetAttribute(k_sw<WARPS, TR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    configured = (int)smem;
+  }
+  const int blocks = ceil_div((long long)(a.task_hi - a.task_lo), WARPS);
+  count_launch();
+  k_sw<WARPS, TR><<<blocks, threads, smem, st>>>(a);
+  DRG_CUDA(cudaGetLastError());
 }
 
 }  // namespace
 
-size_t launch_sw_score(const SwScoreArgs& a, cudaStream_t st) {
-  if (a.n_tasks == 0) return 0;
-  const int threads = kWarpsPerBlock * 32;
-  const int buf = a.max_width + kRows + 1;
-  size_t smem = 640 + kWarpsPerBlock * kProfBytes + (size_t)threads * buf * 4;
-  static int configured_max = 0;
-  if ((int)smem > configured_max) {
-    DRG_CUDA(cudaFuncSetAttribute(k_sw_score, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    configured_max = (int)smem;
+int sw_width_class(int width) {
+  if (width < kSwMinWidth) return -1;
+  for (int c = 0; c < kSwClasses; ++c)
+    if (width <= kSwClassMax[c]) return c;
+  return -1;
+}
+
+void launch_sw_class(const SwScoreArgs& a, int cls, bool trace, cudaStream_t st) {
+  switch (cls) {
+    case 0: trace ? launch_class<4, true>(a, kSwClassMax[0], st) : launch_class<4, false>(a, kSwClassMax[0], st); break;
+    case 1: trace ? launch_class<2, true>(a, kSwClassMax[1], st) : launch_class<2, false>(a, kSwClassMax[1], st); break;
+    case 2: trace ? launch_class<1, true>(a, kSwClassMax[2], st) : launch_class<1, false>(a, kSwClassMax[2], st); break;
+    default: trace ? launch_class<1, true>(a, kSwClassMax[3], st) : launch_class<1, false>(a, kSwClassMax[3], st); break;
   }
-  int blocks = ceil_div((long long)a.n_tasks, kWarpsPerBlock);
+}
+
+void launch_sw_walk(const SwWalkArgs& a, cudaStream_t st) {
+  if (a.n_bands == 0) return;
   count_launch();
-  k_sw_score<<<blocks, threads, smem, st>>>(a);
+  k_sw_walk<<<ceil_div(a.n_bands, 64), 64, 0, st>>>(a);
   DRG_CUDA(cudaGetLastError());
-  return smem;
 }
 
 }  // namespace drg

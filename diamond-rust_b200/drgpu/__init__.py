@@ -84,10 +84,16 @@ class RunStats(C.Structure):
                [(n, C.c_double) for n in ("ms_total", "ms_seed", "ms_join", "ms_sort", "ms_ungapped", "ms_bands",
                                           "ms_sw", "ms_select", "ms_trace", "ms_host", "ms_h2d", "ms_d2h",
                                           "ms_sw_kernel")] + \
-               [("sw_launches", C.c_uint64), ("kernel_launches", C.c_uint64)]
+               [("sw_launches", C.c_uint64), ("kernel_launches", C.c_uint64), ("exact_bands", C.c_uint64),
+                ("sw_class_tasks", C.c_uint64 * 4), ("sw_class_max_steps", C.c_uint64 * 4),
+                ("ms_sw_class", C.c_double * 4), ("ms_trace_kernel", C.c_double)]
 
     def as_dict(self):
-        return {name: getattr(self, name) for name, _ in self._fields_}
+        d = {}
+        for name, _ in self._fields_:
+            v = getattr(self, name)
+            d[name] = list(v) if isinstance(v, C.Array) else v
+        return d
 
 
 class Result(C.Structure):

@@ -97,6 +97,13 @@ typedef struct {
   double ms_h2d, ms_d2h;
   double ms_sw_kernel;      /* device time of the packed score kernel launches alone */
   uint64_t sw_launches, kernel_launches;
+  uint64_t exact_bands;     /* bands the exact kernel handled (not the packed one) */
+  /* packed score kernel per class of the widest band in a warp
+   * (W <= 136, <= 272, <= 544, <= 1700) */
+  uint64_t sw_class_tasks[4];      /* warps (32 bands each at most) */
+  uint64_t sw_class_max_steps[4];  /* longest warp: strips x (W + 16) column steps */
+  double ms_sw_class[4];           /* device time of each class launch */
+  double ms_trace_kernel;          /* device time of the trace-mode kernel launches */
 } drg_run_stats;
 
 /* search::run result: per-target HSP lists, target_offsets[n_targets+1]. */

@@ -179,6 +179,101 @@ int orc_extend_span(const uint8_t* q, size_t n, const uint8_t* s, size_t m, int6
   return 0;
 }
 
+// ---- small helpers for the reference's unit-test vectors ------------------
+size_t orc_decode(const uint8_t* l, size_t n, char* out, size_t cap) {
+  std::string s = decode(l, n);
+  std::strncpy(out, s.c_str(), cap);
+  return s.size();
+}
+size_t orc_seq_id(const char* header, char* out, size_t cap) {
+  std::string s = seq_id(header);
+  std::strncpy(out, s.c_str(), cap);
+  return s.size();
+}
+// Reduction bucket of a letter and the reduction's size (id 0 murphy10, 1 diamond9, 2 none).
+int orc_bucket(int reduction, uint8_t letter, uint64_t* size) {
+  Reduction r = reduction_by_id(reduction);
+  if (size) *size = r.size;
+  return r.bucket(letter);
+}
+uint64_t orc_reduction_size_for(const char* sens) { return reduction_for_sensitivity(sens).size; }
+double orc_seed_cut_for(const char* sens, int has_cut, double cut) {
+  SearchConfig cfg;
+  cfg.sensitivity = sens;
+  cfg.has_seed_cut = has_cut != 0;
+  cfg.seed_cut = cut;
+  return cfg.seed_cut_for();
+}
+size_t orc_index_chunks_for(const char* sens, long chunks) {
+  SearchConfig cfg;
+  cfg.sensitivity = sens;
+  cfg.index_chunks = chunks;
+  return cfg.index_chunks_for();
+}
+size_t orc_translate_frame(const char* nt, size_t offset, uint8_t* out, size_t cap) {
+  auto v = translate_frame(nt, offset);
+  std::memcpy(out, v.data(), std::min(cap, v.size()));
+  return v.size();
+}
+// Six frames of a nucleotide string, concatenated; lens[6] receives their lengths.
+size_t orc_six_frames(const char* nt, uint8_t* out, size_t cap, uint64_t* lens) {
+  auto f = six_frames(nt);
+  size_t k = 0;
+  for (int i = 0; i < 6; ++i) {
+    lens[i] = f[i].size();
+    for (uint8_t l : f[i])
+      if (k < cap) out[k++] = l;
+  }
+  return k;
+}
+void orc_mask_short_orfs(uint8_t* frame, size_t n, size_t min_len) {
+  std::vector<uint8_t> v(frame, frame + n);
+  mask_short_orfs(v, min_len);
+  std::memcpy(frame, v.data(), n);
+}
+size_t orc_min_orf_len(size_t dna_len, long user) { return min_orf_len(dna_len, user); }
+// Field ids of an --outfmt token list ("6 qseqid ..." split on spaces), or -1 on error.
+int orc_parse_outfmt(const char* tokens, int* fields, int cap) {
+  std::vector<std::string> t;
+  std::string cur;
+  for (const char* p = tokens; *p; ++p) {
+    if (*p == ' ') {
+      if (!cur.empty()) t.push_back(cur);
+      cur.clear();
+    } else {
+      cur += *p;
+    }
+  }
+  if (!cur.empty()) t.push_back(cur);
+  std::vector<int> f;
+  if (!parse_outfmt(t, &f, &g_err)) return -1;
+  for (int i = 0; i < (int)f.size() && i < cap; ++i) fields[i] = f[i];
+  return (int)f.size();
+}
+int orc_q_frame(uint32_t frame) {
+  Hsp h{};
+  h.frame = (uint8_t)frame;
+  return h.q_frame();
+}
+void orc_nt_range(uint32_t frame, uint64_t q_begin, uint64_t q_end, uint64_t dna_len, uint64_t* out2) {
+  Hsp h{};
+  h.frame = (uint8_t)frame;
+  h.q_begin = q_begin;
+  h.q_end = q_end;
+  auto r = h.nt_range(dna_len);
+  out2[0] = r.first;
+  out2[1] = r.second;
+}
+double orc_evalue_blast(const char* matrix, int raw, size_t qlen, uint64_t db) {
+  ScoreMatrix m;
+  if (!get_matrix(matrix, -1, -1, &m)) return -1;
+  return m.evalue_blast(raw, qlen, db);
+}
+int orc_matrix_ok(const char* matrix, int go, int ge) {
+  ScoreMatrix m;
+  return get_matrix(matrix, go, ge, &m) ? 1 : 0;
+}
+
 size_t orc_band_for(size_t len) { return band_for(len); }
 double orc_log_erfc(double x) { return log_erfc(x); }
 

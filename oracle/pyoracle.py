@@ -95,7 +95,123 @@ def lib():
         _lib.orc_encode.restype = C.c_size_t
         _lib.orc_encode.argtypes = [C.c_char_p, C.c_size_t, C.c_char_p]
         _lib.orc_free.argtypes = [C.c_void_p]
+        _lib.orc_decode.restype = C.c_size_t
+        _lib.orc_decode.argtypes = [C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t]
+        _lib.orc_seq_id.restype = C.c_size_t
+        _lib.orc_seq_id.argtypes = [C.c_char_p, C.c_char_p, C.c_size_t]
+        _lib.orc_bucket.argtypes = [C.c_int, C.c_uint8, C.POINTER(C.c_uint64)]
+        _lib.orc_reduction_size_for.restype = C.c_uint64
+        _lib.orc_reduction_size_for.argtypes = [C.c_char_p]
+        _lib.orc_seed_cut_for.restype = C.c_double
+        _lib.orc_seed_cut_for.argtypes = [C.c_char_p, C.c_int, C.c_double]
+        _lib.orc_index_chunks_for.restype = C.c_size_t
+        _lib.orc_index_chunks_for.argtypes = [C.c_char_p, C.c_long]
+        _lib.orc_translate_frame.restype = C.c_size_t
+        _lib.orc_translate_frame.argtypes = [C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t]
+        _lib.orc_six_frames.restype = C.c_size_t
+        _lib.orc_six_frames.argtypes = [C.c_char_p, C.c_char_p, C.c_size_t, C.POINTER(C.c_uint64)]
+        _lib.orc_mask_short_orfs.argtypes = [C.c_char_p, C.c_size_t, C.c_size_t]
+        _lib.orc_min_orf_len.restype = C.c_size_t
+        _lib.orc_min_orf_len.argtypes = [C.c_size_t, C.c_long]
+        _lib.orc_parse_outfmt.argtypes = [C.c_char_p, C.POINTER(C.c_int), C.c_int]
+        _lib.orc_q_frame.argtypes = [C.c_uint32]
+        _lib.orc_nt_range.argtypes = [C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64)]
+        _lib.orc_evalue_blast.restype = C.c_double
+        _lib.orc_evalue_blast.argtypes = [C.c_char_p, C.c_int, C.c_size_t, C.c_uint64]
+        _lib.orc_matrix_ok.argtypes = [C.c_char_p, C.c_int, C.c_int]
     return _lib
+
+
+def decode(letters) -> str:
+    b = C.create_string_buffer(len(letters) + 1)
+    n = lib().orc_decode(_bytes(letters) if len(letters) else b"\0", len(letters), b, len(letters) + 1)
+    return b.raw[:n].decode()
+
+
+def seq_id(header: str) -> str:
+    b = C.create_string_buffer(len(header) + 1)
+    n = lib().orc_seq_id(header.encode(), b, len(header) + 1)
+    return b.raw[:n].decode()
+
+
+REDUCTIONS = {"murphy10": 0, "diamond9": 1, "none": 2}
+
+
+def bucket(reduction: str, letter: int):
+    size = C.c_uint64()
+    b = lib().orc_bucket(REDUCTIONS[reduction], letter, C.byref(size))
+    return b, size.value
+
+
+def reduction_size_for(sens: str) -> int:
+    return lib().orc_reduction_size_for(sens.encode())
+
+
+def seed_cut_for(sens: str, cut=None) -> float:
+    return lib().orc_seed_cut_for(sens.encode(), cut is not None, 0.0 if cut is None else cut)
+
+
+def index_chunks_for(sens: str, chunks=None) -> int:
+    return lib().orc_index_chunks_for(sens.encode(), -1 if chunks is None else chunks)
+
+
+def translate_frame(nt: str, offset: int) -> np.ndarray:
+    b = C.create_string_buffer(len(nt) // 3 + 1)
+    n = lib().orc_translate_frame(nt.encode(), offset, b, len(nt) // 3 + 1)
+    return np.frombuffer(b.raw[:n], dtype=np.uint8).copy()
+
+
+def six_frames(nt: str):
+    cap = 2 * len(nt) + 6
+    b = C.create_string_buffer(cap)
+    lens = (C.c_uint64 * 6)()
+    lib().orc_six_frames(nt.encode(), b, cap, lens)
+    out, k = [], 0
+    for i in range(6):
+        out.append(np.frombuffer(b.raw[k:k + lens[i]], dtype=np.uint8).copy())
+        k += lens[i]
+    return out
+
+
+def mask_short_orfs(frame, min_len) -> np.ndarray:
+    b = C.create_string_buffer(_bytes(frame), len(frame))
+    lib().orc_mask_short_orfs(b, len(frame), min_len)
+    return np.frombuffer(b.raw[:len(frame)], dtype=np.uint8).copy()
+
+
+def min_orf_len(dna_len, user=None) -> int:
+    return lib().orc_min_orf_len(dna_len, -1 if user is None else user)
+
+
+FIELD_NAMES = ["qseqid", "qlen", "sseqid", "slen", "qstart", "qend", "sstart", "send", "qseq", "sseq", "evalue",
+               "bitscore", "score", "length", "pident", "nident", "mismatch", "positive", "gapopen", "gaps", "ppos",
+               "qframe", "qcovhsp", "scovhsp", "cigar", "btop", "qtitle", "stitle", "full_sseq", "qseq_translated",
+               "qstrand"]
+
+
+def parse_outfmt(tokens):
+    """Field names of an --outfmt token list, or None when the reference rejects it."""
+    f = (C.c_int * 64)()
+    n = lib().orc_parse_outfmt(" ".join(tokens).encode(), f, 64)
+    return None if n < 0 else [FIELD_NAMES[f[i]] for i in range(n)]
+
+
+def q_frame(frame: int) -> int:
+    return lib().orc_q_frame(frame)
+
+
+def nt_range(frame, q_begin, q_end, dna_len):
+    o = (C.c_uint64 * 2)()
+    lib().orc_nt_range(frame, q_begin, q_end, dna_len, o)
+    return (o[0], o[1])
+
+
+def evalue_blast(raw, qlen, db, matrix="BLOSUM62"):
+    return lib().orc_evalue_blast(matrix.encode(), raw, qlen, db)
+
+
+def matrix_ok(matrix, go=-1, ge=-1) -> bool:
+    return bool(lib().orc_matrix_ok(matrix.encode(), go, ge))
 
 
 def _bytes(a):
