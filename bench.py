@@ -126,7 +126,8 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def dist_setup(n_gpus):
+def dist_setup(n_gpus, backend=None):
+    """Rank plumbing: one process per GPU, NCCL (gloo on hosts without CUDA)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -134,9 +135,18 @@ def dist_setup(n_gpus):
         import torch
         import torch.distributed as dist
         from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+        if backend is None:
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=timedelta(seconds=600))
     return world, rank, local
+
+
+def _on_cuda():
+    import torch
+    import torch.distributed as dist
+    return torch.cuda.is_available() and (not dist.is_initialized() or dist.get_backend() == "nccl")
 
 
 def barrier_sync(world):
@@ -144,15 +154,17 @@ def barrier_sync(world):
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
-    torch.cuda.synchronize()
+    if _on_cuda():
+        torch.cuda.synchronize()
 
 
 def max_over_ranks(x, world):
+    """The slowest rank's time: replicas are timed on the device, the job by its max."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if _on_cuda() else "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -236,18 +248,20 @@ def main():
     launches = sum(s["kernel_launches"] for s in steps)
 
     # ---- end to end through the host-buffer C-ABI call --------------------
-    for _ in range(0 if args.no_e2e else min(args.warmup, 2)):
-        ctx.search(dl, do, tl, to, cfg)
+    # pinned copies of the inputs, as a serving host would hold them
+    pin = lambda a: torch.from_numpy(a).pin_memory().numpy()
+    pdl, pdo, ptl, pto = pin(dl), pin(do), pin(tl), pin(to)
+    for _ in range(0 if args.no_e2e else args.warmup):
+        ctx.search_counts(pdl, pdo, ptl, pto, cfg)
     e2e_s = 1e-9
     d2h = 0
     for _ in range(0 if args.no_e2e else args.steps):
         flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        lists, st = ctx.search(dl, do, tl, to, cfg)
+        n_h, n_ops, st = ctx.search_counts(pdl, pdo, ptl, pto, cfg)
         e2e_s += time.perf_counter() - t0
-        n_h = sum(len(x) for x in lists)
-        d2h = n_h * ctypes.sizeof(drgpu.Hsp) + sum(len(h.ops) for x in lists for h in x) * 4 + (len(to)) * 8
+        d2h = n_h * ctypes.sizeof(drgpu.Hsp) + n_ops * 4 + len(to) * 8
     e2e_s = max_over_ranks(e2e_s, world)
     h2d = int(dl.nbytes + do.nbytes + tl.nbytes + to.nbytes + len(w.queries) * 5)
     e2e = {"value": world * len(w.queries) * args.steps / e2e_s, "unit": "queries/s",

@@ -121,9 +121,18 @@ int drg_ctx_create(int device, drg_ctx** out) {
   drg_ctx* c = new (std::nothrow) drg_ctx();
   if (!c) return DRG_ERR_OOM;
   c->device = device;
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  const uint64_t keep = UINT64_MAX;  // hold freed blocks for reuse by the next call
   if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMemPoolCreate(&c->pool, &props) != cudaSuccess ||
+      cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, (void*)&keep) != cudaSuccess) {
     if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->side) cudaStreamDestroy(c->side);
+    if (c->pool) cudaMemPoolDestroy(c->pool);
     delete c;
     return DRG_ERR_CUDA;
   }
@@ -138,6 +147,7 @@ void drg_ctx_destroy(drg_ctx* c) {
   cudaStreamSynchronize(c->side);
   cudaStreamDestroy(c->stream);
   cudaStreamDestroy(c->side);
+  cudaMemPoolDestroy(c->pool);  // released once the last resident buffer is freed
   delete c;
 }
 
@@ -342,48 +352,62 @@ int drg_extend_span_batch(drg_ctx* c, const uint8_t* ql, const uint64_t* qo, uin
   Seqs qs, ss;
   qs.upload(c, ql, qo, nq);
   ss.upload(c, sl, so, ns);
-  std::vector<ExactJob> ej(n);
-  uint64_t soff = 0, ooff = 0;
+  // one Band per job (whole query as the window); the band kernels take what
+  // they support and the exact kernel the rest, as in the search's traceback
+  std::vector<Band> hb(n);
+  std::vector<uint64_t> ops_off(n + 1, 0);
   for (uint64_t i = 0; i < n; ++i) {
     const drg_span_job& j = jobs[i];
     if (j.query >= nq || j.subject >= ns) throw Error(DRG_ERR_INVALID, "job sequence index out of range");
-    if (j.d0 < INT32_MIN / 2 || j.d0 > INT32_MAX / 2 || j.d1 < INT32_MIN / 2 || j.d1 > INT32_MAX / 2)
-      throw Error(DRG_ERR_INVALID, "diagonal out of range");
-    ExactJob& e = ej[i];
-    e.q = qs.letters + qo[j.query];
-    e.s = ss.letters + so[j.subject];
-    e.n = (uint32_t)(qo[j.query + 1] - qo[j.query]);
-    e.m = (uint32_t)(so[j.subject + 1] - so[j.subject]);
-    e.d0 = (int32_t)j.d0;
-    e.d1 = (int32_t)j.d1;
-    e.scratch_off = soff;
-    e.ops_off = ooff;
-    soff += exact_scratch_bytes(e.n, e.m, e.d0, e.d1, true);
-    ooff += (uint64_t)e.n + e.m;
+    int64_t d0 = std::min(j.d0, j.d1), d1 = std::max(j.d0, j.d1);
+    if (d0 < INT32_MIN / 2 || d1 > INT32_MAX / 2) throw Error(DRG_ERR_INVALID, "diagonal out of range");
+    Band& b = hb[i];
+    std::memset(&b, 0, sizeof b);
+    b.target = j.query;
+    b.subject = j.subject;
+    b.d0 = (int32_t)d0;
+    b.d1 = (int32_t)d1;
+    b.n = (uint32_t)(qo[j.query + 1] - qo[j.query]);
+    ops_off[i + 1] = ops_off[i] + b.n + (so[j.subject + 1] - so[j.subject]);
   }
+  const uint64_t ooff = ops_off[n];
   set_exact_matrix(sc.scores);
-  DevArr<ExactJob> dj(n);
+  DevArr<Band> db_(n);
   DevArr<ExactOut> dout(n);
-  DevArr<uint8_t> scratch(soff);
-  DevArr<uint32_t> dops(ooff);
-  if (n) DRG_CUDA(cudaMemcpyAsync(dj.p, ej.data(), n * sizeof(ExactJob), cudaMemcpyHostToDevice, c->stream));
-  launch_sw_exact(dj.p, n, sc.gap_open, sc.gap_extend, true, scratch.p, dops.p, dout.p, c->stream);
+  DevArr<uint32_t> dops(ooff + 1);
+  DevArr<uint64_t> doff(n + 1);
+  DevArr<int64_t> cnt(2);
+  DevArr<unsigned long long> cells(1);
+  DRG_CUDA(cudaMemsetAsync(cells.p, 0, 8, c->stream));
+  if (n) {
+    DRG_CUDA(cudaMemcpyAsync(db_.p, hb.data(), n * sizeof(Band), cudaMemcpyHostToDevice, c->stream));
+    DRG_CUDA(cudaMemsetAsync(dout.p, 0, n * sizeof(ExactOut), c->stream));
+  }
+  DRG_CUDA(cudaMemcpyAsync(doff.p, ops_off.data(), (n + 1) * 8, cudaMemcpyHostToDevice, c->stream));
+  drg_run_stats st{};
+  run_bands(c, db_.p, n, qs.view(), ss.view(), sc, true, nullptr, nullptr, dout.p, dops.p, doff.p, &ops_off, st,
+            cnt.p, cells.p);
   std::vector<ExactOut> eo(n);
   std::vector<uint32_t> hops(ooff);
   if (n) DRG_CUDA(cudaMemcpyAsync(eo.data(), dout.p, n * sizeof(ExactOut), cudaMemcpyDeviceToHost, c->stream));
   if (ooff) DRG_CUDA(cudaMemcpyAsync(hops.data(), dops.p, ooff * 4, cudaMemcpyDeviceToHost, c->stream));
   sync(c);
   uint64_t total = 0;
-  for (auto& e : eo) total += e.n_ops;
+  for (auto& e : eo) total += e.score > 0 ? e.n_ops : 0;
   uint32_t* o = (uint32_t*)std::malloc(sizeof(uint32_t) * (total + 1));
   if (!o) throw Error(DRG_ERR_OOM, "host allocation failed");
   uint64_t k = 0;
   for (uint64_t i = 0; i < n; ++i) {
     drg_aligned& a = out[i];
     std::memset(&a, 0, sizeof a);
-    a.cells = eo[i].cells;
+    const Band& b = hb[i];
+    a.cells = band_cells_host(b.n, (uint32_t)(so[b.subject + 1] - so[b.subject]), b.d0, b.d1);
     a.ops_offset = k;
-    if (eo[i].score <= 0) continue;
+    if (eo[i].score < 0) {
+      std::free(o);
+      throw Error(DRG_ERR_CUDA, "internal: traceback left the band");
+    }
+    if (eo[i].score == 0) continue;
     a.found = 1;
     a.score = eo[i].score;
     a.q_begin = eo[i].q_begin;
@@ -397,7 +421,7 @@ int drg_extend_span_batch(drg_ctx* c, const uint8_t* ql, const uint64_t* qo, uin
     a.gaps = eo[i].gaps;
     a.length = eo[i].length;
     a.n_ops = eo[i].n_ops;
-    std::memcpy(o + k, hops.data() + ej[i].ops_off, eo[i].n_ops * 4);
+    std::memcpy(o + k, hops.data() + ops_off[i], eo[i].n_ops * 4);
     k += eo[i].n_ops;
   }
   *ops = o;

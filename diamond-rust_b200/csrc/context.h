@@ -14,6 +14,7 @@ struct drg_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaStream_t side = nullptr;  // concurrent launches (wide-band classes)
+  cudaMemPool_t pool = nullptr;  // resident databases and batches (kept across calls)
   std::string err;
   // seed stage
   drg::DevBuf q_keys, q_vals, q_keys_s, q_vals_s, r_keys, r_vals, r_keys_s, r_vals_s, cub_tmp;
@@ -25,7 +26,7 @@ struct drg_ctx {
   drg::DevBuf bands, bands_c, band_valid, pair_first, sw_keys, sw_keys_s, sw_order, sw_order_s, sw_tasks, scores,
       state, sel_idx, sel_bands, exact_jobs, exact_out, exact_scratch, exact_ops;
   drg::DevBuf tband, task_size, task_off, trace, rev, ex_bands, ops_off, trace_out, task_max;
-  drg::DevBuf sw_tasks_u, task_key, task_key_s, task_val, task_val_s, best_row;
+  drg::DevBuf sw_tasks_u, task_key, task_key_s, task_val, task_val_s, best_row, band_jobs_u, band_jobs;
   drg::HostBuf h_stage;
   cudaEvent_t ev[16] = {};
   drg_run_stats last{};

@@ -131,9 +131,10 @@ struct SwTask {        // one warp: up to 32 bands sharing a query window
 };
 // Trace-pass result of one band: where its nibbles are and its first maximum.
 struct TraceBand {
-  uint64_t trace_off;  // task trace_off + lane
+  uint64_t trace_off;  // first nibble word of the band
   uint32_t row_first, width;
-  int32_t score, best_i, best_j, pad;
+  int32_t score, best_i, best_j;
+  int32_t stride;      // words between consecutive column steps of the band
 };
 struct SwScoreArgs {
   const Band* bands;
@@ -151,6 +152,33 @@ struct SwScoreArgs {
   TraceBand* tband;   // trace mode: per band (indexed like bands)
   int8_t scores625[628];  // substitution scores, row-major
 };
+// One band of the intra-band (one warp per band) kernel.
+struct SwBandJob {
+  uint32_t band;       // index into bands
+  uint32_t row_first;  // first DP row (1-based)
+  uint32_t n_strips;   // 16-row strips from row_first
+  uint32_t pad;
+  uint64_t trace_off;  // trace mode: first uint2 of the band's nibbles
+};
+struct SwBandArgs {
+  const Band* bands;
+  const SwBandJob* jobs;
+  uint64_t lo, hi;  // jobs of this launch
+  const uint8_t* q_letters;
+  const uint64_t* q_offsets;
+  const uint8_t* s_letters;
+  const uint64_t* s_offsets;
+  int gap_open, gap_extend;
+  int32_t* score;     // score mode: per band
+  int32_t* best_row;  // score mode: first DP row holding the best
+  uint2* trace;       // trace mode: nibbles, strip k's step c at trace_off + k (W + 16) + c
+  TraceBand* tband;   // trace mode: per band
+  uint32_t xbuf_words;  // set by the launcher
+  int8_t scores625[628];
+};
+size_t sw_band_smem(int max_width);
+void launch_sw_band(SwBandArgs a, int max_width, bool trace, cudaStream_t st);
+
 struct ExactOut;
 struct SwWalkArgs {
   const Band* bands;

@@ -224,6 +224,50 @@ __global__ void k_set_trace_off(SwTask* tasks, const uint64_t* off, uint64_t n) 
   if (t < n) tasks[t].trace_off = off[t];
 }
 
+// Jobs of the one-warp-per-band kernel for the first n bands of the sorted
+// order: rows [rs, re] (re limited to the best row when known), longest first.
+__global__ void k_band_jobs(const uint32_t* order, const uint64_t* keys, uint64_t n, const Band* bands,
+                            const uint64_t* s_offsets, SwBandJob* jobs, uint64_t* sort_key, uint32_t* sort_val,
+                            unsigned long long* max_width) {
+  uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const uint32_t i = order[k];
+  const Band b = bands[i];
+  const int64_t m = (int64_t)(s_offsets[b.subject + 1] - s_offsets[b.subject]);
+  int64_t re = m + b.d1 < (int64_t)b.n ? m + b.d1 : (int64_t)b.n;
+  if (b.pad > 0 && (int64_t)b.pad < re) re = b.pad;  // the traceback needs no row below the best
+  const int64_t rs = (int64_t)(keys[k] & 0xFFFF);
+  if (re < rs) re = rs;
+  const uint32_t W = (uint32_t)(b.d1 - b.d0 + 1);
+  SwBandJob j;
+  j.band = i;
+  j.row_first = (uint32_t)rs;
+  j.n_strips = (uint32_t)((re - rs + 16) / 16);
+  j.pad = W;
+  j.trace_off = 0;
+  jobs[k] = j;
+  const uint64_t blocks = (j.n_strips + 31) / 32;
+  const uint64_t cost = blocks * (W + 16ull) + (uint64_t)(j.n_strips - 1) * 18ull;
+  sort_key[k] = ~cost;  // longest first
+  sort_val[k] = (uint32_t)k;
+  atomicMax(max_width, (unsigned long long)W);
+}
+__global__ void k_gather_band_jobs(const SwBandJob* in, const uint32_t* idx, uint64_t n, SwBandJob* out,
+                                   uint64_t* size) {
+  uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (k < n) {
+    const SwBandJob j = in[idx[k]];
+    out[k] = j;
+    size[k] = (uint64_t)j.n_strips * (j.pad + 16ull);
+  } else if (k == n) {
+    size[k] = 0;
+  }
+}
+__global__ void k_set_band_trace_off(SwBandJob* jobs, const uint64_t* off, uint64_t n) {
+  uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (k < n) jobs[k].trace_off = off[k];
+}
+
 // Bands the packed kernel did not take, or whose best is below 12.
 __global__ void k_exact_flags(const uint32_t* order, uint64_t n_fast, uint64_t n, const int32_t* score,
                               const TraceBand* tband, uint8_t* f) {
@@ -301,7 +345,75 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
     tb = c->tband.as<TraceBand>(n_bands);
     DRG_CUDA(cudaMemsetAsync(tb, 0xFF, n_bands * sizeof(TraceBand), c->stream));  // score -1: not traced
   }
-  if (n_fast > 0) {
+  if (n_fast > 0 && trace) {
+    // traceback: one warp per band (few, long bands)
+    SwBandJob* jobs_u = c->band_jobs_u.as<SwBandJob>(n_fast);
+    SwBandJob* jobs = c->band_jobs.as<SwBandJob>(n_fast);
+    uint64_t* tkey = c->task_key.as<uint64_t>(n_fast);
+    uint64_t* tkey_s = c->task_key_s.as<uint64_t>(n_fast);
+    uint32_t* tval = c->task_val.as<uint32_t>(n_fast);
+    uint32_t* tval_s = c->task_val_s.as<uint32_t>(n_fast);
+    unsigned long long* dmaxw = c->task_max.as<unsigned long long>(2 * kSwClasses);
+    DRG_CUDA(cudaMemsetAsync(dmaxw, 0, sizeof(unsigned long long), c->stream));
+    count_launch();
+    k_band_jobs<<<ceil_div(n_fast, 256), 256, 0, c->stream>>>(swos, swks, n_fast, bc, s.offsets, jobs_u, tkey, tval,
+                                                               dmaxw);
+    cub_call(c, [&](void* t, size_t& b) {
+      return cub::DeviceRadixSort::SortPairs(t, b, tkey, tkey_s, tval, tval_s, (int64_t)n_fast, 0, 64, c->stream);
+    });
+    uint64_t* tsize = c->task_size.as<uint64_t>(n_fast + 1);
+    uint64_t* toff = c->task_off.as<uint64_t>(n_fast + 1);
+    count_launch();
+    k_gather_band_jobs<<<ceil_div(n_fast + 1, 256), 256, 0, c->stream>>>(jobs_u, tval_s, n_fast, jobs, tsize);
+    cub_call(c, [&](void* t, size_t& b) {
+      return cub::DeviceScan::ExclusiveSum(t, b, tsize, toff, (int64_t)n_fast + 1, c->stream);
+    });
+    count_launch();
+    k_set_band_trace_off<<<ceil_div(n_fast, 256), 256, 0, c->stream>>>(jobs, toff, n_fast);
+    const uint64_t total = fetch(c, toff + n_fast);
+    const int max_w = (int)fetch(c, dmaxw);
+    SwBandArgs ba{};
+    ba.bands = bc;
+    ba.jobs = jobs;
+    ba.lo = 0;
+    ba.hi = n_fast;
+    ba.q_letters = qs.letters;
+    ba.q_offsets = qs.offsets;
+    ba.s_letters = s.letters;
+    ba.s_offsets = s.offsets;
+    ba.gap_open = scr.gap_open;
+    ba.gap_extend = scr.gap_extend;
+    ba.trace = c->trace.as<uint2>(total);
+    ba.tband = tb;
+    std::memcpy(ba.scores625, scr.scores, 625);
+    cudaEvent_t e0, e1;
+    DRG_CUDA(cudaEventCreate(&e0));
+    DRG_CUDA(cudaEventCreate(&e1));
+    DRG_CUDA(cudaEventRecord(e0, c->stream));
+    launch_sw_band(ba, max_w, true, c->stream);
+    DRG_CUDA(cudaEventRecord(e1, c->stream));
+    SwWalkArgs wa{};
+    wa.bands = bc;
+    wa.tband = tb;
+    wa.n_bands = n_bands;
+    wa.trace = ba.trace;
+    wa.q_letters = qs.letters;
+    wa.q_offsets = qs.offsets;
+    wa.s_letters = s.letters;
+    wa.s_offsets = s.offsets;
+    wa.ops_off = d_ops_off;
+    wa.rev = c->rev.as<uint8_t>((*h_ops_off)[n_bands] + 16);
+    wa.ops = ops;
+    wa.out = out;
+    std::memcpy(wa.scores625, scr.scores, 625);
+    launch_sw_walk(wa, c->stream);
+    DRG_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    DRG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    st.ms_trace_kernel += ms;
+  } else if (n_fast > 0) {
     uint32_t* gstart = c->idx.as<uint32_t>(n_fast + 1);
     count_launch();
     k_sw_group_start<<<ceil_div(n_fast, 256), 256, 0, c->stream>>>(swks, n_fast, gstart);
@@ -976,6 +1088,16 @@ void search(drg_ctx* ctx, const drg_db* db, const drg_batch* b, const drg_search
   ctx->last = out->stats;
 }
 
+// Resident inputs come from the context's stream-ordered pool, which keeps
+// freed memory for the next call instead of returning it to the driver.
+template <typename T>
+static void pool_alloc(drg_ctx* ctx, T** p, size_t bytes) {
+  DRG_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(p), bytes, ctx->pool, ctx->stream));
+}
+static void pool_free(drg_ctx* ctx, void* p) {
+  if (p) cudaFreeAsync(p, ctx->stream);
+}
+
 drg_db* make_db(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offsets, uint64_t n) {
   drg_db* d = new drg_db();
   d->ctx = ctx;
@@ -990,9 +1112,9 @@ drg_db* make_db(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offsets, u
     d->max_len = std::max<uint32_t>(d->max_len, (uint32_t)(offsets[i + 1] - offsets[i]));
   }
   try {
-    DRG_CUDA(cudaMalloc(&d->letters, d->total + 64));
-    DRG_CUDA(cudaMalloc(&d->offsets, (n + 1) * sizeof(uint64_t)));
-    DRG_CUDA(cudaMalloc(&d->owner, (d->total + 1) * sizeof(uint32_t)));
+    pool_alloc(ctx, &d->letters, d->total + 64);
+    pool_alloc(ctx, &d->offsets, (n + 1) * sizeof(uint64_t));
+    pool_alloc(ctx, &d->owner, (d->total + 1) * sizeof(uint32_t));
     DRG_CUDA(cudaMemsetAsync(d->letters + d->total, 25, 64, ctx->stream));
     if (d->total)
       DRG_CUDA(cudaMemcpyAsync(d->letters, letters, d->total, cudaMemcpyHostToDevice, ctx->stream));
@@ -1026,9 +1148,9 @@ drg_batch* make_batch(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offs
     b->max_len = std::max<uint32_t>(b->max_len, (uint32_t)(offsets[i + 1] - offsets[i]));
   }
   try {
-    DRG_CUDA(cudaMalloc(&b->letters, b->total + 64));
-    DRG_CUDA(cudaMalloc(&b->offsets, (n + 1) * sizeof(uint64_t)));
-    DRG_CUDA(cudaMalloc(&b->owner, (b->total + 1) * sizeof(uint32_t)));
+    pool_alloc(ctx, &b->letters, b->total + 64);
+    pool_alloc(ctx, &b->offsets, (n + 1) * sizeof(uint64_t));
+    pool_alloc(ctx, &b->owner, (b->total + 1) * sizeof(uint32_t));
     DRG_CUDA(cudaMemsetAsync(b->letters + b->total, 25, 64, ctx->stream));
     if (b->total)
       DRG_CUDA(cudaMemcpyAsync(b->letters, letters, b->total, cudaMemcpyHostToDevice, ctx->stream));
@@ -1044,17 +1166,17 @@ drg_batch* make_batch(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offs
 
 void free_db(drg_db* d) {
   if (!d) return;
-  cudaFree(d->letters);
-  cudaFree(d->offsets);
-  cudaFree(d->owner);
+  pool_free(d->ctx, d->letters);
+  pool_free(d->ctx, d->offsets);
+  pool_free(d->ctx, d->owner);
   delete d;
 }
 
 void free_batch(drg_batch* b) {
   if (!b) return;
-  cudaFree(b->letters);
-  cudaFree(b->offsets);
-  cudaFree(b->owner);
+  pool_free(b->ctx, b->letters);
+  pool_free(b->ctx, b->offsets);
+  pool_free(b->ctx, b->owner);
   delete b;
 }
 

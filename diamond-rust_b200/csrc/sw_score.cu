@@ -33,60 +33,13 @@
 // buffer and tracks the first row-major maximum; a walk kernel then follows
 // the reference's traceback (gapped.rs:205-279) through those nibbles.
 #include "kernels.h"
+#include "sw_common.cuh"
 
 namespace drg {
 
 namespace {
 
-constexpr int kRows = 16;          // rows per strip
-constexpr int kPairs = kRows / 2;  // s16x2 pairs
-constexpr int kProfStride = 24;    // bytes per residue row of the strip profile
-constexpr int kProfBytes = 26 * kProfStride;
-constexpr uint32_t kNeg2 = 0xC000C000u;  // (-16384, -16384)
-
-__device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
-  uint32_t r;
-  asm("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(sel));
-  return r;
-}
-__device__ __forceinline__ uint32_t add2(uint32_t a, uint32_t b) {
-  uint32_t r;
-  asm("add.s16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
-  return r;
-}
-__device__ __forceinline__ uint32_t max2(uint32_t a, uint32_t b) {
-  uint32_t r;
-  asm("max.s16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
-  return r;
-}
-__device__ __forceinline__ uint32_t max2_relu(uint32_t a, uint32_t b) {
-  uint32_t r;
-  asm("max.s16x2.relu %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
-  return r;
-}
-// keep halves selected by k (0xFFFF per kept half), replace the others with v
-__device__ __forceinline__ uint32_t sel2(uint32_t x, uint32_t k, uint32_t v) { return (x & k) | (v & ~k); }
-
-// Sign-extending byte pick: low half = byte b of lo, high half = byte b of hi.
-__device__ __forceinline__ constexpr uint32_t pick_sel(int b) {
-  return (uint32_t)(b) | ((uint32_t)(8 | b) << 4) | ((uint32_t)(4 + b) << 8) | ((uint32_t)(8 | (4 + b)) << 12);
-}
-
-struct Lane {
-  const uint8_t* s;  // subject letters
-  int m;             // subject length
-  int jbase;         // absolute column of relative column 0 in this strip
-};
-
-template <bool TR>
-struct Regs {
-  uint32_t H[kPairs], Hm[kPairs], F[kPairs];
-  uint32_t E7;        // E of pair 7 at the previous step
-  uint32_t htop_old;  // top H of the previous step (D operand of pair 0)
-  uint32_t res_prev;  // subject residue of the previous column
-  uint32_t rowmax[kPairs];            // per row of the strip: max H so far
-  uint32_t rowcol[TR ? kPairs : 1];   // trace mode: first column of that max
-};
+using namespace sw;
 
 // One column step.  MODE 0: middle (all rows in band), 1: prologue step
 // C (= c), 2: epilogue step C (= c - W) of a warp whose bands share one
@@ -198,9 +151,6 @@ struct Unroll<MODE, kRows, TR> {
   static __device__ __forceinline__ void run(Regs<TR>&, const Lane&, int, const uint8_t*, uint32_t*, int, int, int&,
                                              uint32_t, uint32_t, uint2*) {}
 };
-
-__device__ __forceinline__ int lo16(uint32_t x) { return (int)(int16_t)(x & 0xFFFFu); }
-__device__ __forceinline__ int hi16(uint32_t x) { return (int)(int16_t)(x >> 16); }
 
 template <int WARPS, bool TR>
 __global__ void __launch_bounds__(WARPS * 32) k_sw(SwScoreArgs a) {
@@ -318,7 +268,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_sw(SwScoreArgs a) {
     t.score = best;
     t.best_i = best_i;
     t.best_j = best_j;
-    t.pad = 0;
+    t.stride = 32;  // lane-interleaved
     a.tband[bidx] = t;
   }
 }
@@ -362,7 +312,7 @@ __global__ void k_sw_walk(SwWalkArgs a) {
     const int64_t k = (i - rf) >> 4, r = (i - rf) & 15;
     const int64_t c = j - (rf + 16 * k - d1);
     const int64_t it = c + (r >= 8 ? 1 : 0);
-    const uint2 w = a.trace[tb.trace_off + (uint64_t)(k * (W + 16) + it) * 32];
+    const uint2 w = a.trace[tb.trace_off + (uint64_t)(k * (W + 16) + it) * (uint64_t)tb.stride];
     const uint32_t p = (uint32_t)(r & 7);
     const uint32_t byte = ((p < 4 ? w.x : w.y) >> (8 * (p & 3))) & 0xFFu;
     const uint32_t nib = r >= 8 ? byte >> 4 : byte & 0xFu;

@@ -128,6 +128,9 @@ _SIGNATURES = {
     "drg_extend_span_scores": (C.c_int, [C.c_void_p, _u8p, _u64p, C.c_uint64, _u8p, _u64p, C.c_uint64,
                                          _P(SpanJob), C.c_uint64, C.c_char_p, C.c_int32, C.c_int32, _i32p,
                                          _P(RunStats)]),
+    "drg_extend_span_noalloc": (C.c_int, [C.c_void_p, _u64p, C.c_uint64, C.c_void_p, _u64p, C.c_uint64,
+                                          _P(SpanJob), C.c_uint64, C.c_char_p, C.c_int32, C.c_int32, C.c_void_p,
+                                          C.c_void_p, C.c_uint64, C.c_void_p, C.c_char_p, C.c_size_t]),
     "drg_db_create": (C.c_int, [C.c_void_p, _u8p, _u64p, C.c_uint64, _P(C.c_void_p)]),
     "drg_db_destroy": (None, [C.c_void_p]),
     "drg_batch_create": (C.c_int, [C.c_void_p, _u8p, _u64p, _u32p, _u8p, C.c_uint64, _P(C.c_void_p)]),
@@ -381,6 +384,24 @@ class Context:
             return _result_lists(res), res.stats.as_dict()
         finally:
             self.lib.drg_result_free(C.byref(res))
+
+    def search_counts(self, db_letters, db_offsets, t_letters, t_offsets, config: SearchConfig):
+        """The same C-ABI call as ``search``, returning only (n_hsps, n_ops, stats): for timing the
+        drop-in call without building Python records."""
+        dl, dlp = _u8(db_letters if len(db_letters) else np.zeros(1, np.uint8))
+        do, dop = _u64(db_offsets)
+        tl, tlp = _u8(t_letters if len(t_letters) else np.zeros(1, np.uint8))
+        to, top = _u64(t_offsets)
+        n_t = len(t_offsets) - 1
+        tq, tqp = _u32(np.arange(n_t))
+        tf, tfp = _u8(np.zeros(n_t))
+        res = Result()
+        self._check(self.lib.drg_search_run(self.h, dlp, dop, len(db_offsets) - 1, tlp, top, tqp, tfp, n_t,
+                                            C.byref(config), C.byref(res)))
+        n_hsps, n_ops = int(res.n_hsps), int(res.n_ops)
+        stats = res.stats.as_dict()
+        self.lib.drg_result_free(C.byref(res))
+        return n_hsps, n_ops, stats
 
     def probe_int_peak(self):
         ops, mhz = C.c_double(), C.c_double()

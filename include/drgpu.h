@@ -186,7 +186,7 @@ int drg_extend_span_noalloc(const uint8_t* d_q_letters, const uint64_t* q_offset
 
 /* Database resident in device memory: letters[offsets[i]..offsets[i+1]]. */
 int drg_db_create(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offsets, uint64_t n_seqs, drg_db** out);
-void drg_db_destroy(drg_db* db);
+void drg_db_destroy(drg_db* db);  /* before the db's context is destroyed */
 
 /* Query batch (search::Target list, search.rs:82-88) resident in device memory. */
 int drg_batch_create(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offsets, const uint32_t* query_index,

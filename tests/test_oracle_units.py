@@ -124,8 +124,6 @@ def test_ln_factorial_is_a_sequential_sum():
 
 
 # ---- ungapped.rs:99-129 -------------------------------------------------------
-BLOSUM62_DIAG = {}
-
 
 def _self_score(seq):
     return sum(orc.xdrop(seq[i:i + 1], seq[i:i + 1], 0, 0, xd=1000)[3] for i in range(len(seq)))
