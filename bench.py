@@ -50,17 +50,22 @@ def parse():
     p.add_argument("--cpu-sample", type=int, default=100, help="queries in the CPU baseline sample")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    p.add_argument("--queries", type=int, default=None,
+                   help="search only the first N queries (a smaller case for ncu captures; not a bench line)")
     return p.parse_args()
 
 
-def workload():
+def workload(n_queries=None):
     from drgpu import synth
-    return synth.workload(2)
+    w = synth.workload(2)
+    if n_queries is not None:
+        w.queries = w.queries[:n_queries]
+    return w
 
 
 def config_desc(w):
     return {
-        "workload": "1000 queries (lognormal mean 350, 50-1500 aa, 5 planted homologs each) x 7,860-sequence "
+        "workload": f"{len(w.queries)} queries (lognormal mean 350, 50-1500 aa, 5 planted homologs each) x 7,860-sequence "
                     "synthetic DB, blastp --sensitive, BLOSUM62 11/1, evalue 1e-3, k 25, max-hsps 1, "
                     "index-chunks 1",
         "queries": len(w.queries),
@@ -214,7 +219,7 @@ def main():
     import drgpu
 
     torch.cuda.set_device(local)
-    w = workload()
+    w = workload(args.queries)
     ctx = drgpu.Context(local)
     peak_ops, probe_mhz = ctx.probe_int_peak()
     peak_gcups = peak_ops * 2.0 / 4.0 / 1e9

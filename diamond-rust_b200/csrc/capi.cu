@@ -377,8 +377,8 @@ int drg_extend_span_batch(drg_ctx* c, const uint8_t* ql, const uint64_t* qo, uin
   DevArr<uint32_t> dops(ooff + 1);
   DevArr<uint64_t> doff(n + 1);
   DevArr<int64_t> cnt(2);
-  DevArr<unsigned long long> cells(1);
-  DRG_CUDA(cudaMemsetAsync(cells.p, 0, 8, c->stream));
+  DevArr<unsigned long long> cells(2);
+  DRG_CUDA(cudaMemsetAsync(cells.p, 0, 16, c->stream));
   if (n) {
     DRG_CUDA(cudaMemcpyAsync(db_.p, hb.data(), n * sizeof(Band), cudaMemcpyHostToDevice, c->stream));
     DRG_CUDA(cudaMemsetAsync(dout.p, 0, n * sizeof(ExactOut), c->stream));
@@ -459,8 +459,8 @@ int drg_extend_span_scores(drg_ctx* c, const uint8_t* ql, const uint64_t* qo, ui
   DevArr<Band> db_(n);
   DevArr<int32_t> ds(n);
   DevArr<int64_t> cnt(2);
-  DevArr<unsigned long long> cells(1);
-  DRG_CUDA(cudaMemsetAsync(cells.p, 0, 8, c->stream));
+  DevArr<unsigned long long> cells(2);
+  DRG_CUDA(cudaMemsetAsync(cells.p, 0, 16, c->stream));
   if (n) DRG_CUDA(cudaMemcpyAsync(db_.p, hb.data(), n * sizeof(Band), cudaMemcpyHostToDevice, c->stream));
   drg_run_stats st{};
   run_bands(c, db_.p, n, qs.view(), ss.view(), sc, false, ds.p, nullptr, nullptr, nullptr, nullptr, nullptr, st, cnt.p,

@@ -26,7 +26,8 @@ struct drg_ctx {
   drg::DevBuf bands, bands_c, band_valid, pair_first, sw_keys, sw_keys_s, sw_order, sw_order_s, sw_tasks, scores,
       state, sel_idx, sel_bands, exact_jobs, exact_out, exact_scratch, exact_ops;
   drg::DevBuf tband, task_size, task_off, trace, rev, ex_bands, ops_off, trace_out, task_max;
-  drg::DevBuf sw_tasks_u, task_key, task_key_s, task_val, task_val_s, best_row, band_jobs_u, band_jobs;
+  drg::DevBuf sw_tasks_u, task_key, task_key_s, task_val, task_val_s, best_row, band_jobs_u, band_jobs, sw_rows, sw_rows_s,
+      sw_keys_r, sw_order_r;
   drg::HostBuf h_stage;
   cudaEvent_t ev[16] = {};
   drg_run_stats last{};

@@ -114,10 +114,13 @@ __host__ __device__ __forceinline__ int sw_class_of(uint32_t w) {
   return w <= (uint32_t)kSwC0 ? 0 : (w <= (uint32_t)kSwC1 ? 1 : (w <= (uint32_t)kSwC2 ? 2 : 3));
 }
 
-// Classify bands for the packed kernel and build its sort keys:
-// (target, window start, width, first real row); others get ~0.
+// Classify bands for the packed kernel and build its two sort keys:
+//  key  (target, window start, width) << 16, or ~0 for the exact kernel;
+//  rows (first-row strip bucket, last row), the last row descending in odd
+//       buckets, so that bands next to each other in (key, rows) order cover
+//       nearly the same rows.
 __global__ void k_sw_keys(const Band* bands, uint64_t n, const uint64_t* s_offsets, int max_score,
-                          uint64_t* keys, uint32_t* order) {
+                          uint64_t* keys, uint32_t* rows, uint32_t* order) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   Band b = bands[i];
@@ -128,10 +131,17 @@ __global__ void k_sw_keys(const Band* bands, uint64_t n, const uint64_t* s_offse
   int64_t mn = m < (int64_t)b.n ? m : (int64_t)b.n;
   bool fast = W >= kSwMinWidth && W <= kSwMaxWidth && (int64_t)max_score * mn <= 32000 && rs <= re &&
               b.target < (1u << 21) && b.q0 < 65536 && re < 65536;
-  keys[i] = fast ? ((uint64_t)b.target << 43) | ((uint64_t)b.q0 << 27) | ((uint64_t)W << 16) | (uint64_t)rs
-                 : ~0ull;
+  keys[i] = fast ? ((uint64_t)b.target << 43) | ((uint64_t)b.q0 << 27) | ((uint64_t)W << 16) : ~0ull;
+  const uint32_t bucket = fast ? (uint32_t)(rs >> 4) : 0xFFFFu;
+  const uint32_t last = fast ? (uint32_t)re : 0u;
+  rows[i] = (bucket << 16) | ((bucket & 1) ? 0xFFFFu - last : last);
   order[i] = (uint32_t)i;
 }
+__global__ void k_gather_keys(const uint64_t* keys, const uint32_t* idx, uint64_t n, uint64_t* out) {
+  uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (k < n) out[k] = keys[idx[k]];
+}
+__device__ __forceinline__ int64_t band_first_row(const Band& b) { return b.d0 + 1 > 1 ? b.d0 + 1 : 1; }
 
 // Task heads: first band of each (target, window) group and every 32nd after
 // (a group's bands are in width order, so a warp's widths are close).
@@ -155,18 +165,20 @@ __global__ void k_sw_fill_tasks(const uint32_t* starts, uint64_t n_tasks, const 
   uint32_t cnt = 0;
   int64_t row_first = INT64_MAX, row_last = 0;
   uint32_t wmin = 0xFFFFFFFFu, wmax = 0;
+  uint64_t lane_cells = 0;
   while (cnt < 32 && s + cnt < n_fast && (keys[s + cnt] >> 27) == grp) {
     const uint64_t key = keys[s + cnt];
     const Band b = bands[order[s + cnt]];
     int64_t m = (int64_t)(s_offsets[b.subject + 1] - s_offsets[b.subject]);
     int64_t re = m + b.d1 < (int64_t)b.n ? m + b.d1 : (int64_t)b.n;
     if (row_limit && b.pad > 0 && (int64_t)b.pad < re) re = b.pad;  // traceback: rows up to the best
-    const int64_t rs = (int64_t)(key & 0xFFFF);
+    const int64_t rs = band_first_row(b);
     const uint32_t w = (uint32_t)((key >> 16) & 0x7FF);
     if (re > row_last) row_last = re;
     if (rs < row_first) row_first = rs;
     if (w < wmin) wmin = w;
     if (w > wmax) wmax = w;
+    lane_cells += (uint64_t)((re - rs + 16) / 16) * 16ull * (w + 16ull);
     ++cnt;
   }
   if (row_last < row_first) row_last = row_first;
@@ -184,7 +196,10 @@ __global__ void k_sw_fill_tasks(const uint32_t* starts, uint64_t n_tasks, const 
   sort_key[t] = ((uint64_t)cls << 60) | ((~steps) & ((1ull << 60) - 1));  // class, then longest first
   sort_val[t] = (uint32_t)t;
   if (trace_size) trace_size[t] = steps * 32ull;
-  atomicAdd(cells_gpu, (unsigned long long)k.n_strips * 16ull * (wmax + 16ull) * cnt);
+  if (cells_gpu) {
+    atomicAdd(cells_gpu, (unsigned long long)k.n_strips * 16ull * (wmax + 16ull) * cnt);
+    atomicAdd(cells_gpu + 1, (unsigned long long)lane_cells);
+  }
 }
 
 __global__ void k_task_trace_size(const SwTask* tasks, uint64_t n, uint64_t* size) {
@@ -236,7 +251,7 @@ __global__ void k_band_jobs(const uint32_t* order, const uint64_t* keys, uint64_
   const int64_t m = (int64_t)(s_offsets[b.subject + 1] - s_offsets[b.subject]);
   int64_t re = m + b.d1 < (int64_t)b.n ? m + b.d1 : (int64_t)b.n;
   if (b.pad > 0 && (int64_t)b.pad < re) re = b.pad;  // the traceback needs no row below the best
-  const int64_t rs = (int64_t)(keys[k] & 0xFFFF);
+  const int64_t rs = band_first_row(b);
   if (re < rs) re = rs;
   const uint32_t W = (uint32_t)(b.d1 - b.d0 + 1);
   SwBandJob j;
@@ -334,10 +349,20 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
   uint64_t* swks = c->sw_keys_s.as<uint64_t>(n_bands);
   uint32_t* swo = c->sw_order.as<uint32_t>(n_bands);
   uint32_t* swos = c->sw_order_s.as<uint32_t>(n_bands);
+  uint32_t* rows = c->sw_rows.as<uint32_t>(n_bands);
+  uint32_t* rows_s = c->sw_rows_s.as<uint32_t>(n_bands);
+  uint64_t* swk_r = c->sw_keys_r.as<uint64_t>(n_bands);
+  uint32_t* swo_r = c->sw_order_r.as<uint32_t>(n_bands);
   count_launch();
-  k_sw_keys<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(bc, n_bands, s.offsets, scr.max_score, swk, swo);
+  k_sw_keys<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(bc, n_bands, s.offsets, scr.max_score, swk, rows, swo);
+  // rows first, then a stable sort by (target, window, width)
   cub_call(c, [&](void* t, size_t& b) {
-    return cub::DeviceRadixSort::SortPairs(t, b, swk, swks, swo, swos, (int64_t)n_bands, 0, 64, c->stream);
+    return cub::DeviceRadixSort::SortPairs(t, b, rows, rows_s, swo, swo_r, (int64_t)n_bands, 0, 32, c->stream);
+  });
+  count_launch();
+  k_gather_keys<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(swk, swo_r, n_bands, swk_r);
+  cub_call(c, [&](void* t, size_t& b) {
+    return cub::DeviceRadixSort::SortPairs(t, b, swk_r, swks, swo_r, swos, (int64_t)n_bands, 16, 64, c->stream);
   });
   const uint64_t n_fast = (uint64_t)count_valid(c, swks, n_bands, d_count);
   TraceBand* tb = nullptr;
@@ -608,7 +633,7 @@ struct Search {
   std::vector<Candidate> cands;
   // device scratch for counters
   int64_t* d_count = nullptr;
-  unsigned long long* d_counters = nullptr;  // [0] xdrops [1] cells_ref [2] computed [3] cells_gpu
+  unsigned long long* d_counters = nullptr;  // [0] xdrops [1] cells_ref [2] computed [3] cells_gpu [4] lane cells
 
   void configure(const drg_search_config* cfg) {
     std::string err;
@@ -982,7 +1007,7 @@ void Search::finish(drg_result* out) {
     DevSeqs qs{q->letters, q->offsets, &q->h_offsets};
     DevSeqs ss{db->letters, db->offsets, &db->h_offsets};
     run_bands(c, db_, nj, qs, ss, sc, true, nullptr, nullptr, dout, dops, doff, &ops_off, st, d_count,
-              d_counters + 4);
+              nullptr);
     fetch_n(c, eo, dout, nj);
     fetch_n(c, ops_all, dops, ops_off[nj]);
     st.ms_trace += tm.stop();
@@ -1064,13 +1089,14 @@ void Search::run(drg_result* out) {
     for (auto [c0, c1] : split_chunks(db->n, index_chunks)) chunk(cid++, c0, c1, n_runs);
   }
   finish(out);
-  unsigned long long cnt[4];
+  unsigned long long cnt[5];
   DRG_CUDA(cudaMemcpyAsync(cnt, d_counters, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
   DRG_CUDA(cudaStreamSynchronize(c->stream));
   st.xdrops = cnt[0];
   st.dp_cells_ref = cnt[1];
   st.bands_computed = cnt[2];
   st.dp_cells_gpu = cnt[3];
+  st.dp_cells_lane = cnt[4];
   st.ms_total = total.stop();
   st.kernel_launches = kernel_launch_count() - launches0;
   out->stats = st;

@@ -86,7 +86,7 @@ class RunStats(C.Structure):
                                           "ms_sw_kernel")] + \
                [("sw_launches", C.c_uint64), ("kernel_launches", C.c_uint64), ("exact_bands", C.c_uint64),
                 ("sw_class_tasks", C.c_uint64 * 4), ("sw_class_max_steps", C.c_uint64 * 4),
-                ("ms_sw_class", C.c_double * 4), ("ms_trace_kernel", C.c_double)]
+                ("ms_sw_class", C.c_double * 4), ("ms_trace_kernel", C.c_double), ("dp_cells_lane", C.c_uint64)]
 
     def as_dict(self):
         d = {}

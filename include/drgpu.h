@@ -104,6 +104,7 @@ typedef struct {
   uint64_t sw_class_max_steps[4];  /* longest warp: strips x (W + 16) column steps */
   double ms_sw_class[4];           /* device time of each class launch */
   double ms_trace_kernel;          /* device time of the trace-mode kernel launches */
+  uint64_t dp_cells_lane;          /* score kernel: each band's own rows x (W + 16), without warp padding */
 } drg_run_stats;
 
 /* search::run result: per-target HSP lists, target_offsets[n_targets+1]. */
