@@ -38,6 +38,12 @@ sys.path.insert(0, os.path.join(ROOT, "diamond-rust_b200"))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 METRIC = "bit-exact queries/sec + SW GCUPS, batched vs plain on 1 B200; p50/p99 latency"
+# DRAM bytes per evaluated DP cell of the score kernel: dram__bytes_read.sum +
+# dram__bytes_write.sum of the k_sw launches of one ncu capture on the
+# 200-query case over that pass's evaluated cells (profiles/); scaled to a full
+# pass by its evaluated cells (the traffic is the bands, query windows and
+# subjects the warps read, in proportion to the work).
+SW_TRAFFIC_PER_CELL = None
 SENS = "sensitive"
 
 
@@ -222,7 +228,10 @@ def main():
     w = workload(args.queries)
     ctx = drgpu.Context(local)
     peak_ops, probe_mhz = ctx.probe_int_peak()
-    peak_gcups = peak_ops * 2.0 / 4.0 / 1e9
+    # the recurrence as implemented: 7 s16x2 ALU ops per 2 cells (score pick,
+    # D add, E and F add-max, H max3 with 0, H - open, strip maximum)
+    ops_per_cell = 3.5
+    peak_gcups = peak_ops / ops_per_cell / 1e9
     dl, do = drgpu.concat(w.db)
     tl, to = drgpu.concat(w.queries)
     cfg = drgpu.make_config(sensitivity=SENS, index_chunks=1)
@@ -249,6 +258,8 @@ def main():
     sw_launches = sum(s["sw_launches"] for s in steps)
     cells_ref = sum(s["dp_cells_ref"] for s in steps)
     cells_gpu = sum(s["dp_cells_gpu"] for s in steps)
+    cells_lane = sum(s["dp_cells_lane"] for s in steps)
+    passes = len(steps)  # one score pass (the concurrent width-class launches) per search
     gcups = cells_ref / (sw_ms / 1000.0) / 1e9 if sw_ms > 0 else 0.0
     launches = sum(s["kernel_launches"] for s in steps)
 
@@ -296,17 +307,20 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "int16x2/int32", "data": "synthetic",
             "config": dict(config_desc(w), parallelism=f"replicas x{world}"),
             "gcups": gcups,
-            "roofline": {"bound": "int", "kernel": "sw_score (banded SW, packed 16-bit DPX)",
+            "roofline": {"bound": "int", "kernel": "k_sw (banded SW score pass, packed s16x2 DPX)",
                          "achieved": gcups, "peak": peak_gcups, "unit": "GCUPS", "frac": gcups / peak_gcups,
-                         "traffic": None,
-                         "peak_source": f"measured live: s16x2 DPX issue {peak_ops / 1e12:.2f} T lane-ops/s at "
-                                        f"~{probe_mhz:.0f} MHz x 2 cells / 4 ops per cell",
-                         "cells_ref_per_launch": cells_ref / max(sw_launches, 1),
-                         "cells_evaluated_per_launch": cells_gpu / max(sw_launches, 1),
-                         "ms_per_launch": sw_ms / max(sw_launches, 1)},
+                         "traffic": SW_TRAFFIC_PER_CELL * cells_gpu / passes if SW_TRAFFIC_PER_CELL else None,
+                         "peak_source": f"measured live: s16x2 integer-pipe issue {peak_ops / 1e12:.2f} T lane-ops/s "
+                                        f"at ~{probe_mhz:.0f} MHz / {ops_per_cell} lane-ops per DP cell",
+                         "ops_per_cell": ops_per_cell,
+                         "cells_ref_per_pass": cells_ref / passes,
+                         "cells_lane_per_pass": cells_lane / passes,
+                         "cells_evaluated_per_pass": cells_gpu / passes,
+                         "ms_per_pass": sw_ms / passes},
             "stages_ms": {k: round(s0[k], 3) for k in ("ms_seed", "ms_join", "ms_sort", "ms_ungapped", "ms_bands",
                                                          "ms_sw", "ms_sw_kernel", "ms_select", "ms_trace",
                                                          "ms_trace_kernel", "ms_host")},
+            "sw_wide": {"bands": int(s0["sw_wide_bands"]), "ms": round(s0["ms_sw_wide"], 3)},
             "sw_classes": {"width_max": [136, 272, 544, 1700], "warps": s0["sw_class_tasks"],
                            "longest_warp_steps": s0["sw_class_max_steps"],
                            "ms": [round(x, 3) for x in s0["ms_sw_class"]]},

@@ -8,6 +8,7 @@
 #include <chrono>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <unordered_map>
 
@@ -112,6 +113,23 @@ const char* drg_version(void) { return "drgpu 0.1 (sm_100a)"; }
 
 void drg_free(void* p) { std::free(p); }
 
+// Constant-memory banks in use, one per live context.
+static std::mutex g_slot_mutex;
+static bool g_slot_used[kConstSlots] = {};
+static int acquire_slot() {
+  std::lock_guard<std::mutex> lock(g_slot_mutex);
+  for (int i = 0; i < kConstSlots; ++i)
+    if (!g_slot_used[i]) {
+      g_slot_used[i] = true;
+      return i;
+    }
+  return -1;
+}
+static void release_slot(int i) {
+  std::lock_guard<std::mutex> lock(g_slot_mutex);
+  if (i >= 0 && i < kConstSlots) g_slot_used[i] = false;
+}
+
 int drg_ctx_create(int device, drg_ctx** out) {
   if (!out) return DRG_ERR_INVALID;
   *out = nullptr;
@@ -121,6 +139,11 @@ int drg_ctx_create(int device, drg_ctx** out) {
   drg_ctx* c = new (std::nothrow) drg_ctx();
   if (!c) return DRG_ERR_OOM;
   c->device = device;
+  c->slot = acquire_slot();
+  if (c->slot < 0) {
+    delete c;
+    return DRG_ERR_INVALID;  // more live contexts than constant banks
+  }
   cudaMemPoolProps props{};
   props.allocType = cudaMemAllocationTypePinned;
   props.location.type = cudaMemLocationTypeDevice;
@@ -133,6 +156,7 @@ int drg_ctx_create(int device, drg_ctx** out) {
     if (c->stream) cudaStreamDestroy(c->stream);
     if (c->side) cudaStreamDestroy(c->side);
     if (c->pool) cudaMemPoolDestroy(c->pool);
+    release_slot(c->slot);
     delete c;
     return DRG_ERR_CUDA;
   }
@@ -148,6 +172,7 @@ void drg_ctx_destroy(drg_ctx* c) {
   cudaStreamDestroy(c->stream);
   cudaStreamDestroy(c->side);
   cudaMemPoolDestroy(c->pool);  // released once the last resident buffer is freed
+  release_slot(c->slot);
   delete c;
 }
 
@@ -188,13 +213,15 @@ int drg_seed_build(drg_ctx* c, const uint8_t* letters, const uint64_t* offsets, 
   p.size = (uint64_t)red.size;
   p.cut = complexity_cut;
   ln_factorial_table(p.lnfact);
+  p.shape_shift = 48;  // one shape: the key is the shape's packed key
+  p.request_shift = 56;
   Seqs s;
   s.upload(c, letters, offsets, n_seqs);
-  upload_seed_params(t, p, c->stream);
+  upload_seed_params(t, p, c->slot, c->stream);
   const uint64_t N = s.total;
   DevArr<uint64_t> k(N), ks(N);
   DevArr<uint32_t> v(N), vs(N);
-  launch_seed_enum(s.letters, s.offsets, s.owner, 0, s.total, 1, k.p, v.p, c->stream);
+  launch_seed_enum(s.letters, s.offsets, s.owner, 0, s.total, 1, k.p, v.p, c->slot, c->stream);
   cub_run(c, [&](void* tmp, size_t& b) {
     return cub::DeviceRadixSort::SortPairs(tmp, b, k.p, ks.p, v.p, vs.p, (int64_t)N, 0, 64, c->stream);
   });
@@ -272,7 +299,8 @@ int drg_seed_join(drg_ctx* c, const drg_seed_entry* q, uint64_t nq, const drg_se
     cub_run(c, [&](void* tmp, size_t& b) {
       return cub::DeviceScan::ExclusiveSum(tmp, b, ucount.p, ustart.p, n_runs, c->stream);
     });
-    launch_join_count(ukeys.p, ucount.p, (uint64_t)n_runs, drk.p, nr, max_expand, rlo.p, rcnt.p, uhits.p, c->stream);
+    launch_join_count(ukeys.p, ucount.p, (uint64_t)n_runs, drk.p, nr, max_expand, rlo.p, rcnt.p, uhits.p, ~0ull,
+                      c->stream);
     DRG_CUDA(cudaMemsetAsync(uhits.p + n_runs, 0, 8, c->stream));
     cub_run(c, [&](void* tmp, size_t& b) {
       return cub::DeviceScan::ExclusiveSum(tmp, b, uhits.p, uoff.p, n_runs + 1, c->stream);
@@ -331,11 +359,11 @@ int drg_xdrop_batch(drg_ctx* c, const uint8_t* ql, const uint64_t* qo, uint64_t 
   Seqs qs, ss;
   qs.upload(c, ql, qo, nq);
   ss.upload(c, sl, so, ns);
-  upload_score_matrix(sc.scores, c->stream);
+  upload_score_matrix(sc.scores, c->slot, c->stream);
   DevArr<drg_xdrop_job> dj(n);
   DevArr<drg_segment> dout(n);
   if (n) DRG_CUDA(cudaMemcpyAsync(dj.p, jobs, n * sizeof(drg_xdrop_job), cudaMemcpyHostToDevice, c->stream));
-  launch_xdrop_jobs(dj.p, n, qs.letters, qs.offsets, ss.letters, ss.offsets, xdrop, dout.p, c->stream);
+  launch_xdrop_jobs(dj.p, n, qs.letters, qs.offsets, ss.letters, ss.offsets, xdrop, dout.p, c->slot, c->stream);
   if (n) DRG_CUDA(cudaMemcpyAsync(out, dout.p, n * sizeof(drg_segment), cudaMemcpyDeviceToHost, c->stream));
   sync(c);
   API_END(c)
@@ -371,7 +399,6 @@ int drg_extend_span_batch(drg_ctx* c, const uint8_t* ql, const uint64_t* qo, uin
     ops_off[i + 1] = ops_off[i] + b.n + (so[j.subject + 1] - so[j.subject]);
   }
   const uint64_t ooff = ops_off[n];
-  set_exact_matrix(sc.scores);
   DevArr<Band> db_(n);
   DevArr<ExactOut> dout(n);
   DevArr<uint32_t> dops(ooff + 1);
@@ -455,7 +482,6 @@ int drg_extend_span_scores(drg_ctx* c, const uint8_t* ql, const uint64_t* qo, ui
     b.q0 = 0;
     b.n = (uint32_t)(qo[j.query + 1] - qo[j.query]);
   }
-  set_exact_matrix(sc.scores);
   DevArr<Band> db_(n);
   DevArr<int32_t> ds(n);
   DevArr<int64_t> cnt(2);
@@ -491,6 +517,14 @@ int drg_batch_create(drg_ctx* c, const uint8_t* letters, const uint64_t* offsets
   if (!c || !offsets || !out) return DRG_ERR_INVALID;
   API_BEGIN(c)
   *out = make_batch(c, letters, offsets, query, frame, n);
+  API_END(c)
+}
+
+int drg_batch_create_requests(drg_ctx* c, const uint8_t* letters, const uint64_t* offsets, const uint32_t* query,
+                              const uint8_t* frame, const uint32_t* request, uint64_t n, drg_batch** out) {
+  if (!c || !offsets || !out || (n && !request)) return DRG_ERR_INVALID;
+  API_BEGIN(c)
+  *out = make_batch(c, letters, offsets, query, frame, n, request);
   API_END(c)
 }
 

@@ -30,6 +30,9 @@ constexpr int kAlpha = 25;
 // Code the kernels use for positions outside a sequence; it scores kSentinelScore
 // against everything so that cells there can never raise a score.
 constexpr int kSentinel = 25;
+// Constant-memory banks: one per live context, so that contexts searching with
+// different presets or matrices at the same time keep separate tables.
+constexpr int kConstSlots = 8;
 constexpr int kSentinelScore = -64;
 
 // Grow-only device allocation owned by a context; contents are not preserved
@@ -113,6 +116,8 @@ struct SeedParams {
   uint64_t size;           // reduction size
   double cut;              // complexity cut (natural log units)
   double lnfact[33];       // ln n!, summed in the reference's order
+  int shape_shift;         // seed key = request << request_shift | shape << shape_shift | key
+  int request_shift;
 };
 
 }  // namespace drg

@@ -12,6 +12,7 @@
 
 struct drg_ctx {
   int device = 0;
+  int slot = -1;                // constant-memory bank of this context (kConstSlots of them)
   cudaStream_t stream = nullptr;
   cudaStream_t side = nullptr;  // concurrent launches (wide-band classes)
   cudaMemPool_t pool = nullptr;  // resident databases and batches (kept across calls)
@@ -28,6 +29,7 @@ struct drg_ctx {
   drg::DevBuf tband, task_size, task_off, trace, rev, ex_bands, ops_off, trace_out, task_max;
   drg::DevBuf sw_tasks_u, task_key, task_key_s, task_val, task_val_s, best_row, band_jobs_u, band_jobs, sw_rows, sw_rows_s,
       sw_keys_r, sw_order_r;
+  drg::DevBuf bj_key, bj_key_s, bj_val, bj_val_s, bj_size, bj_off, bj_max, ops_cnt, ops_coff, ops_compact;
   drg::HostBuf h_stage;
   cudaEvent_t ev[16] = {};
   drg_run_stats last{};
@@ -48,6 +50,7 @@ struct drg_batch {
   uint8_t* letters = nullptr;
   uint64_t* offsets = nullptr;
   uint32_t* owner = nullptr;
+  uint32_t* request = nullptr;  // device: request of each target (null: one request)
   std::vector<uint64_t> h_offsets;
   std::vector<uint8_t> h_letters;
   std::vector<uint32_t> query;
@@ -74,7 +77,7 @@ void search(drg_ctx* ctx, const drg_db* db, const drg_batch* b, const drg_search
 // Device residency helpers.
 drg_db* make_db(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offsets, uint64_t n);
 drg_batch* make_batch(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offsets, const uint32_t* query,
-                      const uint8_t* frame, uint64_t n);
+                      const uint8_t* frame, uint64_t n, const uint32_t* request = nullptr);
 void free_db(drg_db* db);
 void free_batch(drg_batch* b);
 }  // namespace drg

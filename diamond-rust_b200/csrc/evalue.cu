@@ -8,6 +8,8 @@
 // margin of 1e-9 (orders of magnitude above the error of either libm).  A
 // pair that meets an undecided band is handed back to the host, which redoes
 // its walk with the exact host statistics.
+#include <mutex>
+
 #include "kernels.h"
 
 namespace drg {
@@ -17,17 +19,23 @@ namespace {
 }  // namespace
 
 __constant__ double c_xlt1[20], c_x15[25], c_x510[20], c_p8[6], c_q8[7], c_ser[10];
-static bool g_alp_tables_ready = false;
+// The tables are the same for every search: copied once per device, with a
+// blocking copy under a lock, before any context's first E-value launch.
+static std::mutex g_alp_mutex;
+static bool g_alp_ready[64] = {};
 
-void upload_alp_tables(cudaStream_t st) {
-  if (g_alp_tables_ready) return;
-  DRG_CUDA(cudaMemcpyToSymbolAsync(c_xlt1, kErfcXlt1, sizeof(kErfcXlt1), 0, cudaMemcpyHostToDevice, st));
-  DRG_CUDA(cudaMemcpyToSymbolAsync(c_x15, kErfcX15, sizeof(kErfcX15), 0, cudaMemcpyHostToDevice, st));
-  DRG_CUDA(cudaMemcpyToSymbolAsync(c_x510, kErfcX510, sizeof(kErfcX510), 0, cudaMemcpyHostToDevice, st));
-  DRG_CUDA(cudaMemcpyToSymbolAsync(c_p8, kErfc8P, sizeof(kErfc8P), 0, cudaMemcpyHostToDevice, st));
-  DRG_CUDA(cudaMemcpyToSymbolAsync(c_q8, kErfc8Q, sizeof(kErfc8Q), 0, cudaMemcpyHostToDevice, st));
-  DRG_CUDA(cudaMemcpyToSymbolAsync(c_ser, kLogErfcSeries, sizeof(kLogErfcSeries), 0, cudaMemcpyHostToDevice, st));
-  g_alp_tables_ready = true;
+void upload_alp_tables(cudaStream_t) {
+  int dev = 0;
+  DRG_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(g_alp_mutex);
+  if (dev < 0 || dev >= 64 || g_alp_ready[dev]) return;
+  DRG_CUDA(cudaMemcpyToSymbol(c_xlt1, kErfcXlt1, sizeof(kErfcXlt1)));
+  DRG_CUDA(cudaMemcpyToSymbol(c_x15, kErfcX15, sizeof(kErfcX15)));
+  DRG_CUDA(cudaMemcpyToSymbol(c_x510, kErfcX510, sizeof(kErfcX510)));
+  DRG_CUDA(cudaMemcpyToSymbol(c_p8, kErfc8P, sizeof(kErfc8P)));
+  DRG_CUDA(cudaMemcpyToSymbol(c_q8, kErfc8Q, sizeof(kErfc8Q)));
+  DRG_CUDA(cudaMemcpyToSymbol(c_ser, kLogErfcSeries, sizeof(kLogErfcSeries)));
+  g_alp_ready[dev] = true;
 }
 
 namespace {
@@ -105,16 +113,20 @@ __device__ double alp_evalue_dev(const AlpDev& A, int raw, uint64_t qlen, uint64
   return le > 700.0 ? INFINITY : exp(le) * (double)db / m;
 }
 
+// sum over rows i = 1..n of clamp(i - d0, 0, m) - clamp(i - d1, 0, m) + 1, the
+// reference's row ranges (gapped.rs:82-93), in closed form: with
+// G(t) = sum_{x=0..t} clamp(x, 0, m), sum_{i=1..n} clamp(i - d, 0, m) is
+// G(n - d) - G(-d).
+__host__ __device__ __forceinline__ int64_t clamp_prefix(int64_t t, int64_t m) {
+  if (t < 0) return 0;
+  if (t <= m) return t * (t + 1) / 2;
+  return m * (m + 1) / 2 + (t - m) * m;
+}
 __host__ __device__ uint64_t band_cells(uint32_t n, uint32_t m, int32_t d0, int32_t d1) {
-  // sum over rows i = 1..n of clamp(i - d0, 0, m) - clamp(i - d1, 0, m) + 1
-  uint64_t cells = 0;
-  for (int64_t i = 1; i <= (int64_t)n; ++i) {
-    int64_t lo = i - d1, hi = i - d0;
-    lo = lo < 0 ? 0 : (lo > (int64_t)m ? (int64_t)m : lo);
-    hi = hi < 0 ? 0 : (hi > (int64_t)m ? (int64_t)m : hi);
-    cells += (uint64_t)(hi - lo + 1);
-  }
-  return cells;
+  const int64_t N = n, M = m;
+  const int64_t s0 = clamp_prefix(N - d0, M) - clamp_prefix(-(int64_t)d0, M);
+  const int64_t s1 = clamp_prefix(N - d1, M) - clamp_prefix(-(int64_t)d1, M);
+  return (uint64_t)(s0 - s1 + N);
 }
 uint64_t band_cells_host(uint32_t n, uint32_t m, int32_t d0, int32_t d1) { return band_cells(n, m, d0, d1); }
 

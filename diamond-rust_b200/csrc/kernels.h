@@ -8,22 +8,29 @@
 namespace drg {
 
 // ---- seeds (seed_kernels.cu) ----------------------------------------------
-void upload_seed_params(const ShapeTable& shapes, const SeedParams& p, cudaStream_t st);
+// Shape table and seed parameters into constant bank `slot` (the context's).
+void upload_seed_params(const ShapeTable& shapes, const SeedParams& p, int slot, cudaStream_t st);
 // seq index of every letter: out[g] = i with offsets[i] <= g < offsets[i+1].
 void launch_letter_owner(const uint64_t* offsets, uint64_t n_seqs, uint64_t letter_lo, uint64_t letter_hi,
                          uint32_t* out, cudaStream_t st);
 // Enumerate seeds of letters [letter_lo, letter_hi) for shapes [0, n_shapes):
-// keys[(g - letter_lo) * n_shapes + s] = s << 42 | key, or ~0 when no seed.
+// keys[(g - letter_lo) * n_shapes + s] = request << request_shift |
+// s << shape_shift | key (shifts from the search's SeedParams), or ~0 when no
+// seed.  request (per sequence, optional) tags query seeds with the request
+// their target belongs to, so that the join cap counts the query occurrences
+// of each request on its own.
 void launch_seed_enum(const uint8_t* letters, const uint64_t* offsets, const uint32_t* owner, uint64_t letter_lo,
-                      uint64_t letter_hi, int n_shapes, uint64_t* keys, uint32_t* vals, cudaStream_t st);
+                      uint64_t letter_hi, int n_shapes, uint64_t* keys, uint32_t* vals, int slot, cudaStream_t st,
+                      const uint32_t* request = nullptr);
 constexpr uint64_t kNoSeed = ~0ull;
-constexpr int kShapeShift = 42;
+constexpr uint32_t kMaxRequests = 65535;  // request ids of one batch
 
 // For each query run u (unique key, count, start): the reference run [lo, hi)
-// with the same key and the number of hits it yields under the expansion cap.
+// with the same key (query key & key_mask) and the number of hits it yields
+// under the expansion cap.
 void launch_join_count(const uint64_t* run_keys, const uint32_t* run_counts, uint64_t n_runs,
                        const uint64_t* ref_keys, uint64_t n_ref, uint64_t max_expand, uint32_t* run_rlo,
-                       uint32_t* run_rcount, uint64_t* run_hits, cudaStream_t st);
+                       uint32_t* run_rcount, uint64_t* run_hits, uint64_t key_mask, cudaStream_t st);
 
 // Layout of the packed 64-bit hit key (target, subject, diag + doff, spos).
 struct HitKeyLayout {
@@ -62,7 +69,7 @@ void launch_join_expand(const JoinExpandArgs& a, cudaStream_t st);
 
 // ---- ungapped (ungapped_kernels.cu) -----------------------------------------
 // Scores (25x25, int8) in constant memory for X-drop and the band stage.
-void upload_score_matrix(const int8_t* scores625, cudaStream_t st);
+void upload_score_matrix(const int8_t* scores625, int slot, cudaStream_t st);
 
 struct SegmentOut {  // ungapped.rs:11-17 plus the hit key it came from
   uint32_t q_start, s_start, len;
@@ -84,6 +91,7 @@ struct XdropArgs {
   const uint64_t* s_offsets;
   int xdrop;
   int cutoff;
+  int slot;          // constant bank of the score matrix
   SegmentOut* seg;   // indexed like hits
   uint8_t* keep;     // 1 when hit i produced a kept segment
   unsigned long long* xdrop_count;
@@ -92,7 +100,7 @@ void launch_xdrop_runs(const XdropArgs& a, cudaStream_t st);
 
 // Plain ungapped::xdrop for explicit anchors (stage entry point).
 void launch_xdrop_jobs(const drg_xdrop_job* jobs, uint64_t n, const uint8_t* q_letters, const uint64_t* q_offsets,
-                       const uint8_t* s_letters, const uint64_t* s_offsets, int xdrop, drg_segment* out,
+                       const uint8_t* s_letters, const uint64_t* s_offsets, int xdrop, drg_segment* out, int slot,
                        cudaStream_t st);
 
 // Band record (search.rs:206-230 + gapped_hsp window, search.rs:303-312).
@@ -201,9 +209,10 @@ constexpr int kSwMinWidth = 17;   // narrower bands use the exact kernel
 constexpr int kSwC0 = 136, kSwC1 = 272, kSwC2 = 544, kSwC3 = 1700;
 constexpr int kSwClassMax[4] = {kSwC0, kSwC1, kSwC2, kSwC3};  // 4, 2, 1, 1 warps per block
 constexpr int kSwMaxWidth = 1700;                       // wider bands use the exact kernel
+constexpr int kSwBandMinWidth = kSwC1 + 1;  // score pass: wider bands run one warp per band
 constexpr int kSwClasses = 4;
 int sw_width_class(int width);  // 0..3, or -1 for the exact kernel
-void launch_sw_class(const SwScoreArgs& a, int cls, bool trace, cudaStream_t st);
+void launch_sw_class(const SwScoreArgs& a, int cls, cudaStream_t st);  // score mode
 void launch_sw_walk(const SwWalkArgs& a, cudaStream_t st);
 
 // ---- exact DP with traceback (sw_exact.cu) ----------------------------------
@@ -224,14 +233,10 @@ struct ExactOut {
 };
 // scratch bytes a job needs (trace bytes + four int32 rows of max width)
 uint64_t exact_scratch_bytes(uint32_t n, uint32_t m, int32_t d0, int32_t d1, bool trace);
-void set_exact_matrix(const int8_t* scores625);
-// Same kernel with the substitution scores passed per launch (no shared host state).
+// The substitution scores travel with each launch (no shared host state).
 void launch_sw_exact_with_matrix(const ExactJob* jobs, uint64_t n_jobs, int gap_open, int gap_extend, bool trace,
                                  uint8_t* scratch, uint32_t* ops, ExactOut* out, const int8_t* scores625,
                                  cudaStream_t st);
-void launch_sw_exact(const ExactJob* jobs, uint64_t n_jobs, int gap_open, int gap_extend, bool trace,
-                     uint8_t* scratch, uint32_t* ops, ExactOut* out, cudaStream_t st);
-
 // ---- E-value gate (evalue.cu) ---------------------------------------------
 struct AlpDev {
   double lambda, k, ln_k, a, b, alpha, beta, sigma, tau, v_thr, c_thr;

@@ -114,6 +114,19 @@ __host__ __device__ __forceinline__ int sw_class_of(uint32_t w) {
   return w <= (uint32_t)kSwC0 ? 0 : (w <= (uint32_t)kSwC1 ? 1 : (w <= (uint32_t)kSwC2 ? 2 : 3));
 }
 
+constexpr uint64_t kWideKey = 1ull << 63;
+
+// Number of sorted keys below `bound`.
+__global__ void k_count_below(const uint64_t* keys, uint64_t n, uint64_t bound, int64_t* out) {
+  uint64_t lo = 0, hi = n;
+  while (lo < hi) {
+    const uint64_t m = (lo + hi) >> 1;
+    if (keys[m] < bound) lo = m + 1;
+    else hi = m;
+  }
+  *out = (int64_t)lo;
+}
+
 // Classify bands for the packed kernel and build its two sort keys:
 //  key  (target, window start, width) << 16, or ~0 for the exact kernel;
 //  rows (first-row strip bucket, last row), the last row descending in odd
@@ -131,7 +144,11 @@ __global__ void k_sw_keys(const Band* bands, uint64_t n, const uint64_t* s_offse
   int64_t mn = m < (int64_t)b.n ? m : (int64_t)b.n;
   bool fast = W >= kSwMinWidth && W <= kSwMaxWidth && (int64_t)max_score * mn <= 32000 && rs <= re &&
               b.target < (1u << 21) && b.q0 < 65536 && re < 65536;
-  keys[i] = fast ? ((uint64_t)b.target << 43) | ((uint64_t)b.q0 << 27) | ((uint64_t)W << 16) : ~0ull;
+  // wide bands: after every narrow band, before the exact kernel's
+  const bool wide = fast && W >= kSwBandMinWidth;
+  keys[i] = !fast ? ~0ull
+                  : wide ? (kWideKey | ((uint64_t)W << 16))
+                         : ((uint64_t)b.target << 43) | ((uint64_t)b.q0 << 27) | ((uint64_t)W << 16);
   const uint32_t bucket = fast ? (uint32_t)(rs >> 4) : 0xFFFFu;
   const uint32_t last = fast ? (uint32_t)re : 0u;
   rows[i] = (bucket << 16) | ((bucket & 1) ? 0xFFFFu - last : last);
@@ -202,12 +219,6 @@ __global__ void k_sw_fill_tasks(const uint32_t* starts, uint64_t n_tasks, const 
   }
 }
 
-__global__ void k_task_trace_size(const SwTask* tasks, uint64_t n, uint64_t* size) {
-  uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (t < n) size[t] = (uint64_t)tasks[t].n_strips * (tasks[t].width + 16ull) * 32ull;
-  else if (t == n) size[t] = 0;
-}
-
 __global__ void k_gather_tasks(const SwTask* in, const uint32_t* idx, uint64_t n, SwTask* out) {
   uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (t < n) out[t] = in[idx[t]];
@@ -234,9 +245,19 @@ __global__ void k_task_steps(const SwTask* tasks, uint64_t n, unsigned long long
   atomicMax(mx + sw_class_of(k.width), (unsigned long long)k.n_strips * (k.width + 16ull));
 }
 
-__global__ void k_set_trace_off(SwTask* tasks, const uint64_t* off, uint64_t n) {
-  uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (t < n) tasks[t].trace_off = off[t];
+// Ops of the traced bands, compacted in band order (each band owns n + m slots).
+__global__ void k_ops_count(const ExactOut* out, uint64_t n, uint64_t* cnt) {
+  uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (k < n) cnt[k] = out[k].n_ops;
+  else if (k == n) cnt[k] = 0;
+}
+__global__ void k_compact_ops(const uint32_t* ops, const uint64_t* ops_off, const ExactOut* out,
+                              const uint64_t* coff, uint64_t n, uint32_t* dst) {
+  uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const uint32_t* src = ops + ops_off[k];
+  uint32_t* o = dst + coff[k];
+  for (uint32_t i = 0; i < out[k].n_ops; ++i) o[i] = src[i];
 }
 
 // Jobs of the one-warp-per-band kernel for the first n bands of the sorted
@@ -339,6 +360,68 @@ __global__ void k_gather_bands(const uint32_t* idx, uint64_t n, const Band* band
 //  score mode (trace == false): scores[i] = best score (0 = None).
 //  trace mode: out[i] and the band's ops at h_ops_off[i] in ops (n + m slots
 //  per band), the same records the exact kernel produces.
+namespace {
+
+// Jobs of the one-warp-per-band kernel for n bands (order[k] indexes bands),
+// longest first, with their trace offsets when trace is set.
+struct BandJobs {
+  SwBandJob* jobs = nullptr;
+  uint64_t n = 0;
+  int max_width = 0;
+  uint64_t trace_words = 0;
+};
+BandJobs make_band_jobs(drg_ctx* c, const uint32_t* order, const uint64_t* keys, uint64_t n, const Band* bc,
+                        const uint64_t* s_offsets, bool trace) {
+  BandJobs r;
+  r.n = n;
+  if (n == 0) return r;
+  SwBandJob* jobs_u = c->band_jobs_u.as<SwBandJob>(n);
+  r.jobs = c->band_jobs.as<SwBandJob>(n);
+  uint64_t* key = c->bj_key.as<uint64_t>(n);
+  uint64_t* key_s = c->bj_key_s.as<uint64_t>(n);
+  uint32_t* val = c->bj_val.as<uint32_t>(n);
+  uint32_t* val_s = c->bj_val_s.as<uint32_t>(n);
+  unsigned long long* dmaxw = c->bj_max.as<unsigned long long>(1);
+  DRG_CUDA(cudaMemsetAsync(dmaxw, 0, sizeof(unsigned long long), c->stream));
+  count_launch();
+  k_band_jobs<<<ceil_div(n, 256), 256, 0, c->stream>>>(order, keys, n, bc, s_offsets, jobs_u, key, val, dmaxw);
+  cub_call(c, [&](void* t, size_t& b) {
+    return cub::DeviceRadixSort::SortPairs(t, b, key, key_s, val, val_s, (int64_t)n, 0, 64, c->stream);
+  });
+  uint64_t* size = c->bj_size.as<uint64_t>(n + 1);
+  uint64_t* off = c->bj_off.as<uint64_t>(n + 1);
+  count_launch();
+  k_gather_band_jobs<<<ceil_div(n + 1, 256), 256, 0, c->stream>>>(jobs_u, val_s, n, r.jobs, size);
+  if (trace) {
+    cub_call(c, [&](void* t, size_t& b) {
+      return cub::DeviceScan::ExclusiveSum(t, b, size, off, (int64_t)n + 1, c->stream);
+    });
+    count_launch();
+    k_set_band_trace_off<<<ceil_div(n, 256), 256, 0, c->stream>>>(r.jobs, off, n);
+    r.trace_words = fetch(c, off + n);
+  }
+  r.max_width = (int)fetch(c, dmaxw);
+  return r;
+}
+
+SwBandArgs band_args(const Band* bc, const BandJobs& bj, const DevSeqs& qs, const DevSeqs& s, const Scoring& scr) {
+  SwBandArgs ba{};
+  ba.bands = bc;
+  ba.jobs = bj.jobs;
+  ba.lo = 0;
+  ba.hi = bj.n;
+  ba.q_letters = qs.letters;
+  ba.q_offsets = qs.offsets;
+  ba.s_letters = s.letters;
+  ba.s_offsets = s.offsets;
+  ba.gap_open = scr.gap_open;
+  ba.gap_extend = scr.gap_extend;
+  std::memcpy(ba.scores625, scr.scores, 625);
+  return ba;
+}
+
+}  // namespace
+
 void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, const DevSeqs& s,
                const Scoring& scr, bool trace, int32_t* scores, int32_t* best_row, ExactOut* out, uint32_t* ops,
                const uint64_t* d_ops_off, const std::vector<uint64_t>* h_ops_off, drg_run_stats& st,
@@ -372,45 +455,11 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
   }
   if (n_fast > 0 && trace) {
     // traceback: one warp per band (few, long bands)
-    SwBandJob* jobs_u = c->band_jobs_u.as<SwBandJob>(n_fast);
-    SwBandJob* jobs = c->band_jobs.as<SwBandJob>(n_fast);
-    uint64_t* tkey = c->task_key.as<uint64_t>(n_fast);
-    uint64_t* tkey_s = c->task_key_s.as<uint64_t>(n_fast);
-    uint32_t* tval = c->task_val.as<uint32_t>(n_fast);
-    uint32_t* tval_s = c->task_val_s.as<uint32_t>(n_fast);
-    unsigned long long* dmaxw = c->task_max.as<unsigned long long>(2 * kSwClasses);
-    DRG_CUDA(cudaMemsetAsync(dmaxw, 0, sizeof(unsigned long long), c->stream));
-    count_launch();
-    k_band_jobs<<<ceil_div(n_fast, 256), 256, 0, c->stream>>>(swos, swks, n_fast, bc, s.offsets, jobs_u, tkey, tval,
-                                                               dmaxw);
-    cub_call(c, [&](void* t, size_t& b) {
-      return cub::DeviceRadixSort::SortPairs(t, b, tkey, tkey_s, tval, tval_s, (int64_t)n_fast, 0, 64, c->stream);
-    });
-    uint64_t* tsize = c->task_size.as<uint64_t>(n_fast + 1);
-    uint64_t* toff = c->task_off.as<uint64_t>(n_fast + 1);
-    count_launch();
-    k_gather_band_jobs<<<ceil_div(n_fast + 1, 256), 256, 0, c->stream>>>(jobs_u, tval_s, n_fast, jobs, tsize);
-    cub_call(c, [&](void* t, size_t& b) {
-      return cub::DeviceScan::ExclusiveSum(t, b, tsize, toff, (int64_t)n_fast + 1, c->stream);
-    });
-    count_launch();
-    k_set_band_trace_off<<<ceil_div(n_fast, 256), 256, 0, c->stream>>>(jobs, toff, n_fast);
-    const uint64_t total = fetch(c, toff + n_fast);
-    const int max_w = (int)fetch(c, dmaxw);
-    SwBandArgs ba{};
-    ba.bands = bc;
-    ba.jobs = jobs;
-    ba.lo = 0;
-    ba.hi = n_fast;
-    ba.q_letters = qs.letters;
-    ba.q_offsets = qs.offsets;
-    ba.s_letters = s.letters;
-    ba.s_offsets = s.offsets;
-    ba.gap_open = scr.gap_open;
-    ba.gap_extend = scr.gap_extend;
-    ba.trace = c->trace.as<uint2>(total);
+    const BandJobs bj = make_band_jobs(c, swos, swks, n_fast, bc, s.offsets, true);
+    SwBandArgs ba = band_args(bc, bj, qs, s, scr);
+    ba.trace = c->trace.as<uint2>(bj.trace_words);
     ba.tband = tb;
-    std::memcpy(ba.scores625, scr.scores, 625);
+    const int max_w = bj.max_width;
     cudaEvent_t e0, e1;
     DRG_CUDA(cudaEventCreate(&e0));
     DRG_CUDA(cudaEventCreate(&e1));
@@ -439,38 +488,60 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
     cudaEventDestroy(e1);
     st.ms_trace_kernel += ms;
   } else if (n_fast > 0) {
-    uint32_t* gstart = c->idx.as<uint32_t>(n_fast + 1);
-    count_launch();
-    k_sw_group_start<<<ceil_div(n_fast, 256), 256, 0, c->stream>>>(swks, n_fast, gstart);
-    cub_call(c, [&](void* t, size_t& b) {
-      return cub::DeviceScan::InclusiveScan(t, b, gstart, gstart, cub::Max(), (int64_t)n_fast, c->stream);
-    });
-    count_launch();
-    k_sw_task_flags<<<ceil_div(n_fast, 256), 256, 0, c->stream>>>(gstart, n_fast, flags);
-    uint32_t* tstart = c->sel_idx.as<uint32_t>(n_fast + 1);
-    const uint64_t n_tasks = select_indices(c, flags, n_fast, tstart, d_count);
-    SwTask* tasks_u = c->sw_tasks_u.as<SwTask>(n_tasks);
-    SwTask* tasks = c->sw_tasks.as<SwTask>(n_tasks);
-    uint64_t* tkey = c->task_key.as<uint64_t>(n_tasks);
-    uint64_t* tkey_s = c->task_key_s.as<uint64_t>(n_tasks);
-    uint32_t* tval = c->task_val.as<uint32_t>(n_tasks);
-    uint32_t* tval_s = c->task_val_s.as<uint32_t>(n_tasks);
-    count_launch();
-    k_sw_fill_tasks<<<ceil_div(n_tasks, 128), 128, 0, c->stream>>>(tstart, n_tasks, swks, n_fast, swos, bc,
-                                                                    s.offsets, trace, tasks_u, tkey, tval, nullptr,
-                                                                    cells_gpu);
-    // by width class, longest warps first within a class
-    cub_call(c, [&](void* t, size_t& b) {
-      return cub::DeviceRadixSort::SortPairs(t, b, tkey, tkey_s, tval, tval_s, (int64_t)n_tasks, 0, 64, c->stream);
-    });
-    count_launch();
-    k_gather_tasks<<<ceil_div(n_tasks, 256), 256, 0, c->stream>>>(tasks_u, tval_s, n_tasks, tasks);
-    count_launch();
-    // task_max holds the per-class step maxima, then the class bounds
-    int64_t* dbounds = reinterpret_cast<int64_t*>(c->task_max.as<unsigned long long>(2 * kSwClasses)) + kSwClasses;
-    k_task_bounds<<<1, 1, 0, c->stream>>>(tasks, n_tasks, dbounds);
-    int64_t bounds[kSwClasses - 1];
-    DRG_CUDA(cudaMemcpyAsync(bounds, dbounds, sizeof(bounds), cudaMemcpyDeviceToHost, c->stream));
+    // score pass: warps of 32 narrow bands (packed inter-band kernel) and, on
+    // the side stream, one warp per band for the wide ones
+    const uint64_t n_narrow = [&] {
+      count_launch();
+      k_count_below<<<1, 1, 0, c->stream>>>(swks, n_fast, kWideKey, d_count);
+      return (uint64_t)fetch(c, d_count);
+    }();
+    const BandJobs wide = make_band_jobs(c, swos + n_narrow, swks + n_narrow, n_fast - n_narrow, bc, s.offsets,
+                                         false);
+    uint64_t n_tasks = 0;
+    SwTask* tasks = nullptr;
+    int64_t bounds[kSwClasses - 1] = {0, 0, 0};
+    if (n_narrow > 0) {
+      uint32_t* gstart = c->idx.as<uint32_t>(n_narrow + 1);
+      count_launch();
+      k_sw_group_start<<<ceil_div(n_narrow, 256), 256, 0, c->stream>>>(swks, n_narrow, gstart);
+      cub_call(c, [&](void* t, size_t& b) {
+        return cub::DeviceScan::InclusiveScan(t, b, gstart, gstart, cub::Max(), (int64_t)n_narrow, c->stream);
+      });
+      count_launch();
+      k_sw_task_flags<<<ceil_div(n_narrow, 256), 256, 0, c->stream>>>(gstart, n_narrow, flags);
+      uint32_t* tstart = c->sel_idx.as<uint32_t>(n_narrow + 1);
+      n_tasks = select_indices(c, flags, n_narrow, tstart, d_count);
+      SwTask* tasks_u = c->sw_tasks_u.as<SwTask>(n_tasks);
+      tasks = c->sw_tasks.as<SwTask>(n_tasks);
+      uint64_t* tkey = c->task_key.as<uint64_t>(n_tasks);
+      uint64_t* tkey_s = c->task_key_s.as<uint64_t>(n_tasks);
+      uint32_t* tval = c->task_val.as<uint32_t>(n_tasks);
+      uint32_t* tval_s = c->task_val_s.as<uint32_t>(n_tasks);
+      count_launch();
+      k_sw_fill_tasks<<<ceil_div(n_tasks, 128), 128, 0, c->stream>>>(tstart, n_tasks, swks, n_narrow, swos, bc,
+                                                                      s.offsets, false, tasks_u, tkey, tval, nullptr,
+                                                                      cells_gpu);
+      // by width class, longest warps first within a class
+      cub_call(c, [&](void* t, size_t& b) {
+        return cub::DeviceRadixSort::SortPairs(t, b, tkey, tkey_s, tval, tval_s, (int64_t)n_tasks, 0, 64,
+                                               c->stream);
+      });
+      count_launch();
+      k_gather_tasks<<<ceil_div(n_tasks, 256), 256, 0, c->stream>>>(tasks_u, tval_s, n_tasks, tasks);
+      // task_max holds the per-class step maxima, then the class bounds
+      int64_t* dbounds = reinterpret_cast<int64_t*>(c->task_max.as<unsigned long long>(2 * kSwClasses)) + kSwClasses;
+      count_launch();
+      k_task_bounds<<<1, 1, 0, c->stream>>>(tasks, n_tasks, dbounds);
+      DRG_CUDA(cudaMemcpyAsync(bounds, dbounds, sizeof(bounds), cudaMemcpyDeviceToHost, c->stream));
+    }
+    unsigned long long* dmax = c->task_max.as<unsigned long long>(2 * kSwClasses);
+    DRG_CUDA(cudaMemsetAsync(dmax, 0, kSwClasses * sizeof(unsigned long long), c->stream));
+    if (n_tasks > 0) {
+      count_launch();
+      k_task_steps<<<ceil_div(n_tasks, 256), 256, 0, c->stream>>>(tasks, n_tasks, dmax);
+    }
+    unsigned long long hmax[kSwClasses];
+    DRG_CUDA(cudaMemcpyAsync(hmax, dmax, sizeof(hmax), cudaMemcpyDeviceToHost, c->stream));
     DRG_CUDA(cudaStreamSynchronize(c->stream));
     SwScoreArgs sa{};
     sa.bands = bc;
@@ -484,86 +555,59 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
     sa.gap_extend = scr.gap_extend;
     sa.score = scores;
     sa.best_row = best_row;
-    sa.tband = tb;
     std::memcpy(sa.scores625, scr.scores, 625);
-    if (trace) {
-      uint64_t* tsize = c->task_size.as<uint64_t>(n_tasks + 1);
-      uint64_t* toff = c->task_off.as<uint64_t>(n_tasks + 1);
-      count_launch();
-      k_task_trace_size<<<ceil_div(n_tasks + 1, 256), 256, 0, c->stream>>>(tasks, n_tasks, tsize);
-      cub_call(c, [&](void* t, size_t& b) {
-        return cub::DeviceScan::ExclusiveSum(t, b, tsize, toff, (int64_t)n_tasks + 1, c->stream);
-      });
-      count_launch();
-      k_set_trace_off<<<ceil_div(n_tasks, 256), 256, 0, c->stream>>>(tasks, toff, n_tasks);
-      const uint64_t total = fetch(c, toff + n_tasks);
-      sa.trace = c->trace.as<uint2>(total);
-    }
     uint64_t lo[kSwClasses], hi[kSwClasses];
     for (int k = 0; k < kSwClasses; ++k) {
       lo[k] = k == 0 ? 0 : (uint64_t)bounds[k - 1];
       hi[k] = k == kSwClasses - 1 ? n_tasks : (uint64_t)bounds[k];
     }
-    unsigned long long* dmax = c->task_max.as<unsigned long long>(2 * kSwClasses);
-    DRG_CUDA(cudaMemsetAsync(dmax, 0, kSwClasses * sizeof(unsigned long long), c->stream));
-    count_launch();
-    k_task_steps<<<ceil_div(n_tasks, 256), 256, 0, c->stream>>>(tasks, n_tasks, dmax);
-    unsigned long long hmax[kSwClasses];
-    DRG_CUDA(cudaMemcpyAsync(hmax, dmax, sizeof(hmax), cudaMemcpyDeviceToHost, c->stream));
-    // The bulk class runs on the main stream while the wide classes run on the
-    // side stream, so a few long wide-band warps do not serialise behind it.
-    cudaEvent_t ev[2 * kSwClasses + 1];
+    // The bulk class runs on the main stream; the wider classes and the wide
+    // bands run on the side stream, queued first so that the long warps start
+    // early and the pass ends on the bulk class's shortest tasks.
+    cudaEvent_t ev[2 * kSwClasses + 3];
     for (auto& e : ev) DRG_CUDA(cudaEventCreate(&e));
-    const int fork = 2 * kSwClasses;
+    const int fork = 2 * kSwClasses, wide0 = fork + 1, wide1 = fork + 2;
     DRG_CUDA(cudaEventRecord(ev[fork], c->stream));
     DRG_CUDA(cudaStreamWaitEvent(c->side, ev[fork], 0));
-    for (int cls = 0; cls < kSwClasses; ++cls) {
+    auto launch_cls = [&](int cls) {
       cudaStream_t sc = cls == 0 ? c->stream : c->side;
       sa.task_lo = lo[cls];
       sa.task_hi = hi[cls];
       DRG_CUDA(cudaEventRecord(ev[2 * cls], sc));
       if (hi[cls] > lo[cls]) {
-        launch_sw_class(sa, cls, trace, sc);
-        if (!trace) st.sw_launches += 1;
+        launch_sw_class(sa, cls, sc);
+        st.sw_launches += 1;
       }
       DRG_CUDA(cudaEventRecord(ev[2 * cls + 1], sc));
+    };
+    DRG_CUDA(cudaEventRecord(ev[wide0], c->side));
+    if (wide.n > 0) {
+      SwBandArgs ba = band_args(bc, wide, qs, s, scr);
+      ba.score = scores;
+      ba.best_row = best_row;
+      launch_sw_band(ba, wide.max_width, false, c->side);
+      st.sw_launches += 1;
     }
-    const int side_end = 2 * kSwClasses - 1;
+    DRG_CUDA(cudaEventRecord(ev[wide1], c->side));
+    for (int cls = kSwClasses - 1; cls >= 1; --cls) launch_cls(cls);
+    launch_cls(0);
+    const int side_end = 2 * 1 + 1;  // class 1 is the side stream's last launch
     DRG_CUDA(cudaStreamWaitEvent(c->stream, ev[side_end], 0));
     DRG_CUDA(cudaEventSynchronize(ev[1]));
     DRG_CUDA(cudaEventSynchronize(ev[side_end]));
-    float cls_ms[kSwClasses], side_span = 0;
+    float cls_ms[kSwClasses], side_span = 0, wide_ms = 0;
     for (int k = 0; k < kSwClasses; ++k) DRG_CUDA(cudaEventElapsedTime(&cls_ms[k], ev[2 * k], ev[2 * k + 1]));
     DRG_CUDA(cudaEventElapsedTime(&side_span, ev[fork], ev[side_end]));
+    DRG_CUDA(cudaEventElapsedTime(&wide_ms, ev[wide0], ev[wide1]));
     for (auto& e : ev) cudaEventDestroy(e);
-    const double kms = cls_ms[0] > side_span ? cls_ms[0] : side_span;  // wall of the concurrent launches
-    if (!trace) {
-      st.ms_sw_kernel += kms;
-      for (int k = 0; k < kSwClasses; ++k) {
-        st.ms_sw_class[k] += cls_ms[k];
-        st.sw_class_tasks[k] += hi[k] - lo[k];
-        if (hmax[k] > st.sw_class_max_steps[k]) st.sw_class_max_steps[k] = hmax[k];
-      }
-    } else {
-      st.ms_trace_kernel += kms;
+    st.ms_sw_kernel += cls_ms[0] > side_span ? cls_ms[0] : side_span;  // wall of the concurrent launches
+    for (int k = 0; k < kSwClasses; ++k) {
+      st.ms_sw_class[k] += cls_ms[k];
+      st.sw_class_tasks[k] += hi[k] - lo[k];
+      if (hmax[k] > st.sw_class_max_steps[k]) st.sw_class_max_steps[k] = hmax[k];
     }
-    if (trace) {
-      SwWalkArgs wa{};
-      wa.bands = bc;
-      wa.tband = tb;
-      wa.n_bands = n_bands;
-      wa.trace = sa.trace;
-      wa.q_letters = qs.letters;
-      wa.q_offsets = qs.offsets;
-      wa.s_letters = s.letters;
-      wa.s_offsets = s.offsets;
-      wa.ops_off = d_ops_off;
-      wa.rev = c->rev.as<uint8_t>((*h_ops_off)[n_bands] + 16);
-      wa.ops = ops;
-      wa.out = out;
-      std::memcpy(wa.scores625, scr.scores, 625);
-      launch_sw_walk(wa, c->stream);
-    }
+    st.ms_sw_wide += wide_ms;
+    st.sw_wide_bands += wide.n;
   }
   // the exact kernel for the bands the packed kernel did not settle
   count_launch();
@@ -626,6 +670,7 @@ struct Search {
   std::vector<ShapeCode> shapes;
   ReducedAlphabet red;
   double complexity_cut = 0;
+  int seed_key_bits = 48;  // sorted bits of a seed key (shape id and packed key)
   uint64_t index_chunks = 1;
   double evalue = 1e-3;
   uint64_t max_hsps = 1, max_targets = 25;
@@ -663,9 +708,20 @@ struct Search {
     p.size = (uint64_t)red.size;
     p.cut = complexity_cut;
     ln_factorial_table(p.lnfact);
-    upload_seed_params(t, p, c->stream);
-    upload_score_matrix(sc.scores, c->stream);
-    set_exact_matrix(sc.scores);
+    // key layout: the widest shape key, then the shape id (one spare bit, so
+    // that no valid key has all sorted bits set like "no seed"), then requests
+    int kb = 0;
+    for (const auto& sh : shapes) {
+      uint64_t mx = 1;
+      for (int k = 0; k < sh.weight; ++k) mx *= (uint64_t)red.size;
+      kb = std::max(kb, bits_for(mx - 1));
+    }
+    p.shape_shift = kb;
+    p.request_shift = kb + bits_for((uint64_t)shapes.size());
+    seed_key_bits = p.request_shift;
+    if (seed_key_bits + bits_for(kMaxRequests) > 64) throw Error(DRG_ERR_INVALID, "seed keys need more than 64 bits");
+    upload_seed_params(t, p, c->slot, c->stream);
+    upload_score_matrix(sc.scores, c->slot, c->stream);
     upload_alp_tables(c->stream);
   }
 
@@ -696,9 +752,10 @@ void Search::query_seeds(uint64_t* n_runs_out) {
   uint32_t* vals = c->q_vals.as<uint32_t>(N);
   uint64_t* keys_s = c->q_keys_s.as<uint64_t>(N);
   uint32_t* vals_s = c->q_vals_s.as<uint32_t>(N);
-  launch_seed_enum(q->letters, q->offsets, q->owner, 0, q->total, S, keys, vals, c->stream);
+  launch_seed_enum(q->letters, q->offsets, q->owner, 0, q->total, S, keys, vals, c->slot, c->stream, q->request);
+  const int key_bits = q->request ? 64 : seed_key_bits;  // request ids sit above the seed key
   cub_call(c, [&](void* t, size_t& b) {
-    return cub::DeviceRadixSort::SortPairs(t, b, keys, keys_s, vals, vals_s, (int64_t)N, 0, 48, c->stream);
+    return cub::DeviceRadixSort::SortPairs(t, b, keys, keys_s, vals, vals_s, (int64_t)N, 0, key_bits, c->stream);
   });
   int64_t nv = count_valid(c, keys_s, N, d_count);
   st.query_seeds = (uint64_t)nv;
@@ -730,9 +787,10 @@ void Search::chunk(uint64_t chunk_id, uint64_t c0, uint64_t c1, uint64_t n_runs)
   uint32_t* vals = c->r_vals.as<uint32_t>(N);
   uint64_t* keys_s = c->r_keys_s.as<uint64_t>(N);
   uint32_t* vals_s = c->r_vals_s.as<uint32_t>(N);
-  launch_seed_enum(db->letters, db->offsets, db->owner + lo, lo, hi, S, keys, vals, c->stream);
+  launch_seed_enum(db->letters, db->offsets, db->owner + lo, lo, hi, S, keys, vals, c->slot, c->stream);
   cub_call(c, [&](void* t, size_t& b) {
-    return cub::DeviceRadixSort::SortPairs(t, b, keys, keys_s, vals, vals_s, (int64_t)N, 0, 48, c->stream);
+    return cub::DeviceRadixSort::SortPairs(t, b, keys, keys_s, vals, vals_s, (int64_t)N, 0, seed_key_bits,
+                                           c->stream);
   });
   int64_t nr = count_valid(c, keys_s, N, d_count);
   st.ref_seeds += (uint64_t)nr;
@@ -741,7 +799,7 @@ void Search::chunk(uint64_t chunk_id, uint64_t c0, uint64_t c1, uint64_t n_runs)
   uint64_t* rhits = c->run_hits.as<uint64_t>(n_runs + 1);
   uint64_t* roff = c->run_hit_off.as<uint64_t>(n_runs + 1);
   launch_join_count(c->run_keys.as<uint64_t>(0), c->run_counts.as<uint32_t>(0), n_runs, keys_s, (uint64_t)nr, 4096,
-                    rlo, rcnt, rhits, c->stream);
+                    rlo, rcnt, rhits, (1ull << seed_key_bits) - 1, c->stream);
   count_launch();
   k_set_u64<<<1, 1, 0, c->stream>>>(rhits + n_runs, 0);
   cub_call(c, [&](void* t, size_t& b) {
@@ -807,6 +865,7 @@ void Search::chunk(uint64_t chunk_id, uint64_t c0, uint64_t c1, uint64_t n_runs)
   xa.seg = segs;
   xa.keep = keep;
   xa.xdrop_count = d_counters + 0;
+  xa.slot = c->slot;
   launch_xdrop_runs(xa, c->stream);
   uint64_t* sk = c->seg_keys.as<uint64_t>(n_u);
   SegmentOut* sc_ = c->segs_c.as<SegmentOut>(n_u);
@@ -1008,8 +1067,20 @@ void Search::finish(drg_result* out) {
     DevSeqs ss{db->letters, db->offsets, &db->h_offsets};
     run_bands(c, db_, nj, qs, ss, sc, true, nullptr, nullptr, dout, dops, doff, &ops_off, st, d_count,
               nullptr);
+    // only the ops the alignments use come back (each band has n + m slots)
+    uint64_t* cnt = c->ops_cnt.as<uint64_t>(nj + 1);
+    uint64_t* coff = c->ops_coff.as<uint64_t>(nj + 1);
+    count_launch();
+    k_ops_count<<<ceil_div(nj + 1, 256), 256, 0, c->stream>>>(dout, nj, cnt);
+    cub_call(c, [&](void* t, size_t& b) {
+      return cub::DeviceScan::ExclusiveSum(t, b, cnt, coff, (int64_t)nj + 1, c->stream);
+    });
+    const uint64_t n_used = fetch(c, coff + nj);
+    uint32_t* cops = c->ops_compact.as<uint32_t>(n_used + 1);
+    count_launch();
+    k_compact_ops<<<ceil_div(nj, 128), 128, 0, c->stream>>>(dops, doff, dout, coff, nj, cops);
     fetch_n(c, eo, dout, nj);
-    fetch_n(c, ops_all, dops, ops_off[nj]);
+    fetch_n(c, ops_all, cops, n_used);
     st.ms_trace += tm.stop();
   }
   auto t1 = std::chrono::steady_clock::now();
@@ -1050,7 +1121,7 @@ void Search::finish(drg_result* out) {
       o.ops_offset = ko;
       o.n_ops = r.n_ops;
       o.pad = 0;
-      std::memcpy(out->ops + ko, ops_all.data() + ops_off[k], r.n_ops * sizeof(uint32_t));
+      std::memcpy(out->ops + ko, ops_all.data() + ko, r.n_ops * sizeof(uint32_t));  // compacted in this order
       ko += r.n_ops;
     }
     out->target_offsets[t + 1] = h;
@@ -1155,7 +1226,7 @@ drg_db* make_db(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offsets, u
 }
 
 drg_batch* make_batch(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offsets, const uint32_t* query,
-                      const uint8_t* frame, uint64_t n) {
+                      const uint8_t* frame, uint64_t n, const uint32_t* request) {
   drg_batch* b = new drg_batch();
   b->ctx = ctx;
   b->n = n;
@@ -1182,6 +1253,12 @@ drg_batch* make_batch(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offs
       DRG_CUDA(cudaMemcpyAsync(b->letters, letters, b->total, cudaMemcpyHostToDevice, ctx->stream));
     DRG_CUDA(cudaMemcpyAsync(b->offsets, offsets, (n + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, ctx->stream));
     launch_letter_owner(b->offsets, n, 0, b->total, b->owner, ctx->stream);
+    if (request && n > 0) {  // per-request join accounting
+      for (uint64_t i = 0; i < n; ++i)
+        if (request[i] > kMaxRequests) throw Error(DRG_ERR_INVALID, "request id out of range");
+      pool_alloc(ctx, &b->request, n * sizeof(uint32_t));
+      DRG_CUDA(cudaMemcpyAsync(b->request, request, n * sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
+    }
     DRG_CUDA(cudaStreamSynchronize(ctx->stream));
   } catch (...) {
     free_batch(b);
@@ -1203,6 +1280,7 @@ void free_batch(drg_batch* b) {
   pool_free(b->ctx, b->letters);
   pool_free(b->ctx, b->offsets);
   pool_free(b->ctx, b->owner);
+  pool_free(b->ctx, b->request);
   delete b;
 }
 

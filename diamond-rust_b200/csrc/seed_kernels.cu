@@ -11,12 +11,16 @@
 
 namespace drg {
 
-__constant__ ShapeTable c_shapes;
-__constant__ SeedParams c_seed;
+// One bank per context slot, so that contexts searching with different
+// presets at the same time do not overwrite each other's tables.
+__constant__ ShapeTable c_shapes[kConstSlots];
+__constant__ SeedParams c_seed[kConstSlots];
 
-void upload_seed_params(const ShapeTable& shapes, const SeedParams& p, cudaStream_t st) {
-  DRG_CUDA(cudaMemcpyToSymbolAsync(c_shapes, &shapes, sizeof(ShapeTable), 0, cudaMemcpyHostToDevice, st));
-  DRG_CUDA(cudaMemcpyToSymbolAsync(c_seed, &p, sizeof(SeedParams), 0, cudaMemcpyHostToDevice, st));
+void upload_seed_params(const ShapeTable& shapes, const SeedParams& p, int slot, cudaStream_t st) {
+  DRG_CUDA(cudaMemcpyToSymbolAsync(c_shapes, &shapes, sizeof(ShapeTable), slot * sizeof(ShapeTable),
+                                   cudaMemcpyHostToDevice, st));
+  DRG_CUDA(cudaMemcpyToSymbolAsync(c_seed, &p, sizeof(SeedParams), slot * sizeof(SeedParams),
+                                   cudaMemcpyHostToDevice, st));
 }
 
 __global__ void k_letter_owner(const uint64_t* __restrict__ offsets, uint64_t n_seqs, uint64_t lo, uint64_t hi,
@@ -45,14 +49,16 @@ void launch_letter_owner(const uint64_t* offsets, uint64_t n_seqs, uint64_t lo, 
 // counts live in three 64-bit words (8 buckets x 8 bits each); the entropy is
 // lnfact[w] minus lnfact[c_b] for b = 0, 1, ... in bucket order, the order the
 // reference subtracts in, so the double result is identical.
-__device__ __forceinline__ bool seed_at(const uint8_t* __restrict__ p, int s, uint64_t* key_out) {
-  const int w = c_shapes.weight[s];
-  const uint64_t size = c_seed.size;
+__device__ __forceinline__ bool seed_at(const uint8_t* __restrict__ p, int s, int slot, uint64_t* key_out) {
+  const ShapeTable& shp = c_shapes[slot];
+  const SeedParams& sp = c_seed[slot];
+  const int w = shp.weight[s];
+  const uint64_t size = sp.size;
   uint64_t key = 0, c0 = 0, c1 = 0, c2 = 0;
   for (int k = 0; k < w; ++k) {
-    uint32_t l = p[c_shapes.pos[s][k]];
+    uint32_t l = p[shp.pos[s][k]];
     if (l >= 20) return false;
-    uint32_t b = c_seed.bucket[l];
+    uint32_t b = sp.bucket[l];
     if (b >= 24) return false;
     key = key * size + b;
     uint64_t inc = 1ull << (8 * (b & 7));
@@ -60,13 +66,13 @@ __device__ __forceinline__ bool seed_at(const uint8_t* __restrict__ p, int s, ui
     else if (b < 16) c1 += inc;
     else c2 += inc;
   }
-  const double cut = c_seed.cut;
+  const double cut = sp.cut;
   if (cut > 0.0) {
-    double e = c_seed.lnfact[w];
+    double e = sp.lnfact[w];
     for (int b = 0; b < (int)size; ++b) {
       uint64_t word = b < 8 ? c0 : (b < 16 ? c1 : c2);
       uint32_t c = (uint32_t)(word >> (8 * (b & 7))) & 0xffu;
-      if (c > 0) e = __dsub_rn(e, c_seed.lnfact[c]);
+      if (c > 0) e = __dsub_rn(e, sp.lnfact[c]);
     }
     if (!(e >= cut)) return false;
   }
@@ -76,7 +82,8 @@ __device__ __forceinline__ bool seed_at(const uint8_t* __restrict__ p, int s, ui
 
 __global__ void k_seed_enum(const uint8_t* __restrict__ letters, const uint64_t* __restrict__ offsets,
                             const uint32_t* __restrict__ owner, uint64_t lo, uint64_t hi, int n_shapes,
-                            uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+                            uint64_t* __restrict__ keys, uint32_t* __restrict__ vals,
+                            const uint32_t* __restrict__ request, int slot) {
   uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   uint64_t n = (hi - lo) * (uint64_t)n_shapes;
   if (t >= n) return;
@@ -85,27 +92,31 @@ __global__ void k_seed_enum(const uint8_t* __restrict__ letters, const uint64_t*
   uint32_t seq = owner[g - lo];
   uint64_t end = offsets[seq + 1];
   uint64_t key = 0;
-  bool ok = g + c_shapes.span[s] <= end && seed_at(letters + g, s, &key);
-  keys[t] = ok ? ((uint64_t)s << kShapeShift) | key : kNoSeed;
+  bool ok = g + c_shapes[slot].span[s] <= end && seed_at(letters + g, s, slot, &key);
+  const SeedParams& sp = c_seed[slot];
+  const uint64_t req = request ? (uint64_t)request[seq] << sp.request_shift : 0;
+  keys[t] = ok ? req | ((uint64_t)s << sp.shape_shift) | key : kNoSeed;
   vals[t] = (uint32_t)g;
 }
 
 void launch_seed_enum(const uint8_t* letters, const uint64_t* offsets, const uint32_t* owner, uint64_t lo,
-                      uint64_t hi, int n_shapes, uint64_t* keys, uint32_t* vals, cudaStream_t st) {
+                      uint64_t hi, int n_shapes, uint64_t* keys, uint32_t* vals, int slot, cudaStream_t st,
+                      const uint32_t* request) {
   uint64_t n = (hi - lo) * (uint64_t)n_shapes;
   if (n == 0) return;
   count_launch();
-  k_seed_enum<<<ceil_div(n, 256), 256, 0, st>>>(letters, offsets, owner, lo, hi, n_shapes, keys, vals);
+  k_seed_enum<<<ceil_div(n, 256), 256, 0, st>>>(letters, offsets, owner, lo, hi, n_shapes, keys, vals, request,
+                                                slot);
   DRG_CUDA(cudaGetLastError());
 }
 
 __global__ void k_join_count(const uint64_t* __restrict__ run_keys, const uint32_t* __restrict__ run_counts,
                              uint64_t n_runs, const uint64_t* __restrict__ ref_keys, uint64_t n_ref,
                              uint64_t max_expand, uint32_t* __restrict__ run_rlo, uint32_t* __restrict__ run_rcount,
-                             uint64_t* __restrict__ run_hits) {
+                             uint64_t* __restrict__ run_hits, uint64_t key_mask) {
   uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (u >= n_runs) return;
-  uint64_t key = run_keys[u];
+  const uint64_t key = run_keys[u] & key_mask;  // the query run's request does not take part
   uint64_t a = 0, b = n_ref;
   while (a < b) {  // lower bound
     uint64_t m = (a + b) >> 1;
@@ -128,11 +139,11 @@ __global__ void k_join_count(const uint64_t* __restrict__ run_keys, const uint32
 
 void launch_join_count(const uint64_t* run_keys, const uint32_t* run_counts, uint64_t n_runs,
                        const uint64_t* ref_keys, uint64_t n_ref, uint64_t max_expand, uint32_t* run_rlo,
-                       uint32_t* run_rcount, uint64_t* run_hits, cudaStream_t st) {
+                       uint32_t* run_rcount, uint64_t* run_hits, uint64_t key_mask, cudaStream_t st) {
   if (n_runs == 0) return;
   count_launch();
   k_join_count<<<ceil_div(n_runs, 256), 256, 0, st>>>(run_keys, run_counts, n_runs, ref_keys, n_ref, max_expand,
-                                                      run_rlo, run_rcount, run_hits);
+                                                      run_rlo, run_rcount, run_hits, key_mask);
   DRG_CUDA(cudaGetLastError());
 }
 

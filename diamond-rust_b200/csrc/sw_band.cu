@@ -42,8 +42,7 @@ template <bool TR>
 __device__ __forceinline__ uint32_t band_step(Regs<TR>& R, const Lane& L, int c, uint32_t cc2, uint32_t cw2,
                                               const uint8_t* __restrict__ prof, uint32_t rw, uint32_t noc2,
                                               uint32_t nge2, uint2* __restrict__ trace) {
-  const int jm1 = L.jbase + c - 1;
-  const uint32_t res = ((unsigned)jm1 < (unsigned)L.m) ? (uint32_t)__ldg(L.s + jm1) : 25u;
+  const uint32_t res = subject_residue(L, L.jbase + c - 1);
   const uint2 lo8 = *reinterpret_cast<const uint2*>(prof + res * kRows);
   const uint2 hi8 = *reinterpret_cast<const uint2*>(prof + R.res_prev * kRows + 8);
   R.res_prev = res;
@@ -192,7 +191,7 @@ __global__ void __launch_bounds__(kBandWarps * 32) k_sw_band(SwBandArgs a) {
           R.E7 = kNeg2;
           R.htop_old = rw_prev & 0xFFFFu;
           const int jm1 = L.jbase - 2;
-          R.res_prev = ((unsigned)jm1 < (unsigned)L.m) ? (uint32_t)L.s[jm1] : 25u;
+          R.res_prev = subject_residue(L, jm1);
         }
         const uint32_t cc2 = (uint32_t)c * 0x10001u;
         const uint32_t cw2 = (uint32_t)(uint16_t)(c - W) * 0x10001u;

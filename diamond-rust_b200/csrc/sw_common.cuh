@@ -49,7 +49,22 @@ struct Lane {
   const uint8_t* s;  // subject letters
   int m;             // subject length
   int jbase;         // absolute column of relative column 0 in this strip
+  uint32_t r0, r1;   // prefetched residues of the next two columns
 };
+
+// Residue of subject index j, or the sentinel off the sequence.
+__device__ __forceinline__ uint32_t subject_residue(const Lane& L, int j) {
+  return ((unsigned)j < (unsigned)L.m) ? (uint32_t)__ldg(L.s + j) : (uint32_t)kSentinel;
+}
+// The residue of column c (subject index jbase + c - 1) from the prefetch
+// queue, issuing the load of column c + 2 two steps ahead of its use.
+__device__ __forceinline__ uint32_t next_residue(Lane& L, int c) {
+  const uint32_t ahead = subject_residue(L, L.jbase + c + 1);
+  const uint32_t res = L.r0;
+  L.r0 = L.r1;
+  L.r1 = ahead;
+  return res;
+}
 
 template <bool TR>
 struct Regs {

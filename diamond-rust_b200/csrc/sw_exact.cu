@@ -248,17 +248,4 @@ void launch_sw_exact_with_matrix(const ExactJob* jobs, uint64_t n_jobs, int go, 
   DRG_CUDA(cudaGetLastError());
 }
 
-static MatArg g_mat_arg;
-void set_exact_matrix(const int8_t* s625) {
-  for (int i = 0; i < 625; ++i) g_mat_arg.s[i] = s625[i];
-}
-
-void launch_sw_exact(const ExactJob* jobs, uint64_t n_jobs, int go, int ge, bool trace, uint8_t* scratch,
-                     uint32_t* ops, ExactOut* out, cudaStream_t st) {
-  if (n_jobs == 0) return;
-  count_launch();
-  k_sw_exact<<<ceil_div(n_jobs, 64), 64, 0, st>>>(jobs, n_jobs, go, ge, trace, scratch, ops, out, g_mat_arg);
-  DRG_CUDA(cudaGetLastError());
-}
-
 }  // namespace drg

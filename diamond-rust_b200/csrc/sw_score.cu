@@ -41,55 +41,40 @@ namespace {
 
 using namespace sw;
 
+// Registers of one lane's 16-row strip in the score pass.
+struct SRegs {
+  uint32_t H[kPairs], Hm[kPairs], F[kPairs];
+  uint32_t E7;        // E of pair 7 at the previous step
+  uint32_t htop_old;  // top H of the previous step (D operand of pair 0)
+  uint32_t res_prev;  // subject residue of the previous column
+  uint32_t mx0, mx1;  // maximum H of the strip so far, folded over rows
+};
+
 // One column step.  MODE 0: middle (all rows in band), 1: prologue step
 // C (= c), 2: epilogue step C (= c - W) of a warp whose bands share one
 // width, 3: step past the narrowest band of a warp with mixed widths
-// (cw = c - this lane's W, masks computed at run time).
-template <int MODE, int C, bool TR>
-__device__ __forceinline__ void sw_step(Regs<TR>& R, const Lane& L, int c, const uint8_t* __restrict__ prof,
-                                        uint32_t* __restrict__ ring_r, uint32_t* __restrict__ ring_w, uint32_t noc2,
-                                        uint32_t nge2, uint2* __restrict__ trace, int cw = 0) {
-  const int jm1 = L.jbase + c - 1;  // subject index j - 1 of this column
-  const uint32_t res = ((unsigned)jm1 < (unsigned)L.m) ? (uint32_t)__ldg(L.s + jm1) : 25u;
+// (cw = c - this lane's W, masks computed at run time).  rp holds the (H, E)
+// word of the row above at column c; wp receives row 15's word of column c - 1.
+template <int MODE, int C>
+__device__ __forceinline__ void sw_step(SRegs& R, Lane& L, int c, const uint8_t* __restrict__ prof,
+                                        const uint32_t* __restrict__ rp, uint32_t* __restrict__ wp, uint32_t noc2,
+                                        uint32_t nge2, int cw = 0) {
+  const uint32_t res = next_residue(L, c);  // subject residue of this column
   const uint2 lo8 = *reinterpret_cast<const uint2*>(prof + res * kProfStride);
   const uint2 hi8 = *reinterpret_cast<const uint2*>(prof + R.res_prev * kProfStride + 8);
   R.res_prev = res;
-  const uint32_t rw = *ring_r;  // (H, E) of the row above row 0, column c
+  const uint32_t rw = *rp;  // (H, E) of the row above row 0, column c
   const uint32_t htop = prmt(rw, R.H[kPairs - 1], 0x5410);
   uint32_t e_up = prmt(rw, R.E7, 0x5432);
   uint32_t hm_up = add2(htop, noc2);
   uint32_t hd = R.htop_old;
-  uint32_t tr_lo = 0, tr_hi = 0;
-  const uint32_t colpair = TR ? ((uint32_t)c | ((uint32_t)(c - 1) << 16)) : 0u;
 #pragma unroll
   for (int p = 0; p < kPairs; ++p) {
     const uint32_t sc = prmt(p < 4 ? lo8.x : lo8.y, p < 4 ? hi8.x : hi8.y, pick_sel(p & 3));
     const uint32_t d = add2(hd, sc);
-    uint32_t e, f, h;
-    if (!TR) {
-      e = __viaddmax_s16x2(e_up, nge2, hm_up);
-      f = __viaddmax_s16x2(R.F[p], nge2, R.Hm[p]);
-      h = __vimax3_s16x2_relu(d, e, f);
-    } else {
-      const uint32_t te = add2(e_up, nge2);
-      const uint32_t tf = add2(R.F[p], nge2);
-      e = max2(te, hm_up);
-      f = max2(tf, R.Hm[p]);
-      const uint32_t m1 = max2_relu(d, 0u);
-      const uint32_t ce = __vcmpgts2(e, m1);
-      const uint32_t m2 = max2(e, m1);
-      const uint32_t cf = __vcmpgts2(f, m2);
-      h = max2(f, m2);
-      const uint32_t cd = __vcmpgts2(d, 0u);
-      const uint32_t ee = __vcmpgts2(te, hm_up);
-      const uint32_t fe = __vcmpgts2(tf, R.Hm[p]);
-      // nibble per half: choice (bit0, bit1), e_ext (bit2), f_ext (bit3)
-      uint32_t bits = ((cf | (cd & ~ce)) & 0x00010001u) | ((cf | ce) & 0x00020002u) | (ee & 0x00040004u) |
-                      (fe & 0x00080008u);
-      const uint32_t byte = (bits & 0xFu) | ((bits >> 12) & 0xF0u);  // low row in the low nibble
-      if (p < 4) tr_lo |= byte << (8 * (p & 3));
-      else tr_hi |= byte << (8 * (p & 3));
-    }
+    uint32_t e = __viaddmax_s16x2(e_up, nge2, hm_up);
+    uint32_t f = __viaddmax_s16x2(R.F[p], nge2, R.Hm[p]);
+    uint32_t h = __vimax3_s16x2_relu(d, e, f);
     if (MODE == 1) {
       // left of the band: row p at column C (low), row p+8 at column C-1 (high)
       const bool lo_left = C < p;
@@ -114,13 +99,6 @@ __device__ __forceinline__ void sw_step(Regs<TR>& R, const Lane& L, int c, const
       e = sel2(e, k, kNeg2);
     }
     const uint32_t hm = add2(h, noc2);
-    if (!TR) {
-      R.rowmax[p] = max2(R.rowmax[p], h);
-    } else {
-      const uint32_t gt = __vcmpgts2(h, R.rowmax[p]);
-      R.rowmax[p] = max2(R.rowmax[p], h);
-      R.rowcol[p] = (R.rowcol[p] & ~gt) | (colpair & gt);
-    }
     hd = R.H[p];
     R.H[p] = h;
     R.Hm[p] = hm;
@@ -128,32 +106,51 @@ __device__ __forceinline__ void sw_step(Regs<TR>& R, const Lane& L, int c, const
     hm_up = hm;
     e_up = e;
   }
+  // the strip's maximum, two accumulators of four pairs each
+  R.mx0 = __vimax3_s16x2(R.mx0, R.H[0], R.H[1]);
+  R.mx1 = __vimax3_s16x2(R.mx1, R.H[4], R.H[5]);
+  R.mx0 = __vimax3_s16x2(R.mx0, R.H[2], R.H[3]);
+  R.mx1 = __vimax3_s16x2(R.mx1, R.H[6], R.H[7]);
   R.E7 = e_up;
-  *ring_w = prmt(R.H[kPairs - 1], R.E7, 0x7632);  // (H, E) of row 15 at column c - 1
+  *wp = prmt(R.H[kPairs - 1], R.E7, 0x7632);  // (H, E) of row 15 at column c - 1
   R.htop_old = htop;
-  if (TR) *trace = make_uint2(tr_lo, tr_hi);
 }
 
-template <int MODE, int C, bool TR>
-struct Unroll {
-  static __device__ __forceinline__ void run(Regs<TR>& R, const Lane& L, int c0, const uint8_t* prof, uint32_t* ring,
-                                             int buf, int stride, int& slot, uint32_t noc2, uint32_t nge2,
-                                             uint2* trace) {
-    int wslot = slot == 0 ? buf - 1 : slot - 1;
-    sw_step<MODE, C, TR>(R, L, c0 + C, prof, ring + slot * stride, ring + wslot * stride, noc2, nge2,
-                         TR ? trace + (c0 + C) * 32 : nullptr);
-    slot = slot + 1 == buf ? 0 : slot + 1;
-    Unroll<MODE, C + 1, TR>::run(R, L, c0, prof, ring, buf, stride, slot, noc2, nge2, trace);
+// The ring of one lane: W + 1 words at stride `stride`; rp reads column c,
+// wp (the slot read one step earlier) takes column c - 1.
+struct RingPtr {
+  uint32_t *rp, *wp;
+  uint32_t* begin;
+  uint32_t* end;
+  int stride;
+  __device__ __forceinline__ void advance() {
+    wp = rp;
+    rp += stride;
+    if (rp == end) rp = begin;
   }
 };
-template <int MODE, bool TR>
-struct Unroll<MODE, kRows, TR> {
-  static __device__ __forceinline__ void run(Regs<TR>&, const Lane&, int, const uint8_t*, uint32_t*, int, int, int&,
-                                             uint32_t, uint32_t, uint2*) {}
+
+template <int MODE, int C>
+struct Unroll {
+  static __device__ __forceinline__ void run(SRegs& R, Lane& L, int c0, const uint8_t* prof, RingPtr& rg,
+                                             uint32_t noc2, uint32_t nge2) {
+    sw_step<MODE, C>(R, L, c0 + C, prof, rg.rp, rg.wp, noc2, nge2);
+    rg.advance();
+    Unroll<MODE, C + 1>::run(R, L, c0, prof, rg, noc2, nge2);
+  }
+};
+template <int MODE>
+struct Unroll<MODE, kRows> {
+  static __device__ __forceinline__ void run(SRegs&, Lane&, int, const uint8_t*, RingPtr&, uint32_t, uint32_t) {}
 };
 
-template <int WARPS, bool TR>
-__global__ void __launch_bounds__(WARPS * 32) k_sw(SwScoreArgs a) {
+// Score pass: scores[band] = the band's best H, best_row[band] = the last row
+// of the first strip that holds it (an upper bound of the reference's best_i,
+// which is all the traceback pass needs).
+// Shared memory holds three blocks per SM in the 4- and 2-warp classes, so
+// registers are budgeted for three (without the hint the compiler spills).
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, WARPS >= 2 ? 3 : 1) k_sw(SwScoreArgs a) {
   extern __shared__ __align__(16) uint8_t smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint64_t task_id = a.task_lo + (uint64_t)blockIdx.x * WARPS + warp;
@@ -183,10 +180,13 @@ __global__ void __launch_bounds__(WARPS * 32) k_sw(SwScoreArgs a) {
   // E is -inf; column Wl - 1 is outside row 0's band on the right.
   for (int g = 0; g < buf; ++g) ring[g * stride] = 0xC0000000u;
   ring[(Wl - 1) * stride] = kNeg2;
+  RingPtr rg;
+  rg.begin = ring;
+  rg.end = ring + buf * stride;
+  rg.stride = stride;
   int base = 0;  // ring slot of relative column 0 of the current strip
-  Regs<TR> R;
-  int best = 0, best_i = 0, best_j = 0;
-  uint2* tr = TR ? a.trace + task.trace_off + lane : nullptr;
+  SRegs R;
+  int best = 0, best_i = 0;
   for (uint32_t k = 0; k < task.n_strips; ++k) {
     const int i0 = (int)task.row_first + (int)(k * kRows);
     // strip profile: prof[res * stride + r] = S(q[i0 + r - 1], res)
@@ -206,33 +206,29 @@ __global__ void __launch_bounds__(WARPS * 32) k_sw(SwScoreArgs a) {
       R.H[p] = 0;
       R.Hm[p] = kNeg2;
       R.F[p] = kNeg2;
-      R.rowmax[p] = 0;
-      if (TR) R.rowcol[p] = 0;
     }
+    R.mx0 = R.mx1 = 0;
     R.E7 = kNeg2;
-    const int slot_m1 = base == 0 ? buf - 1 : base - 1;
-    R.htop_old = ring[slot_m1 * stride] & 0xFFFFu;
+    rg.rp = ring + base * stride;
+    rg.wp = ring + (base == 0 ? buf - 1 : base - 1) * stride;
+    R.htop_old = *rg.wp & 0xFFFFu;
     {
       const int jm1 = L.jbase - 2;  // column -1
-      R.res_prev = ((unsigned)jm1 < (unsigned)L.m) ? (uint32_t)L.s[jm1] : 25u;
+      R.res_prev = subject_residue(L, jm1);
+      L.r0 = subject_residue(L, jm1 + 1);  // columns 0 and 1
+      L.r1 = subject_residue(L, jm1 + 2);
     }
-    uint2* trs = TR ? tr + (uint64_t)k * (W + kRows) * 32 : nullptr;
-    int slot = base;
-    Unroll<1, 0, TR>::run(R, L, 0, prof, ring, buf, stride, slot, noc2, nge2, trs);
+    Unroll<1, 0>::run(R, L, 0, prof, rg, noc2, nge2);
     for (int c = kRows; c < Wmin; ++c) {
-      const int wslot = slot == 0 ? buf - 1 : slot - 1;
-      sw_step<0, 0, TR>(R, L, c, prof, ring + slot * stride, ring + wslot * stride, noc2, nge2,
-                        TR ? trs + c * 32 : nullptr);
-      slot = slot + 1 == buf ? 0 : slot + 1;
+      sw_step<0, 0>(R, L, c, prof, rg.rp, rg.wp, noc2, nge2);
+      rg.advance();
     }
     if (Wmin == W) {  // one width in the warp: compile-time masks
-      Unroll<2, 0, TR>::run(R, L, W, prof, ring, buf, stride, slot, noc2, nge2, trs);
+      Unroll<2, 0>::run(R, L, W, prof, rg, noc2, nge2);
     } else {          // mixed widths: each lane masks past its own right edge
       for (int c = Wmin; c < W + kRows; ++c) {
-        const int wslot = slot == 0 ? buf - 1 : slot - 1;
-        sw_step<3, 0, TR>(R, L, c, prof, ring + slot * stride, ring + wslot * stride, noc2, nge2,
-                          TR ? trs + c * 32 : nullptr, c - Wl);
-        slot = slot + 1 == buf ? 0 : slot + 1;
+        sw_step<3, 0>(R, L, c, prof, rg.rp, rg.wp, noc2, nge2, c - Wl);
+        rg.advance();
       }
     }
     // this lane's column Wl + 15 is the next strip's column Wl - 1: outside
@@ -245,32 +241,17 @@ __global__ void __launch_bounds__(WARPS * 32) k_sw(SwScoreArgs a) {
     }
     base += kRows;
     if (base >= buf) base -= buf;
-    // first row-major maximum: rows in order, strictly greater wins
-#pragma unroll
-    for (int r = 0; r < kRows; ++r) {
-      const int v = r < kPairs ? lo16(R.rowmax[r]) : hi16(R.rowmax[r - kPairs]);
-      if (v > best) {
-        best = v;
-        best_i = i0 + r;
-        if (TR) best_j = L.jbase + (r < kPairs ? lo16(R.rowcol[r]) : hi16(R.rowcol[r - kPairs]));
-      }
+    // strictly greater: the first strip holding the maximum keeps it
+    const uint32_t m2 = max2(R.mx0, R.mx1);
+    const int v = max(lo16(m2), hi16(m2));
+    if (v > best) {
+      best = v;
+      best_i = i0 + kRows - 1;
     }
   }
   if (!active) return;
-  if (!TR) {
-    a.score[bidx] = best;
-    if (a.best_row) a.best_row[bidx] = best_i;
-  } else {
-    TraceBand t;
-    t.trace_off = task.trace_off + lane;
-    t.row_first = task.row_first;
-    t.width = (uint32_t)W;
-    t.score = best;
-    t.best_i = best_i;
-    t.best_j = best_j;
-    t.stride = 32;  // lane-interleaved
-    a.tband[bidx] = t;
-  }
+  a.score[bidx] = best;
+  if (a.best_row) a.best_row[bidx] = best_i;
 }
 
 // Traceback of one band through the nibbles of the trace pass, in the
@@ -372,19 +353,19 @@ __global__ void k_sw_walk(SwWalkArgs a) {
   a.out[t] = R;
 }
 
-template <int WARPS, bool TR>
+template <int WARPS>
 void launch_class(const SwScoreArgs& a, int max_width, cudaStream_t st) {
   if (a.task_hi <= a.task_lo) return;
   const int threads = WARPS * 32;
   const size_t smem = 640 + WARPS * kProfBytes + (size_t)threads * (max_width + 1) * 4;
   static int configured = 0;  // per template instance
   if ((int)smem > configured) {
-    DRG_CUDA(cudaFuncSetAttribute(k_sw<WARPS, TR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    DRG_CUDA(cudaFuncSetAttribute(k_sw<WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     configured = (int)smem;
   }
   const int blocks = ceil_div((long long)(a.task_hi - a.task_lo), WARPS);
   count_launch();
-  k_sw<WARPS, TR><<<blocks, threads, smem, st>>>(a);
+  k_sw<WARPS><<<blocks, threads, smem, st>>>(a);
   DRG_CUDA(cudaGetLastError());
 }
 
@@ -397,12 +378,12 @@ int sw_width_class(int width) {
   return -1;
 }
 
-void launch_sw_class(const SwScoreArgs& a, int cls, bool trace, cudaStream_t st) {
+void launch_sw_class(const SwScoreArgs& a, int cls, cudaStream_t st) {
   switch (cls) {
-    case 0: trace ? launch_class<4, true>(a, kSwClassMax[0], st) : launch_class<4, false>(a, kSwClassMax[0], st); break;
-    case 1: trace ? launch_class<2, true>(a, kSwClassMax[1], st) : launch_class<2, false>(a, kSwClassMax[1], st); break;
-    case 2: trace ? launch_class<1, true>(a, kSwClassMax[2], st) : launch_class<1, false>(a, kSwClassMax[2], st); break;
-    default: trace ? launch_class<1, true>(a, kSwClassMax[3], st) : launch_class<1, false>(a, kSwClassMax[3], st); break;
+    case 0: launch_class<4>(a, kSwClassMax[0], st); break;
+    case 1: launch_class<2>(a, kSwClassMax[1], st); break;
+    case 2: launch_class<1>(a, kSwClassMax[2], st); break;
+    default: launch_class<1>(a, kSwClassMax[3], st); break;
   }
 }
 

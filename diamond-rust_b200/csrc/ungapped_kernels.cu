@@ -12,25 +12,26 @@
 
 namespace drg {
 
-__constant__ int8_t c_score[625];
+// One score matrix per context slot (contexts may search concurrently).
+__constant__ int8_t c_score[kConstSlots][625];
 
-void upload_score_matrix(const int8_t* s, cudaStream_t st) {
-  DRG_CUDA(cudaMemcpyToSymbolAsync(c_score, s, 625, 0, cudaMemcpyHostToDevice, st));
+void upload_score_matrix(const int8_t* s, int slot, cudaStream_t st) {
+  DRG_CUDA(cudaMemcpyToSymbolAsync(c_score, s, 625, (size_t)slot * 625, cudaMemcpyHostToDevice, st));
 }
 
-__device__ __forceinline__ int mscore(uint32_t a, uint32_t b) {
+__device__ __forceinline__ int mscore(uint32_t a, uint32_t b, int slot) {
   a = a < 24 ? a : 24;
   b = b < 24 ? b : 24;
-  return c_score[a * 25 + b];
+  return c_score[slot][a * 25 + b];
 }
 
 __device__ SegmentOut xdrop_dev(const uint8_t* __restrict__ q, uint32_t qlen, const uint8_t* __restrict__ s,
-                                uint32_t slen, uint32_t qa, uint32_t sa, int xd) {
+                                uint32_t slen, uint32_t qa, uint32_t sa, int xd, int slot) {
   int score = 0, st = 0;
   uint32_t n = 1, delta = 0, len = 0;
   int64_t qi = (int64_t)qa - 1, si = (int64_t)sa - 1;
   while (score - st < xd && qi >= 0 && si >= 0) {
-    st += mscore(q[qi], s[si]);
+    st += mscore(q[qi], s[si], slot);
     if (st > score) {
       score = st;
       delta = n;
@@ -44,7 +45,7 @@ __device__ SegmentOut xdrop_dev(const uint8_t* __restrict__ q, uint32_t qlen, co
   st = score;
   n = 1;
   while (score - st < xd && qi < (int64_t)qlen && si < (int64_t)slen) {
-    st += mscore(q[qi], s[si]);
+    st += mscore(q[qi], s[si], slot);
     if (st > score) {
       score = st;
       len = n;
@@ -94,7 +95,7 @@ __global__ void k_xdrop_runs(XdropArgs a) {
     a.keep[i] = 0;
     if (last_end >= (int64_t)spos) continue;
     uint32_t qpos = (uint32_t)(diag + spos);
-    SegmentOut seg = xdrop_dev(q, qlen, s, slen, qpos, spos, a.xdrop);
+    SegmentOut seg = xdrop_dev(q, qlen, s, slen, qpos, spos, a.xdrop, a.slot);
     ++nx;
     if (seg.score >= a.cutoff) {
       a.seg[i] = seg;
@@ -114,12 +115,12 @@ void launch_xdrop_runs(const XdropArgs& a, cudaStream_t st) {
 
 __global__ void k_xdrop_jobs(const drg_xdrop_job* __restrict__ jobs, uint64_t n, const uint8_t* __restrict__ ql,
                              const uint64_t* __restrict__ qo, const uint8_t* __restrict__ sl,
-                             const uint64_t* __restrict__ so, int xd, drg_segment* __restrict__ out) {
+                             const uint64_t* __restrict__ so, int xd, drg_segment* __restrict__ out, int slot) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   drg_xdrop_job j = jobs[i];
   SegmentOut g = xdrop_dev(ql + qo[j.query], (uint32_t)(qo[j.query + 1] - qo[j.query]), sl + so[j.subject],
-                           (uint32_t)(so[j.subject + 1] - so[j.subject]), (uint32_t)j.qa, (uint32_t)j.sa, xd);
+                           (uint32_t)(so[j.subject + 1] - so[j.subject]), (uint32_t)j.qa, (uint32_t)j.sa, xd, slot);
   drg_segment r;
   r.q_start = g.q_start;
   r.s_start = g.s_start;
@@ -130,10 +131,10 @@ __global__ void k_xdrop_jobs(const drg_xdrop_job* __restrict__ jobs, uint64_t n,
 }
 
 void launch_xdrop_jobs(const drg_xdrop_job* jobs, uint64_t n, const uint8_t* ql, const uint64_t* qo,
-                       const uint8_t* sl, const uint64_t* so, int xd, drg_segment* out, cudaStream_t st) {
+                       const uint8_t* sl, const uint64_t* so, int xd, drg_segment* out, int slot, cudaStream_t st) {
   if (n == 0) return;
   count_launch();
-  k_xdrop_jobs<<<ceil_div(n, 128), 128, 0, st>>>(jobs, n, ql, qo, sl, so, xd, out);
+  k_xdrop_jobs<<<ceil_div(n, 128), 128, 0, st>>>(jobs, n, ql, qo, sl, so, xd, out, slot);
   DRG_CUDA(cudaGetLastError());
 }
 

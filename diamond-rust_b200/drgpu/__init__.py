@@ -86,7 +86,8 @@ class RunStats(C.Structure):
                                           "ms_sw_kernel")] + \
                [("sw_launches", C.c_uint64), ("kernel_launches", C.c_uint64), ("exact_bands", C.c_uint64),
                 ("sw_class_tasks", C.c_uint64 * 4), ("sw_class_max_steps", C.c_uint64 * 4),
-                ("ms_sw_class", C.c_double * 4), ("ms_trace_kernel", C.c_double), ("dp_cells_lane", C.c_uint64)]
+                ("ms_sw_class", C.c_double * 4), ("ms_trace_kernel", C.c_double), ("dp_cells_lane", C.c_uint64),
+                ("sw_wide_bands", C.c_uint64), ("ms_sw_wide", C.c_double)]
 
     def as_dict(self):
         d = {}
@@ -134,6 +135,8 @@ _SIGNATURES = {
     "drg_db_create": (C.c_int, [C.c_void_p, _u8p, _u64p, C.c_uint64, _P(C.c_void_p)]),
     "drg_db_destroy": (None, [C.c_void_p]),
     "drg_batch_create": (C.c_int, [C.c_void_p, _u8p, _u64p, _u32p, _u8p, C.c_uint64, _P(C.c_void_p)]),
+    "drg_batch_create_requests": (C.c_int, [C.c_void_p, _u8p, _u64p, _u32p, _u8p, _u32p, C.c_uint64,
+                                            _P(C.c_void_p)]),
     "drg_batch_destroy": (None, [C.c_void_p]),
     "drg_search_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, _P(SearchConfig), _P(Result)]),
     "drg_search_run": (C.c_int, [C.c_void_p, _u8p, _u64p, C.c_uint64, _u8p, _u64p, _u32p, _u8p, C.c_uint64,
@@ -429,7 +432,8 @@ class ResidentDb:
 class ResidentBatch:
     """Query batch resident in device memory (drg_batch)."""
 
-    def __init__(self, ctx: Context, letters, offsets, query=None, frame=None):
+    def __init__(self, ctx: Context, letters, offsets, query=None, frame=None, request=None):
+        """request[t]: request id of target t; each request is searched as if alone."""
         self.ctx = ctx
         n = len(offsets) - 1
         self._l, lp = _u8(letters if len(letters) else np.zeros(1, np.uint8))
@@ -437,7 +441,11 @@ class ResidentBatch:
         self._q, qp = _u32(np.arange(n) if query is None else query)
         self._f, fp = _u8(np.zeros(n) if frame is None else frame)
         h = C.c_void_p()
-        ctx._check(ctx.lib.drg_batch_create(ctx.h, lp, op, qp, fp, n, C.byref(h)))
+        if request is None:
+            ctx._check(ctx.lib.drg_batch_create(ctx.h, lp, op, qp, fp, n, C.byref(h)))
+        else:
+            self._r, rp = _u32(request)
+            ctx._check(ctx.lib.drg_batch_create_requests(ctx.h, lp, op, qp, fp, rp, n, C.byref(h)))
         self.h = h
 
     def close(self):

@@ -1,0 +1,185 @@
+"""Serving: a request loop over a database resident in HBM.
+
+Requests (a list of protein queries plus a sensitivity preset) arrive at any
+time.  Worker threads, one CUDA context each, share the resident database;
+whenever a worker is free it admits every queued request with the preset of
+the oldest one, up to a budget of query letters, as one batch
+(drg_batch_create_requests) and searches it.  The batch's join cap is counted
+per request, so each request's HSP lists equal those of the request searched
+alone; requests that arrive while a batch runs wait only for the next free
+worker (continuous batching), and the workers' batches overlap on the GPU.
+
+The plain path (`workers=1, batch=False`) serves one request at a time.
+Latency is the wall time from a request's arrival to its results being back on
+the host; throughput is queries over the whole run.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import statistics
+import threading
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import (Context, HspRecord, ResidentBatch, ResidentDb, Result, _result_lists, concat, make_config)
+
+
+@dataclass
+class Request:
+    rid: int
+    preset: str
+    queries: list
+    arrival: float = 0.0          # seconds, on the server's clock
+    done: float = 0.0
+    results: list = field(default_factory=list)  # per query: HSP records
+    batch_size: int = 0           # requests in the batch that served it
+
+
+def search_batch(ctx: Context, db: ResidentDb, requests, preset: str, index_chunks=None):
+    """Search several requests of one preset as one batch; fills each request's results."""
+    seqs, rid = [], []
+    for k, r in enumerate(requests):
+        seqs.extend(r.queries)
+        rid.extend([k] * len(r.queries))
+    letters, offsets = concat(seqs)
+    batch = ResidentBatch(ctx, letters, offsets, request=np.asarray(rid, np.uint32))
+    cfg = make_config(sensitivity=preset, index_chunks=index_chunks)
+    res = Result()
+    try:
+        ctx._check(ctx.lib.drg_search_batch(ctx.h, db.h, batch.h, C.byref(cfg), C.byref(res)))
+        lists = _result_lists(res)
+    finally:
+        ctx.lib.drg_result_free(C.byref(res))
+        batch.close()
+    t = 0
+    for r in requests:
+        n = len(r.queries)
+        r.results = [[HspRecord(h.query - t, *h.key()[1:]) for h in lst] for lst in lists[t:t + n]]
+        r.batch_size = len(requests)
+        t += n
+    return requests
+
+
+class Server:
+    """Continuous-batching request loop over one resident database."""
+
+    def __init__(self, db_letters, db_offsets, workers=2, batch=True, budget_letters=4_000_000, device=0,
+                 index_chunks=None):
+        self.ctxs = [Context(device) for _ in range(workers)]
+        self.db = ResidentDb(self.ctxs[0], db_letters, db_offsets)
+        self.batch = batch
+        self.budget = budget_letters
+        self.index_chunks = index_chunks
+        self.pending: list[Request] = []
+        self.lock = threading.Condition()
+        self.closed = False
+        self.finished: list[Request] = []
+        self.t0 = time.perf_counter()
+        self.errors: list[BaseException] = []
+        self.threads = [threading.Thread(target=self._worker, args=(c,), daemon=True) for c in self.ctxs]
+        for t in self.threads:
+            t.start()
+
+    def now(self):
+        return time.perf_counter() - self.t0
+
+    def submit(self, req: Request):
+        with self.lock:
+            req.arrival = self.now()
+            self.pending.append(req)
+            self.lock.notify()
+
+    def _take(self):
+        """The oldest request and, when batching, every queued request of its
+        preset that fits the letter budget (admission by memory)."""
+        head = self.pending[0]
+        if not self.batch:
+            self.pending.pop(0)
+            return [head]
+        take, used = [], 0
+        for r in list(self.pending):
+            if r.preset != head.preset:
+                continue
+            size = sum(len(q) for q in r.queries)
+            if take and used + size > self.budget:
+                break
+            take.append(r)
+            used += size
+        for r in take:
+            self.pending.remove(r)
+        return take
+
+    def _worker(self, ctx):
+        while True:
+            with self.lock:
+                while not self.pending and not self.closed:
+                    self.lock.wait()
+                if not self.pending and self.closed:
+                    return
+                reqs = self._take()
+            try:
+                search_batch(ctx, self.db, reqs, reqs[0].preset, self.index_chunks)
+            except BaseException as e:  # surfaced by close()
+                self.errors.append(e)
+            t = self.now()
+            with self.lock:
+                for r in reqs:
+                    r.done = t
+                self.finished.extend(reqs)
+                self.lock.notify_all()
+
+    def close(self):
+        with self.lock:
+            self.closed = True
+            self.lock.notify_all()
+        for t in self.threads:
+            t.join()
+        self.db.close()
+        for c in self.ctxs:
+            c.close()
+        if self.errors:
+            raise self.errors[0]
+
+
+def poisson_stream(rng, n_requests, rate, max_queries, presets, q_mean=350, q_lo=20, q_hi=3000):
+    """Requests of a serving stream: exponential gaps at `rate` per second,
+    1..max_queries queries each (lengths lognormal), presets drawn uniformly."""
+    from . import synth
+    reqs, t = [], 0.0
+    for k in range(n_requests):
+        t += float(rng.exponential(1.0 / rate))
+        nq = int(rng.integers(1, max_queries + 1))
+        qs = [synth.random_protein(rng, L) for L in synth.lognormal_lengths(rng, nq, q_mean, q_lo, q_hi)]
+        reqs.append((t, Request(k, str(rng.choice(presets)), qs)))
+    return reqs
+
+
+def run_stream(server: Server, stream):
+    """Replays the stream in real time; returns the finished requests and the span."""
+    start = time.perf_counter()
+    for at, req in stream:
+        delay = at - (time.perf_counter() - start)
+        if delay > 0:
+            time.sleep(delay)
+        server.submit(req)
+    with server.lock:
+        while len(server.finished) < len(stream) and not server.errors:
+            server.lock.wait(timeout=1.0)
+    span = time.perf_counter() - start
+    return list(server.finished), span
+
+
+def latency_summary(finished, span):
+    lat = sorted(r.done - r.arrival for r in finished)
+    q = sum(len(r.queries) for r in finished)
+
+    def pct(p):
+        if not lat:
+            return None
+        k = min(len(lat) - 1, max(0, int(round(p / 100.0 * (len(lat) - 1)))))
+        return lat[k]
+    return {"requests": len(finished), "queries": q, "p50_s": pct(50), "p99_s": pct(99),
+            "mean_s": statistics.fmean(lat) if lat else None, "queries_per_s": q / span if span > 0 else None,
+            "mean_batch_requests": statistics.fmean(r.batch_size for r in finished) if finished else None}

@@ -173,4 +173,90 @@ def workload(config_id: int, scale: float = 1.0, n_queries=None, n_db=None, seed
             q = queries[k // 5]
             db[s] = planted_homolog(rng, q, 30, len(q), 0.25, 0.70, max(len(db[s]), 40))
         return Workload(db, queries, "config2")
+    if config_id == 3:
+        ndb = n_db or max(8, int(2_000_000 * scale))
+        nq = n_queries or max(1, int(50_000 * scale))
+        queries = [random_protein(rng, L) for L in lognormal_lengths(rng, nq, 350, 20, 2000)]
+        db = make_db(rng, ndb)
+        with_homologs = rng.random(nq) < 0.10
+        slot = 0
+        order = rng.permutation(ndb)
+        for qi in np.nonzero(with_homologs)[0]:
+            q = queries[qi]
+            for _ in range(int(rng.integers(1, 21))):
+                if slot >= ndb:
+                    break
+                s = order[slot]
+                slot += 1
+                db[s] = planted_homolog(rng, q, min(30, len(q)), len(q), 0.25, 0.70, max(len(db[s]), 40))
+        return Workload(db, queries, "config3")
     raise ValueError(f"unknown workload {config_id}")
+
+
+# The standard genetic code, codons in T, C, A, G base order.
+CODON_TABLE = "FFLLSSSSYY**CC*WLLLLPPPPHHQQRRRRIIIMTTTTNNKKSSRRVVVVAAAADDEEGGGG"
+_BASES = "TCAG"
+_SYNONYMS = {}
+for _i, _aa in enumerate(CODON_TABLE):
+    _SYNONYMS.setdefault(_aa, []).append(_BASES[_i // 16] + _BASES[(_i // 4) % 4] + _BASES[_i % 4])
+_COMPLEMENT = str.maketrans("ACGT", "TGCA")
+
+
+def reverse_translate(rng, protein, sub_rate=0.01):
+    """Nucleotides coding for `protein` (uniform synonymous codons), with substitutions."""
+    nt = []
+    for c in protein:
+        aa = AA[c] if c < 20 else "*"
+        cod = _SYNONYMS.get(aa) or _SYNONYMS["*"]
+        nt.append(cod[int(rng.integers(0, len(cod)))])
+    s = list("".join(nt))
+    for k in np.nonzero(rng.random(len(s)) < sub_rate)[0]:
+        s[k] = "ACGT"[int(rng.integers(0, 4))]
+    return "".join(s)
+
+
+class ReadWorkload:
+    """blastx input: a protein DB and nucleotide reads (strings)."""
+
+    def __init__(self, db, reads, name):
+        self.db = db
+        self.reads = reads
+        self.name = name
+        self.db_ids = [f"S{i}" for i in range(len(db))]
+        self.read_ids = [f"R{i}" for i in range(len(reads))]
+
+    def write_fasta(self, db_path, read_path):
+        with open(db_path, "w") as f:
+            for i, s in zip(self.db_ids, self.db):
+                f.write(f">{i} synthetic\n" + "".join(AA[c] for c in s) + "\n")
+        with open(read_path, "w") as f:
+            for i, r in zip(self.read_ids, self.reads):
+                f.write(f">{i} read\n{r}\n")
+
+
+def read_workload(scale: float = 1.0, n_reads=None, n_db=None, seed_offset=0) -> ReadWorkload:
+    """blastx configuration: reads of 150-300 nt against the 2M-sequence protein DB
+    generator; 30 % of the reads are reverse-translated fragments of DB proteins
+    (random strand and frame, 1 % substitutions), the rest random ACGT at 50 % GC."""
+    rng = np.random.Generator(np.random.PCG64(20261203 + 4 + seed_offset))
+    ndb = n_db or max(8, int(2_000_000 * scale))
+    nr = n_reads or max(1, int(500_000 * scale))
+    db = make_db(rng, ndb)
+    reads = []
+    for _ in range(nr):
+        L = int(rng.integers(150, 301))
+        if rng.random() < 0.30:
+            p = db[int(rng.integers(0, ndb))]
+            n_aa = L // 3 + 2
+            if len(p) > n_aa:
+                a = int(rng.integers(0, len(p) - n_aa + 1))
+                p = p[a:a + n_aa]
+            nt = reverse_translate(rng, p)
+            off = int(rng.integers(0, 3))
+            nt = (nt[off:] + "".join("ACGT"[int(x)] for x in rng.integers(0, 4, 3)))[:L]
+            if rng.random() < 0.5:
+                nt = nt.translate(_COMPLEMENT)[::-1]
+            reads.append(nt)
+        else:
+            reads.append("".join("ACGT"[int(x)] for x in rng.integers(0, 4, L)))
+    return ReadWorkload(db, reads, "config4")

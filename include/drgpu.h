@@ -105,6 +105,8 @@ typedef struct {
   double ms_sw_class[4];           /* device time of each class launch */
   double ms_trace_kernel;          /* device time of the trace-mode kernel launches */
   uint64_t dp_cells_lane;          /* score kernel: each band's own rows x (W + 16), without warp padding */
+  uint64_t sw_wide_bands;          /* score pass: bands wider than 272 columns, one warp per band */
+  double ms_sw_wide;               /* device time of their launch (concurrent with the classes) */
 } drg_run_stats;
 
 /* search::run result: per-target HSP lists, target_offsets[n_targets+1]. */
@@ -119,6 +121,9 @@ typedef struct {
 } drg_result;
 
 /* ---- context --------------------------------------------------------- */
+/* One context per host thread; up to 8 contexts may be live in a process at
+ * a time (each holds its own bank of constant tables, so contexts can search
+ * concurrently with different presets).  A ninth returns DRG_ERR_INVALID. */
 int drg_ctx_create(int device, drg_ctx** out);
 void drg_ctx_destroy(drg_ctx* ctx);
 const char* drg_last_error(const drg_ctx* ctx);
@@ -192,6 +197,15 @@ void drg_db_destroy(drg_db* db);  /* before the db's context is destroyed */
 /* Query batch (search::Target list, search.rs:82-88) resident in device memory. */
 int drg_batch_create(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offsets, const uint32_t* query_index,
                      const uint8_t* frame, uint64_t n_targets, drg_batch** out);
+/* A batch holding several independent requests (serving): request[t] is the
+ * request of target t (at most 65535).  The seed join's expansion cap counts
+ * query occurrences per request (search.rs:109-131 counts them over the whole
+ * run), so every request's HSPs equal those of a search of its targets alone;
+ * all requests of a batch share the database and the search configuration.
+ * No reference counterpart: search::run serves one request per call. */
+int drg_batch_create_requests(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offsets,
+                              const uint32_t* query_index, const uint8_t* frame, const uint32_t* request,
+                              uint64_t n_targets, drg_batch** out);
 void drg_batch_destroy(drg_batch* b);
 
 /* search::run over resident inputs.  Results are per-target HSP lists, each

@@ -230,6 +230,17 @@ int cmd_blast(const std::vector<std::string>& args, bool translated) {  // workf
   return 0;
 }
 
+// db.rs:298-308 fmt_count: decimal digits grouped by three with commas.
+std::string group_thousands(uint64_t v) {
+  const std::string d = std::to_string(v);
+  std::string out;
+  for (size_t i = 0; i < d.size(); ++i) {
+    if (i > 0 && (d.size() - i) % 3 == 0) out += ',';
+    out += d[i];
+  }
+  return out;
+}
+
 int cmd_makedb(const std::vector<std::string>& args) {  // workflow.rs:42-60 + cli.rs:88-123
   std::string input, output;
   bool have_in = false, have_out = false, no_auto_append = false, quiet = false;
@@ -255,8 +266,8 @@ int cmd_makedb(const std::vector<std::string>& args) {  // workflow.rs:42-60 + c
   auto t0 = std::chrono::steady_clock::now();
   if (!db_build(input, path, &err, &n, &letters)) throw CliError{err};
   if (!quiet) {
-    fprintf(stderr, "Database: %s\nSequences: %zu\nLetters: %llu\nTotal time = %.3fs\n", path.c_str(), n,
-            (unsigned long long)letters,
+    fprintf(stderr, "Database: %s\nSequences: %zu\nLetters: %s\nTotal time = %.3fs\n", path.c_str(), n,
+            group_thousands(letters).c_str(),
             std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
   }
   return 0;
@@ -286,8 +297,8 @@ int cli_main(int argc, char** argv) {
       if (path.empty()) throw CliError{"Missing option: --db"};
       Database db;
       if (!db_open(path, &db, &err)) throw CliError{err};
-      printf("Database: %s\nSequences: %zu\nLetters: %llu\nType: protein\n", db.path.c_str(), db.seq_count,
-             (unsigned long long)db.total_letters);
+      printf("Database: %s\nSequences: %zu\nLetters: %s\nType: protein\n", db.path.c_str(), db.seq_count,
+             group_thousands(db.total_letters).c_str());
       return 0;
     }
     fprintf(stderr, "Unknown command: %s\n", args[0].c_str());
