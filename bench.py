@@ -43,7 +43,7 @@ METRIC = "bit-exact queries/sec + SW GCUPS, batched vs plain on 1 B200; p50/p99 
 # 200-query case over that pass's evaluated cells (profiles/); scaled to a full
 # pass by its evaluated cells (the traffic is the bands, query windows and
 # subjects the warps read, in proportion to the work).
-SW_TRAFFIC_PER_CELL = None
+SW_TRAFFIC_PER_CELL = 19.898624e6 / 13.531323984e9
 SENS = "sensitive"
 
 
@@ -56,6 +56,8 @@ def parse():
     p.add_argument("--cpu-sample", type=int, default=100, help="queries in the CPU baseline sample")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    p.add_argument("--no-serve", action="store_true", help="skip the serving stream (profiling runs)")
+    p.add_argument("--serve-requests", type=int, default=100, help="requests in the serving stream")
     p.add_argument("--queries", type=int, default=None,
                    help="search only the first N queries (a smaller case for ncu captures; not a bench line)")
     return p.parse_args()
@@ -180,6 +182,31 @@ def max_over_ranks(x, world):
     return float(t.item())
 
 
+def serve_stream(w, device, n_requests):
+    """A Poisson request stream (20 requests/s, 1-2000 queries each, lengths
+    lognormal mean 350 clipped 20-3000, presets uniform over fast / default /
+    sensitive / very-sensitive) against the resident database, served plain
+    (one request at a time) and continuously batched (2 worker contexts)."""
+    import numpy as np
+    import drgpu
+    from drgpu import serve
+    dl, do = drgpu.concat(w.db)
+    out = {"stream": f"{n_requests} requests, Poisson 20/s, 1-2000 queries each (lognormal mean 350, 20-3000 aa), "
+                     f"presets uniform over fast/default/sensitive/very-sensitive, resident "
+                     f"{len(w.db)}-sequence DB; latency = arrival to results on the host"}
+    for name, workers, batched in (("plain", 1, False), ("batched", 2, True)):
+        rng = np.random.Generator(np.random.PCG64(20261208))
+        stream = serve.poisson_stream(rng, n_requests, 20.0, 2000,
+                                      ["fast", "default", "sensitive", "very-sensitive"])
+        srv = serve.Server(dl, do, workers=workers, batch=batched, device=device)
+        try:
+            finished, span = serve.run_stream(srv, stream)
+        finally:
+            srv.close()
+        out[name] = serve.latency_summary(finished, span)
+    return out
+
+
 def cpu_sample_run(w, n_sample, threads):
     import pyoracle
     qs = w.queries[:n_sample]
@@ -283,6 +310,11 @@ def main():
     e2e = {"value": world * len(w.queries) * args.steps / e2e_s, "unit": "queries/s",
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(d2h)}
 
+    # ---- serving: the same request stream, plain and continuously batched ---
+    serving = None
+    if not args.no_serve:
+        serving = serve_stream(w, local, args.serve_requests)
+
     # ---- CPU baseline and sample parity (rank 0, N = 1) ---------------------
     cpu = None
     parity = None
@@ -328,6 +360,7 @@ def main():
                                                 "segments", "bands", "bands_computed", "exact_bands", "traced_bands",
                                                 "hsps")},
             "e2e": e2e,
+            "serving": serving,
             "gpu_launches": int(launches),
             "cpu_baseline": cpu,
             "parity_sample": parity,
