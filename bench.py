@@ -193,17 +193,21 @@ def serve_stream(w, device, n_requests):
     dl, do = drgpu.concat(w.db)
     out = {"stream": f"{n_requests} requests, Poisson 20/s, 1-2000 queries each (lognormal mean 350, 20-3000 aa), "
                      f"presets uniform over fast/default/sensitive/very-sensitive, resident "
-                     f"{len(w.db)}-sequence DB; latency = arrival to results on the host"}
-    for name, workers, batched in (("plain", 1, False), ("batched", 2, True)):
-        rng = np.random.Generator(np.random.PCG64(20261208))
-        stream = serve.poisson_stream(rng, n_requests, 20.0, 2000,
-                                      ["fast", "default", "sensitive", "very-sensitive"])
-        srv = serve.Server(dl, do, workers=workers, batch=batched, device=device)
-        try:
-            finished, span = serve.run_stream(srv, stream)
-        finally:
-            srv.close()
-        out[name] = serve.latency_summary(finished, span)
+                     f"{len(w.db)}-sequence DB; latency = arrival to results on the host; *_capacity: the same "
+                     f"requests queued at once"}
+    # at the stream's rate (latency), and with every request queued at once
+    # (capacity: the throughput each form sustains)
+    for rate, tag in ((20.0, ""), (1e6, "_capacity")):
+        for name, workers, batched in (("plain", 1, False), ("batched", 2, True)):
+            rng = np.random.Generator(np.random.PCG64(20261208))
+            stream = serve.poisson_stream(rng, n_requests, rate, 2000,
+                                          ["fast", "default", "sensitive", "very-sensitive"])
+            srv = serve.Server(dl, do, workers=workers, batch=batched, device=device)
+            try:
+                finished, span = serve.run_stream(srv, stream)
+            finally:
+                srv.close()
+            out[name + tag] = serve.latency_summary(finished, span)
     return out
 
 

@@ -98,7 +98,9 @@ def test_server_stream_continuous_batching():
     w = synth.workload(2, n_queries=10, n_db=1200, seed_offset=33)
     dl, do = drgpu.concat(w.db)
     rng = np.random.Generator(np.random.PCG64(5))
-    stream = serve.poisson_stream(rng, 24, rate=60.0, max_queries=12,
+    # the requests arrive together, so that queued requests of one preset are
+    # admitted as one batch whatever the speed of the GPU
+    stream = serve.poisson_stream(rng, 24, rate=1e6, max_queries=12,
                                   presets=["fast", "default", "sensitive", "very-sensitive"], q_hi=600)
     srv = serve.Server(dl, do, workers=2, batch=True)
     try:
