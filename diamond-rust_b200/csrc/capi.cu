@@ -149,8 +149,12 @@ int drg_ctx_create(int device, drg_ctx** out) {
   props.location.type = cudaMemLocationTypeDevice;
   props.location.id = device;
   const uint64_t keep = UINT64_MAX;  // hold freed blocks for reuse by the next call
+  int prio_low = 0, prio_high = 0;
   if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high) != cudaSuccess ||
+      // the side stream carries the long warps of the score pass: its blocks
+      // are dispatched ahead of the bulk class's whenever an SM frees up
+      cudaStreamCreateWithPriority(&c->side, cudaStreamNonBlocking, prio_high) != cudaSuccess ||
       cudaMemPoolCreate(&c->pool, &props) != cudaSuccess ||
       cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, (void*)&keep) != cudaSuccess) {
     if (c->stream) cudaStreamDestroy(c->stream);

@@ -213,10 +213,7 @@ __global__ void k_sw_fill_tasks(const uint32_t* starts, uint64_t n_tasks, const 
   sort_key[t] = ((uint64_t)cls << 60) | ((~steps) & ((1ull << 60) - 1));  // class, then longest first
   sort_val[t] = (uint32_t)t;
   if (trace_size) trace_size[t] = steps * 32ull;
-  if (cells_gpu) {
-    atomicAdd(cells_gpu, (unsigned long long)k.n_strips * 16ull * (wmax + 16ull) * cnt);
-    atomicAdd(cells_gpu + 1, (unsigned long long)lane_cells);
-  }
+  if (cells_gpu) atomicAdd(cells_gpu + 1, (unsigned long long)lane_cells);  // evaluated cells: counted by k_sw
 }
 
 __global__ void k_gather_tasks(const SwTask* in, const uint32_t* idx, uint64_t n, SwTask* out) {
@@ -555,6 +552,7 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
     sa.gap_extend = scr.gap_extend;
     sa.score = scores;
     sa.best_row = best_row;
+    sa.cells_eval = cells_gpu;
     std::memcpy(sa.scores625, scr.scores, 625);
     uint64_t lo[kSwClasses], hi[kSwClasses];
     for (int k = 0; k < kSwClasses; ++k) {

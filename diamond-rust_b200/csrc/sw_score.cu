@@ -187,6 +187,7 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS >= 2 ? 3 : 1) k_sw(SwScoreAr
   int base = 0;  // ring slot of relative column 0 of the current strip
   SRegs R;
   int best = 0, best_i = 0;
+  uint64_t steps_done = 0;  // column steps run (all strips)
   for (uint32_t k = 0; k < task.n_strips; ++k) {
     const int i0 = (int)task.row_first + (int)(k * kRows);
     // strip profile: prof[res * stride + r] = S(q[i0 + r - 1], res)
@@ -209,26 +210,64 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS >= 2 ? 3 : 1) k_sw(SwScoreAr
     }
     R.mx0 = R.mx1 = 0;
     R.E7 = kNeg2;
-    rg.rp = ring + base * stride;
-    rg.wp = ring + (base == 0 ? buf - 1 : base - 1) * stride;
-    R.htop_old = *rg.wp & 0xFFFFu;
+    // Steps whose cells all lie off the matrix for every lane of the warp are
+    // skipped: at step c a lane's cells sit at subject columns jbase + c (rows
+    // 0-7) and jbase + c - 1 (rows 8-15), all j <= 0 for c <= -jbase and all
+    // j > m for c >= m + 2 - jbase.  Such cells are H = 0 on the left and can
+    // never exceed an in-matrix value on the right, so only the ring words a
+    // later strip reads need care (below).
+    const int lead = __reduce_min_sync(0xFFFFFFFFu, max(0, 1 - L.jbase));
+    const int trail = __reduce_max_sync(0xFFFFFFFFu, L.m + 2 - L.jbase);
+    const int c_begin = lead >= kRows ? min(lead, Wmin) : 0;  // whole prologue or none of it
+    const int c_end = max(c_begin, min(W + kRows, max(trail, kRows)));
+    steps_done += (uint64_t)(c_end - c_begin);
     {
-      const int jm1 = L.jbase - 2;  // column -1
+      int slot = base + c_begin;
+      slot = slot >= buf ? slot - buf : slot;
+      rg.rp = ring + slot * stride;
+      rg.wp = ring + (slot == 0 ? buf - 1 : slot - 1) * stride;
+    }
+    R.htop_old = *rg.wp & 0xFFFFu;  // column c_begin - 1 of the row above
+    {
+      const int jm1 = L.jbase + c_begin - 2;  // column c_begin - 1
       R.res_prev = subject_residue(L, jm1);
-      L.r0 = subject_residue(L, jm1 + 1);  // columns 0 and 1
+      L.r0 = subject_residue(L, jm1 + 1);  // columns c_begin and c_begin + 1
       L.r1 = subject_residue(L, jm1 + 2);
     }
-    Unroll<1, 0>::run(R, L, 0, prof, rg, noc2, nge2);
-    for (int c = kRows; c < Wmin; ++c) {
+    int c = c_begin;
+    if (c_begin == 0) {
+      Unroll<1, 0>::run(R, L, 0, prof, rg, noc2, nge2);
+      c = kRows;
+    }
+    const int mid_end = min(Wmin, c_end);
+    for (; c < mid_end; ++c) {
       sw_step<0, 0>(R, L, c, prof, rg.rp, rg.wp, noc2, nge2);
       rg.advance();
     }
-    if (Wmin == W) {  // one width in the warp: compile-time masks
+    if (Wmin == W && c == W && c_end == W + kRows) {  // one width in the warp: compile-time masks
       Unroll<2, 0>::run(R, L, W, prof, rg, noc2, nge2);
-    } else {          // mixed widths: each lane masks past its own right edge
-      for (int c = Wmin; c < W + kRows; ++c) {
+    } else {  // mixed widths or an early stop: each lane masks past its own right edge
+      for (; c < c_end; ++c) {
         sw_step<3, 0>(R, L, c, prof, rg.rp, rg.wp, noc2, nge2, c - Wl);
         rg.advance();
+      }
+    }
+    // Ring words the next strip may read that this strip did not write: the
+    // next strip's column x reads this strip's column x + 16.  Skipped columns
+    // on the left hold dead cells (H = 0, E = -inf); past the early stop the
+    // next strip computes only off-matrix cells, which must see -inf.
+    for (int x = kRows - 1; x <= c_begin - 2; ++x) {
+      int ls = base + x;
+      ls = ls >= buf ? ls - buf : ls;
+      ring[ls * stride] = 0xC0000000u;
+    }
+    if (c_end < W + kRows) {
+      const int x_hi = min(W + kRows - 1, max(c_end - 1, 2 * kRows - 1));
+      for (int x = c_end - 1; x <= x_hi; ++x) {
+        int ls = base + x;
+        ls = ls >= buf ? ls - buf : ls;
+        ls = ls >= buf ? ls - buf : ls;
+        ring[ls * stride] = kNeg2;
       }
     }
     // this lane's column Wl + 15 is the next strip's column Wl - 1: outside
@@ -249,6 +288,7 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS >= 2 ? 3 : 1) k_sw(SwScoreAr
       best_i = i0 + kRows - 1;
     }
   }
+  if (lane == 0 && a.cells_eval) atomicAdd(a.cells_eval, (unsigned long long)(steps_done * kRows * task.count));
   if (!active) return;
   a.score[bidx] = best;
   if (a.best_row) a.best_row[bidx] = best_i;
