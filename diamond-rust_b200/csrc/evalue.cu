@@ -131,6 +131,28 @@ __host__ __device__ uint64_t band_cells(uint32_t n, uint32_t m, int32_t d0, int3
 uint64_t band_cells_host(uint32_t n, uint32_t m, int32_t d0, int32_t d1) { return band_cells(n, m, d0, d1); }
 
 namespace {
+// E-value verdict of every band: 1 fails, 2 passes, 3 too close to the
+// threshold to decide on the device (the host ALP settles it).  Independent per
+// band (it depends on score, qlen, slen only), so one thread per band.
+__global__ void k_band_verdict(SelectArgs a) {
+  const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= a.n_bands) return;
+  const int sc = a.score[i];
+  if (sc <= 0) {
+    a.verdict[i] = 1;
+    return;
+  }
+  const Band bd = a.bands[i];
+  const uint32_t slen = (uint32_t)(a.s_offsets[bd.subject + 1] - a.s_offsets[bd.subject]);
+  const uint64_t qlen = a.q_offsets[bd.target + 1] - a.q_offsets[bd.target];
+  const double lo_thr = a.evalue * (1.0 - 1e-9), hi_thr = a.evalue * (1.0 + 1e-9);
+  const double ev = alp_evalue_dev(a.alp, sc, qlen, slen, a.db_letters);
+  a.verdict[i] = ev <= lo_thr ? 2 : ((ev > hi_thr || isnan(ev)) ? 1 : 3);
+}
+
+// The reference's walk over a pair's bands in rank order (search.rs:233-255):
+// bands are computed until max_hsps pass; an undecided verdict stops the
+// device walk and leaves the rest of the pair to the host.
 __global__ void k_select(SelectArgs a) {
   uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (p >= a.n_pairs) return;
@@ -138,7 +160,6 @@ __global__ void k_select(SelectArgs a) {
   uint32_t kept = 0;
   bool undecided = false;
   unsigned long long cells = 0, computed = 0;
-  const double lo_thr = a.evalue * (1.0 - 1e-9), hi_thr = a.evalue * (1.0 + 1e-9);
   for (uint64_t i = b; i < e; ++i) {
     if (undecided) {
       a.state[i] = 3;
@@ -150,24 +171,12 @@ __global__ void k_select(SelectArgs a) {
     }
     const Band bd = a.bands[i];
     const uint32_t slen = (uint32_t)(a.s_offsets[bd.subject + 1] - a.s_offsets[bd.subject]);
-    const uint64_t qlen = a.q_offsets[bd.target + 1] - a.q_offsets[bd.target];
     cells += band_cells(bd.n, slen, bd.d0, bd.d1);
     ++computed;
-    const int sc = a.score[i];
-    if (sc <= 0) {
-      a.state[i] = 1;
-      continue;
-    }
-    const double ev = alp_evalue_dev(a.alp, sc, qlen, slen, a.db_letters);
-    if (ev <= lo_thr) {
-      a.state[i] = 2;
-      ++kept;
-    } else if (ev > hi_thr || isnan(ev)) {
-      a.state[i] = 1;
-    } else {
-      a.state[i] = 3;
-      undecided = true;
-    }
+    const uint8_t v = a.verdict[i];
+    a.state[i] = v;
+    if (v == 2) ++kept;
+    else if (v == 3) undecided = true;
   }
   atomicAdd(a.cells_ref, cells);
   atomicAdd(a.n_computed, computed);
@@ -176,6 +185,10 @@ __global__ void k_select(SelectArgs a) {
 
 void launch_select(const SelectArgs& a, cudaStream_t st) {
   if (a.n_pairs == 0) return;
+  if (a.n_bands > 0) {
+    count_launch();
+    k_band_verdict<<<ceil_div(a.n_bands, 128), 128, 0, st>>>(a);
+  }
   count_launch();
   k_select<<<ceil_div(a.n_pairs, 128), 128, 0, st>>>(a);
   DRG_CUDA(cudaGetLastError());

@@ -254,7 +254,8 @@ struct SelectArgs {
   AlpDev alp;
   double evalue;
   uint32_t max_hsps;
-  uint8_t* state;  // per band: 0 skipped, 1 computed-failed, 2 selected, 3 undecided
+  uint8_t* state;    // per band: 0 skipped, 1 computed-failed, 2 selected, 3 undecided
+  uint8_t* verdict;  // per band scratch: the E-value verdict (1 fail, 2 pass, 3 undecided)
   unsigned long long* cells_ref;
   unsigned long long* n_computed;
 };

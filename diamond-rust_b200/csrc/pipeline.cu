@@ -936,6 +936,7 @@ void Search::chunk(uint64_t chunk_id, uint64_t c0, uint64_t c1, uint64_t n_runs)
   ga.evalue = evalue;
   ga.max_hsps = (uint32_t)std::min<uint64_t>(max_hsps, 0xFFFFFFFFu);
   ga.state = state;
+  ga.verdict = c->verdict.as<uint8_t>(n_bands);
   ga.cells_ref = d_counters + 1;
   ga.n_computed = d_counters + 2;
   launch_select(ga, c->stream);
