@@ -408,8 +408,8 @@ int drg_extend_span_batch(drg_ctx* c, const uint8_t* ql, const uint64_t* qo, uin
   DevArr<uint32_t> dops(ooff + 1);
   DevArr<uint64_t> doff(n + 1);
   DevArr<int64_t> cnt(2);
-  DevArr<unsigned long long> cells(2);
-  DRG_CUDA(cudaMemsetAsync(cells.p, 0, 16, c->stream));
+  DevArr<unsigned long long> cells(3);  // evaluated, lane, issued cells
+  DRG_CUDA(cudaMemsetAsync(cells.p, 0, 3 * sizeof(unsigned long long), c->stream));
   if (n) {
     DRG_CUDA(cudaMemcpyAsync(db_.p, hb.data(), n * sizeof(Band), cudaMemcpyHostToDevice, c->stream));
     DRG_CUDA(cudaMemsetAsync(dout.p, 0, n * sizeof(ExactOut), c->stream));
@@ -489,8 +489,8 @@ int drg_extend_span_scores(drg_ctx* c, const uint8_t* ql, const uint64_t* qo, ui
   DevArr<Band> db_(n);
   DevArr<int32_t> ds(n);
   DevArr<int64_t> cnt(2);
-  DevArr<unsigned long long> cells(2);
-  DRG_CUDA(cudaMemsetAsync(cells.p, 0, 16, c->stream));
+  DevArr<unsigned long long> cells(3);  // evaluated, lane, issued cells
+  DRG_CUDA(cudaMemsetAsync(cells.p, 0, 3 * sizeof(unsigned long long), c->stream));
   if (n) DRG_CUDA(cudaMemcpyAsync(db_.p, hb.data(), n * sizeof(Band), cudaMemcpyHostToDevice, c->stream));
   drg_run_stats st{};
   run_bands(c, db_.p, n, qs.view(), ss.view(), sc, false, ds.p, nullptr, nullptr, nullptr, nullptr, nullptr, st, cnt.p,
@@ -514,6 +514,21 @@ int drg_db_create(drg_ctx* c, const uint8_t* letters, const uint64_t* offsets, u
 void drg_db_destroy(drg_db* d) {
   if (d) cudaSetDevice(d->ctx->device);
   free_db(d);
+}
+
+int drg_db_set_index_budget(drg_db* d, uint64_t budget_bytes) {
+  if (!d || !d->cache) return DRG_ERR_INVALID;
+  drg_ctx* c = d->ctx;
+  API_BEGIN(c)
+  d->cache->set_budget(budget_bytes);
+  API_END(c)
+}
+
+int drg_db_index_stats(const drg_db* d, drg_index_stats* out) {
+  if (!d || !d->cache || !out) return DRG_ERR_INVALID;
+  const auto s = d->cache->stats();
+  *out = drg_index_stats{s.entries, s.bytes, s.hits, s.misses, s.evictions};
+  return DRG_OK;
 }
 
 int drg_batch_create(drg_ctx* c, const uint8_t* letters, const uint64_t* offsets, const uint32_t* query,

@@ -2,10 +2,12 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <memory>
 #include <string>
 #include <vector>
 
 #include "common.cuh"
+#include "index_cache.h"
 #include "drgpu.h"
 #include "host/presets.h"
 #include "host/scoring.h"
@@ -43,6 +45,7 @@ struct drg_db {
   std::vector<uint64_t> h_offsets;
   uint64_t n = 0, total = 0;
   uint32_t max_len = 0;
+  std::unique_ptr<drg::IndexCache> cache;  // sorted reference seeds kept for later searches
 };
 
 struct drg_batch {

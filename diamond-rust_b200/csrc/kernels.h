@@ -156,7 +156,7 @@ struct SwScoreArgs {
   int gap_open, gap_extend;
   int32_t* score;     // score mode: per band (indexed like bands)
   int32_t* best_row;  // score mode: first DP row holding the best (0 if none)
-  unsigned long long* cells_eval;  // optional: DP cells the kernel evaluated (after skipping)
+  unsigned long long* cells_eval;  // optional: [0] DP cells the lanes evaluated (after skipping), [2] the warps' (idle lanes too)
   uint2* trace;       // trace mode: nibble buffer
   TraceBand* tband;   // trace mode: per band (indexed like bands)
   int8_t scores625[628];  // substitution scores, row-major

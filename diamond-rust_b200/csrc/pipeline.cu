@@ -676,7 +676,8 @@ struct Search {
   std::vector<Candidate> cands;
   // device scratch for counters
   int64_t* d_count = nullptr;
-  unsigned long long* d_counters = nullptr;  // [0] xdrops [1] cells_ref [2] computed [3] cells_gpu [4] lane cells
+  // [0] xdrops [1] cells_ref [2] computed [3] cells_gpu [4] lane cells [5] issued cells
+  unsigned long long* d_counters = nullptr;
 
   void configure(const drg_search_config* cfg) {
     std::string err;
@@ -721,6 +722,19 @@ struct Search {
     upload_seed_params(t, p, c->slot, c->stream);
     upload_score_matrix(sc.scores, c->slot, c->stream);
     upload_alp_tables(c->stream);
+  }
+
+  // What the sorted reference seeds of chunk [c0, c1) depend on.
+  std::string index_key(uint64_t c0, uint64_t c1) const {
+    std::string k;
+    for (const auto& sh : shapes) k += sh.code + ",";
+    k += "|";
+    for (int i = 0; i < 25; ++i) k += std::to_string((int)red.bucket[i]) + ".";
+    uint64_t cut_bits;
+    std::memcpy(&cut_bits, &complexity_cut, sizeof cut_bits);
+    k += "|" + std::to_string(red.size) + "|" + std::to_string(cut_bits) + "|" + std::to_string(seed_key_bits) + "|" +
+         std::to_string(c0) + "-" + std::to_string(c1);
+    return k;
   }
 
   HitKeyLayout layout() const {
@@ -779,18 +793,33 @@ void Search::chunk(uint64_t chunk_id, uint64_t c0, uint64_t c1, uint64_t n_runs)
   const int S = (int)shapes.size();
   const uint64_t lo = db->h_offsets[c0], hi = db->h_offsets[c1];
   const uint64_t N = (hi - lo) * (uint64_t)S;
-  // ---- reference seeds + join
+  // ---- reference seeds (or the database's cached index of them) + join
   tm.start();
-  uint64_t* keys = c->r_keys.as<uint64_t>(N);
-  uint32_t* vals = c->r_vals.as<uint32_t>(N);
-  uint64_t* keys_s = c->r_keys_s.as<uint64_t>(N);
-  uint32_t* vals_s = c->r_vals_s.as<uint32_t>(N);
-  launch_seed_enum(db->letters, db->offsets, db->owner + lo, lo, hi, S, keys, vals, c->slot, c->stream);
-  cub_call(c, [&](void* t, size_t& b) {
-    return cub::DeviceRadixSort::SortPairs(t, b, keys, keys_s, vals, vals_s, (int64_t)N, 0, seed_key_bits,
-                                           c->stream);
-  });
-  int64_t nr = count_valid(c, keys_s, N, d_count);
+  IndexCache* cache = db->cache && db->cache->budget() > 0 ? db->cache.get() : nullptr;
+  const std::string ikey = cache ? index_key(c0, c1) : std::string();
+  std::shared_ptr<SeedIndex> held = cache ? cache->find(ikey) : nullptr;  // kept until the join has read it
+  const uint64_t* keys_s;
+  const uint32_t* vals_s;
+  int64_t nr;
+  if (held) {
+    keys_s = held->keys;
+    vals_s = held->vals;
+    nr = (int64_t)held->n;
+    st.index_hits += 1;
+  } else {
+    uint64_t* keys = c->r_keys.as<uint64_t>(N);
+    uint32_t* vals = c->r_vals.as<uint32_t>(N);
+    uint64_t* ks = c->r_keys_s.as<uint64_t>(N);
+    uint32_t* vs = c->r_vals_s.as<uint32_t>(N);
+    launch_seed_enum(db->letters, db->offsets, db->owner + lo, lo, hi, S, keys, vals, c->slot, c->stream);
+    cub_call(c, [&](void* t, size_t& b) {
+      return cub::DeviceRadixSort::SortPairs(t, b, keys, ks, vals, vs, (int64_t)N, 0, seed_key_bits, c->stream);
+    });
+    nr = count_valid(c, ks, N, d_count);
+    keys_s = ks;
+    vals_s = vs;
+    if (cache) held = cache->insert(ikey, ks, vs, (uint64_t)nr, c->stream);
+  }
   st.ref_seeds += (uint64_t)nr;
   uint32_t* rlo = c->run_rlo.as<uint32_t>(n_runs + 1);
   uint32_t* rcnt = c->run_rcount.as<uint32_t>(n_runs + 1);
@@ -1159,7 +1188,7 @@ void Search::run(drg_result* out) {
     for (auto [c0, c1] : split_chunks(db->n, index_chunks)) chunk(cid++, c0, c1, n_runs);
   }
   finish(out);
-  unsigned long long cnt[5];
+  unsigned long long cnt[6];
   DRG_CUDA(cudaMemcpyAsync(cnt, d_counters, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
   DRG_CUDA(cudaStreamSynchronize(c->stream));
   st.xdrops = cnt[0];
@@ -1167,6 +1196,7 @@ void Search::run(drg_result* out) {
   st.bands_computed = cnt[2];
   st.dp_cells_gpu = cnt[3];
   st.dp_cells_lane = cnt[4];
+  st.dp_cells_issued = cnt[5];
   st.ms_total = total.stop();
   st.kernel_launches = kernel_launch_count() - launches0;
   out->stats = st;
@@ -1207,6 +1237,7 @@ drg_db* make_db(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offsets, u
     }
     d->max_len = std::max<uint32_t>(d->max_len, (uint32_t)(offsets[i + 1] - offsets[i]));
   }
+  d->cache.reset(new IndexCache(ctx->device));
   try {
     pool_alloc(ctx, &d->letters, d->total + 64);
     pool_alloc(ctx, &d->offsets, (n + 1) * sizeof(uint64_t));
@@ -1268,6 +1299,7 @@ drg_batch* make_batch(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offs
 
 void free_db(drg_db* d) {
   if (!d) return;
+  d->cache.reset();
   pool_free(d->ctx, d->letters);
   pool_free(d->ctx, d->offsets);
   pool_free(d->ctx, d->owner);

@@ -288,7 +288,10 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS >= 2 ? 3 : 1) k_sw(SwScoreAr
       best_i = i0 + kRows - 1;
     }
   }
-  if (lane == 0 && a.cells_eval) atomicAdd(a.cells_eval, (unsigned long long)(steps_done * kRows * task.count));
+  if (lane == 0 && a.cells_eval) {
+    atomicAdd(a.cells_eval, (unsigned long long)(steps_done * kRows * task.count));
+    atomicAdd(a.cells_eval + 2, (unsigned long long)(steps_done * kRows * 32));  // idle lanes included
+  }
   if (!active) return;
   a.score[bidx] = best;
   if (a.best_row) a.best_row[bidx] = best_i;

@@ -87,7 +87,8 @@ class RunStats(C.Structure):
                [("sw_launches", C.c_uint64), ("kernel_launches", C.c_uint64), ("exact_bands", C.c_uint64),
                 ("sw_class_tasks", C.c_uint64 * 4), ("sw_class_max_steps", C.c_uint64 * 4),
                 ("ms_sw_class", C.c_double * 4), ("ms_trace_kernel", C.c_double), ("dp_cells_lane", C.c_uint64),
-                ("sw_wide_bands", C.c_uint64), ("ms_sw_wide", C.c_double)]
+                ("sw_wide_bands", C.c_uint64), ("ms_sw_wide", C.c_double), ("dp_cells_issued", C.c_uint64),
+                ("index_hits", C.c_uint64)]
 
     def as_dict(self):
         d = {}
@@ -134,6 +135,8 @@ _SIGNATURES = {
                                           C.c_void_p, C.c_uint64, C.c_void_p, C.c_char_p, C.c_size_t]),
     "drg_db_create": (C.c_int, [C.c_void_p, _u8p, _u64p, C.c_uint64, _P(C.c_void_p)]),
     "drg_db_destroy": (None, [C.c_void_p]),
+    "drg_db_set_index_budget": (C.c_int, [C.c_void_p, C.c_uint64]),
+    "drg_db_index_stats": (C.c_int, [C.c_void_p, C.c_void_p]),
     "drg_batch_create": (C.c_int, [C.c_void_p, _u8p, _u64p, _u32p, _u8p, C.c_uint64, _P(C.c_void_p)]),
     "drg_batch_create_requests": (C.c_int, [C.c_void_p, _u8p, _u64p, _u32p, _u8p, _u32p, C.c_uint64,
                                             _P(C.c_void_p)]),
@@ -412,16 +415,34 @@ class Context:
         return ops.value, mhz.value
 
 
-class ResidentDb:
-    """Database letters resident in device memory (drg_db)."""
+class IndexStats(C.Structure):
+    _fields_ = [("entries", C.c_uint64), ("bytes", C.c_uint64), ("hits", C.c_uint64), ("misses", C.c_uint64),
+                ("evictions", C.c_uint64)]
 
-    def __init__(self, ctx: Context, letters, offsets):
+
+class ResidentDb:
+    """Database letters resident in device memory (drg_db).
+
+    index_budget > 0 keeps the sorted reference seeds of each preset and index
+    chunk in device memory for later searches (drg_db_set_index_budget)."""
+
+    def __init__(self, ctx: Context, letters, offsets, index_budget=0):
         self.ctx = ctx
         self._l, lp = _u8(letters if len(letters) else np.zeros(1, np.uint8))
         self._o, op = _u64(offsets)
         h = C.c_void_p()
         ctx._check(ctx.lib.drg_db_create(ctx.h, lp, op, len(offsets) - 1, C.byref(h)))
         self.h = h
+        if index_budget:
+            self.set_index_budget(index_budget)
+
+    def set_index_budget(self, nbytes):
+        self.ctx._check(self.ctx.lib.drg_db_set_index_budget(self.h, int(nbytes)))
+
+    def index_stats(self):
+        s = IndexStats()
+        self.ctx._check(self.ctx.lib.drg_db_index_stats(self.h, C.byref(s)))
+        return {k: int(getattr(s, k)) for k, _ in IndexStats._fields_}
 
     def close(self):
         if self.h:

@@ -66,9 +66,10 @@ class Server:
     """Continuous-batching request loop over one resident database."""
 
     def __init__(self, db_letters, db_offsets, workers=2, batch=True, budget_letters=4_000_000, device=0,
-                 index_chunks=None):
+                 index_chunks=None, index_budget=0):
         self.ctxs = [Context(device) for _ in range(workers)]
-        self.db = ResidentDb(self.ctxs[0], db_letters, db_offsets)
+        # index_budget > 0: each preset's sorted reference seeds stay resident
+        self.db = ResidentDb(self.ctxs[0], db_letters, db_offsets, index_budget=index_budget)
         self.batch = batch
         self.budget = budget_letters
         self.index_chunks = index_chunks

@@ -107,6 +107,8 @@ typedef struct {
   uint64_t dp_cells_lane;          /* score kernel: each band's own rows x (W + 16), without warp padding */
   uint64_t sw_wide_bands;          /* score pass: bands wider than 272 columns, one warp per band */
   double ms_sw_wide;               /* device time of their launch (concurrent with the classes) */
+  uint64_t dp_cells_issued;        /* score kernel: warps x column steps x 16 x 32, idle lanes included */
+  uint64_t index_hits;             /* index chunks whose sorted reference seeds came from the db's cache */
 } drg_run_stats;
 
 /* search::run result: per-target HSP lists, target_offsets[n_targets+1]. */
@@ -193,6 +195,20 @@ int drg_extend_span_noalloc(const uint8_t* d_q_letters, const uint64_t* q_offset
 /* Database resident in device memory: letters[offsets[i]..offsets[i+1]]. */
 int drg_db_create(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offsets, uint64_t n_seqs, drg_db** out);
 void drg_db_destroy(drg_db* db);  /* before the db's context is destroyed */
+
+/* Seed index cache of a resident database.  drg_search_batch enumerates and
+ * sorts the reference seeds of every index chunk it covers, as the reference
+ * does on every run (search.rs:104-126).  With a budget > 0 the sorted seeds of
+ * each (shape set, reduction, complexity cut, index chunk) stay in device
+ * memory (12 bytes per seed) for later searches from any context, the least
+ * recently used leaving first when the held bytes pass the budget.  Results
+ * are the same with or without it.  0 (the default) holds nothing and frees
+ * what is held. */
+int drg_db_set_index_budget(drg_db* db, uint64_t budget_bytes);
+typedef struct {
+  uint64_t entries, bytes, hits, misses, evictions;
+} drg_index_stats;
+int drg_db_index_stats(const drg_db* db, drg_index_stats* out);
 
 /* Query batch (search::Target list, search.rs:82-88) resident in device memory. */
 int drg_batch_create(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offsets, const uint32_t* query_index,

@@ -34,6 +34,12 @@ def test_library_exports_every_declared_function():
     assert sorted(drgpu.exported_symbols()) == names
 
 
+def test_index_budget_on_a_null_db_is_an_error():
+    lib = drgpu.load_library()
+    assert lib.drg_db_set_index_budget(None, 1) == 1  # DRG_ERR_INVALID
+    assert lib.drg_db_index_stats(None, None) == 1
+
+
 def test_version_names_the_target():
     lib = drgpu.load_library()
     assert b"sm_100a" in lib.drg_version()
