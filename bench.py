@@ -300,9 +300,9 @@ def main():
     launches = sum(s["kernel_launches"] for s in steps)
 
     # ---- resident seed index: the DB's sorted reference seeds kept in HBM
-    # across searches (built by the first warm-up search), not part of value
+    # across searches (built by the first, untimed search), not part of value
     idb = drgpu.ResidentDb(ctx, dl, do, index_budget=16 << 30)
-    for _ in range(args.warmup):
+    for _ in range(max(1, args.warmup)):
         drgpu.search_resident(ctx, idb, batch, cfg, want_lists=False)
     isteps = []
     barrier_sync(world)

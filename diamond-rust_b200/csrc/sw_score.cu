@@ -46,7 +46,7 @@ struct SRegs {
   uint32_t H[kPairs], Hm[kPairs], F[kPairs];
   uint32_t E7;        // E of pair 7 at the previous step
   uint32_t htop_old;  // top H of the previous step (D operand of pair 0)
-  uint32_t res_prev;  // subject residue of the previous column
+  const uint8_t* prow_prev;  // profile row of the previous column's residue
   uint32_t mx0, mx1;  // maximum H of the strip so far, folded over rows
 };
 
@@ -60,9 +60,10 @@ __device__ __forceinline__ void sw_step(SRegs& R, Lane& L, int c, const uint8_t*
                                         const uint32_t* __restrict__ rp, uint32_t* __restrict__ wp, uint32_t noc2,
                                         uint32_t nge2, int cw = 0) {
   const uint32_t res = next_residue(L, c);  // subject residue of this column
-  const uint2 lo8 = *reinterpret_cast<const uint2*>(prof + res * kProfStride);
-  const uint2 hi8 = *reinterpret_cast<const uint2*>(prof + R.res_prev * kProfStride + 8);
-  R.res_prev = res;
+  const uint8_t* prow = prof + res * kProfStride;
+  const uint2 lo8 = *reinterpret_cast<const uint2*>(prow);
+  const uint2 hi8 = *reinterpret_cast<const uint2*>(R.prow_prev + 8);
+  R.prow_prev = prow;
   const uint32_t rw = *rp;  // (H, E) of the row above row 0, column c
   const uint32_t htop = prmt(rw, R.H[kPairs - 1], 0x5410);
   uint32_t e_up = prmt(rw, R.E7, 0x5432);
@@ -230,7 +231,7 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS >= 2 ? 3 : 1) k_sw(SwScoreAr
     R.htop_old = *rg.wp & 0xFFFFu;  // column c_begin - 1 of the row above
     {
       const int jm1 = L.jbase + c_begin - 2;  // column c_begin - 1
-      R.res_prev = subject_residue(L, jm1);
+      R.prow_prev = prof + subject_residue(L, jm1) * kProfStride;
       L.r0 = subject_residue(L, jm1 + 1);  // columns c_begin and c_begin + 1
       L.r1 = subject_residue(L, jm1 + 2);
     }
@@ -240,9 +241,23 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS >= 2 ? 3 : 1) k_sw(SwScoreAr
       c = kRows;
     }
     const int mid_end = min(Wmin, c_end);
-    for (; c < mid_end; ++c) {
-      sw_step<0, 0>(R, L, c, prof, rg.rp, rg.wp, noc2, nge2);
-      rg.advance();
+    {
+      // in runs that end where the read pointer wraps, so that the steps
+      // themselves carry no wrap test
+      uint32_t* rp = rg.rp;
+      uint32_t* wp = rg.wp;
+      while (c < mid_end) {
+        const int stop = min(mid_end, c + (int)((rg.end - rp) / stride));
+#pragma unroll 2
+        for (; c < stop; ++c) {
+          sw_step<0, 0>(R, L, c, prof, rp, wp, noc2, nge2);
+          wp = rp;
+          rp += stride;
+        }
+        if (rp == rg.end) rp = rg.begin;
+      }
+      rg.rp = rp;
+      rg.wp = wp;
     }
     if (Wmin == W && c == W && c_end == W + kRows) {  // one width in the warp: compile-time masks
       Unroll<2, 0>::run(R, L, W, prof, rg, noc2, nge2);
