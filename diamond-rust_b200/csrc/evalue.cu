@@ -154,9 +154,9 @@ __global__ void k_band_verdict(SelectArgs a) {
 // bands are computed until max_hsps pass; an undecided verdict stops the
 // device walk and leaves the rest of the pair to the host.
 __global__ void k_select(SelectArgs a) {
-  uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (p >= a.n_pairs) return;
-  uint64_t b = a.pair_first[p], e = a.pair_first[p + 1];
+  const uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  // threads past the last pair walk an empty range and join the reduction
+  const uint64_t b = p < a.n_pairs ? a.pair_first[p] : 0, e = p < a.n_pairs ? a.pair_first[p + 1] : 0;
   uint32_t kept = 0;
   bool undecided = false;
   unsigned long long cells = 0, computed = 0;
@@ -178,8 +178,8 @@ __global__ void k_select(SelectArgs a) {
     if (v == 2) ++kept;
     else if (v == 3) undecided = true;
   }
-  atomicAdd(a.cells_ref, cells);
-  atomicAdd(a.n_computed, computed);
+  warp_sum_atomic(a.cells_ref, cells);
+  warp_sum_atomic(a.n_computed, computed);
 }
 }  // namespace
 

@@ -1,12 +1,16 @@
 // Seed enumeration (shape.rs:60-75, seed.rs:46-104) and the sort-merge
 // double-index join (seed.rs:110-143) on the device.
 //
-// Layout: one thread per (letter, shape).  Letters of a sequence batch are
-// contiguous in HBM, so the w reads of a seed hit one or two 32-byte sectors
-// shared by neighbouring threads (L1 absorbs the reuse across shapes).  Seeds
-// are written as 64-bit keys (shape << 42 | key) with a 32-bit payload (the
-// global letter index) and radix-sorted by CUB; the join walks query key runs
-// and binary-searches the sorted reference keys (they stay L2-resident).
+// Layout: one thread per letter, looping over the shapes, so that a warp
+// reads each shape's table entries at one constant address (a broadcast) and
+// writes each shape's keys as one coalesced run: entry s * L + i holds shape
+// s at letter i.  Letters of a sequence batch are contiguous in HBM, so the w
+// reads of a seed hit one or two 32-byte sectors shared by neighbouring
+// threads.  Seeds are written as 64-bit keys (request | shape | key) with a
+// 32-bit payload (the global letter index) and radix-sorted by CUB (stable:
+// equal keys share a shape and stay in letter order, as in the reference's
+// build); the join walks query key runs and binary-searches the sorted
+// reference keys.
 #include "kernels.h"
 
 namespace drg {
@@ -48,8 +52,11 @@ void launch_letter_owner(const uint64_t* offsets, uint64_t n_seqs, uint64_t lo, 
 // One seed: the reduced key and the log-multinomial complexity test.  The
 // counts live in three 64-bit words (8 buckets x 8 bits each); the entropy is
 // lnfact[w] minus lnfact[c_b] for b = 0, 1, ... in bucket order, the order the
-// reference subtracts in, so the double result is identical.
-__device__ __forceinline__ bool seed_at(const uint8_t* __restrict__ p, int s, int slot, uint64_t* key_out) {
+// reference subtracts in, so the double result is identical.  The bucket and
+// ln-factorial tables are indexed by per-lane data, so they are read from
+// shared copies (constant memory serialises distinct addresses in a warp).
+__device__ __forceinline__ bool seed_at(const uint8_t* __restrict__ p, int s, int slot, const uint8_t* bucket,
+                                        const double* lnfact, uint64_t* key_out) {
   const ShapeTable& shp = c_shapes[slot];
   const SeedParams& sp = c_seed[slot];
   const int w = shp.weight[s];
@@ -58,7 +65,7 @@ __device__ __forceinline__ bool seed_at(const uint8_t* __restrict__ p, int s, in
   for (int k = 0; k < w; ++k) {
     uint32_t l = p[shp.pos[s][k]];
     if (l >= 20) return false;
-    uint32_t b = sp.bucket[l];
+    uint32_t b = bucket[l];
     if (b >= 24) return false;
     key = key * size + b;
     uint64_t inc = 1ull << (8 * (b & 7));
@@ -68,11 +75,11 @@ __device__ __forceinline__ bool seed_at(const uint8_t* __restrict__ p, int s, in
   }
   const double cut = sp.cut;
   if (cut > 0.0) {
-    double e = sp.lnfact[w];
+    double e = lnfact[w];
     for (int b = 0; b < (int)size; ++b) {
       uint64_t word = b < 8 ? c0 : (b < 16 ? c1 : c2);
       uint32_t c = (uint32_t)(word >> (8 * (b & 7))) & 0xffu;
-      if (c > 0) e = __dsub_rn(e, sp.lnfact[c]);
+      if (c > 0) e = __dsub_rn(e, lnfact[c]);
     }
     if (!(e >= cut)) return false;
   }
@@ -84,29 +91,34 @@ __global__ void k_seed_enum(const uint8_t* __restrict__ letters, const uint64_t*
                             const uint32_t* __restrict__ owner, uint64_t lo, uint64_t hi, int n_shapes,
                             uint64_t* __restrict__ keys, uint32_t* __restrict__ vals,
                             const uint32_t* __restrict__ request, int slot) {
-  uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  uint64_t n = (hi - lo) * (uint64_t)n_shapes;
-  if (t >= n) return;
-  uint64_t g = lo + t / n_shapes;
-  int s = (int)(t % n_shapes);
-  uint32_t seq = owner[g - lo];
-  uint64_t end = offsets[seq + 1];
-  uint64_t key = 0;
-  bool ok = g + c_shapes[slot].span[s] <= end && seed_at(letters + g, s, slot, &key);
+  __shared__ uint8_t bucket[32];
+  __shared__ double lnfact[33];
+  if (threadIdx.x < 32) bucket[threadIdx.x] = c_seed[slot].bucket[threadIdx.x];
+  if (threadIdx.x < 33) lnfact[threadIdx.x] = c_seed[slot].lnfact[threadIdx.x];
+  __syncthreads();
+  const uint64_t L = hi - lo;
+  const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= L) return;
+  const uint64_t g = lo + i;
+  const uint32_t seq = owner[i];
+  const uint64_t end = offsets[seq + 1];
   const SeedParams& sp = c_seed[slot];
   const uint64_t req = request ? (uint64_t)request[seq] << sp.request_shift : 0;
-  keys[t] = ok ? req | ((uint64_t)s << sp.shape_shift) | key : kNoSeed;
-  vals[t] = (uint32_t)g;
+  for (int s = 0; s < n_shapes; ++s) {
+    uint64_t key = 0;
+    const bool ok = g + c_shapes[slot].span[s] <= end && seed_at(letters + g, s, slot, bucket, lnfact, &key);
+    keys[s * L + i] = ok ? req | ((uint64_t)s << sp.shape_shift) | key : kNoSeed;
+    vals[s * L + i] = (uint32_t)g;
+  }
 }
 
 void launch_seed_enum(const uint8_t* letters, const uint64_t* offsets, const uint32_t* owner, uint64_t lo,
                       uint64_t hi, int n_shapes, uint64_t* keys, uint32_t* vals, int slot, cudaStream_t st,
                       const uint32_t* request) {
-  uint64_t n = (hi - lo) * (uint64_t)n_shapes;
-  if (n == 0) return;
+  if (hi <= lo || n_shapes == 0) return;
   count_launch();
-  k_seed_enum<<<ceil_div(n, 256), 256, 0, st>>>(letters, offsets, owner, lo, hi, n_shapes, keys, vals, request,
-                                                slot);
+  k_seed_enum<<<ceil_div(hi - lo, 256), 256, 0, st>>>(letters, offsets, owner, lo, hi, n_shapes, keys, vals, request,
+                                                     slot);
   DRG_CUDA(cudaGetLastError());
 }
 

@@ -315,6 +315,9 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS >= 2 ? 3 : 1) k_sw(SwScoreAr
 // Traceback of one band through the nibbles of the trace pass, in the
 // reference's order and with its stopping rules (gapped.rs:205-279).
 __global__ void k_sw_walk(SwWalkArgs a) {
+  __shared__ int8_t mat[625];  // lanes look up unrelated pairs: shared, not parameter space
+  for (int i = threadIdx.x; i < 625; i += blockDim.x) mat[i] = a.scores625[i];
+  __syncthreads();
   const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (t >= a.n_bands) return;
   const Band b = a.bands[t];
@@ -363,7 +366,7 @@ __global__ void k_sw_walk(SwWalkArgs a) {
         R.length++;
         if (x == y) R.identities++;
         else R.mismatches++;
-        if (a.scores625[(x < 24 ? x : 24) * 25 + (y < 24 ? y : 24)] > 0) R.positives++;
+        if (mat[(x < 24 ? x : 24) * 25 + (y < 24 ? y : 24)] > 0) R.positives++;
         rev[nrev++] = 0;
         in_gap = false;
         --i;

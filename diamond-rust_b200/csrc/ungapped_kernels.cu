@@ -19,19 +19,26 @@ void upload_score_matrix(const int8_t* s, int slot, cudaStream_t st) {
   DRG_CUDA(cudaMemcpyToSymbolAsync(c_score, s, 625, (size_t)slot * 625, cudaMemcpyHostToDevice, st));
 }
 
-__device__ __forceinline__ int mscore(uint32_t a, uint32_t b, int slot) {
+// The lanes of a warp look up unrelated residue pairs: from shared memory
+// that costs a bank conflict at worst, from constant memory one serialised
+// access per distinct address.  Each block stages its slot's matrix first.
+__device__ __forceinline__ void stage_matrix(int8_t* mat, int slot) {
+  for (int i = threadIdx.x; i < 625; i += blockDim.x) mat[i] = c_score[slot][i];
+  __syncthreads();
+}
+__device__ __forceinline__ int mscore(uint32_t a, uint32_t b, const int8_t* mat) {
   a = a < 24 ? a : 24;
   b = b < 24 ? b : 24;
-  return c_score[slot][a * 25 + b];
+  return mat[a * 25 + b];
 }
 
 __device__ SegmentOut xdrop_dev(const uint8_t* __restrict__ q, uint32_t qlen, const uint8_t* __restrict__ s,
-                                uint32_t slen, uint32_t qa, uint32_t sa, int xd, int slot) {
+                                uint32_t slen, uint32_t qa, uint32_t sa, int xd, const int8_t* mat) {
   int score = 0, st = 0;
   uint32_t n = 1, delta = 0, len = 0;
   int64_t qi = (int64_t)qa - 1, si = (int64_t)sa - 1;
   while (score - st < xd && qi >= 0 && si >= 0) {
-    st += mscore(q[qi], s[si], slot);
+    st += mscore(q[qi], s[si], mat);
     if (st > score) {
       score = st;
       delta = n;
@@ -45,7 +52,7 @@ __device__ SegmentOut xdrop_dev(const uint8_t* __restrict__ q, uint32_t qlen, co
   st = score;
   n = 1;
   while (score - st < xd && qi < (int64_t)qlen && si < (int64_t)slen) {
-    st += mscore(q[qi], s[si], slot);
+    st += mscore(q[qi], s[si], mat);
     if (st > score) {
       score = st;
       len = n;
@@ -75,9 +82,9 @@ void launch_run_heads(const uint64_t* keys, uint64_t n, int shift, uint8_t* flag
   DRG_CUDA(cudaGetLastError());
 }
 
-__global__ void k_xdrop_runs(XdropArgs a) {
-  uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (r >= a.n_runs) return;
+// The hits of one (target, subject, diagonal) run, in spos order; returns the
+// number of X-drop extensions run.
+__device__ __forceinline__ unsigned long long xdrop_run(const XdropArgs& a, uint64_t r, const int8_t* mat) {
   uint64_t i = a.run_head_idx[r];
   const HitKeyLayout L = a.layout;
   const uint64_t run = a.hit_keys[i] >> L.pb;
@@ -89,13 +96,13 @@ __global__ void k_xdrop_runs(XdropArgs a) {
   const uint8_t* s = a.s_letters + a.s_offsets[sj];
   const uint32_t slen = (uint32_t)(a.s_offsets[sj + 1] - a.s_offsets[sj]);
   int64_t last_end = -1;  // s_end of the last kept segment of this run
-  unsigned long long nx = 0;
+  unsigned long long nx = 0;  // X-drop extensions run
   for (; i < a.n_hits && (a.hit_keys[i] >> L.pb) == run; ++i) {
     uint32_t spos = (uint32_t)(a.hit_keys[i] & ((1ull << L.pb) - 1));
     a.keep[i] = 0;
     if (last_end >= (int64_t)spos) continue;
     uint32_t qpos = (uint32_t)(diag + spos);
-    SegmentOut seg = xdrop_dev(q, qlen, s, slen, qpos, spos, a.xdrop, a.slot);
+    SegmentOut seg = xdrop_dev(q, qlen, s, slen, qpos, spos, a.xdrop, mat);
     ++nx;
     if (seg.score >= a.cutoff) {
       a.seg[i] = seg;
@@ -103,7 +110,16 @@ __global__ void k_xdrop_runs(XdropArgs a) {
       last_end = (int64_t)seg.s_start + seg.len;
     }
   }
-  if (nx) atomicAdd(a.xdrop_count, nx);
+  return nx;
+}
+
+__global__ void k_xdrop_runs(XdropArgs a) {
+  __shared__ int8_t mat[625];
+  stage_matrix(mat, a.slot);
+  const uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  unsigned long long nx = 0;
+  if (r < a.n_runs) nx = xdrop_run(a, r, mat);
+  warp_sum_atomic(a.xdrop_count, nx);
 }
 
 void launch_xdrop_runs(const XdropArgs& a, cudaStream_t st) {
@@ -116,11 +132,13 @@ void launch_xdrop_runs(const XdropArgs& a, cudaStream_t st) {
 __global__ void k_xdrop_jobs(const drg_xdrop_job* __restrict__ jobs, uint64_t n, const uint8_t* __restrict__ ql,
                              const uint64_t* __restrict__ qo, const uint8_t* __restrict__ sl,
                              const uint64_t* __restrict__ so, int xd, drg_segment* __restrict__ out, int slot) {
+  __shared__ int8_t mat[625];
+  stage_matrix(mat, slot);
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   drg_xdrop_job j = jobs[i];
   SegmentOut g = xdrop_dev(ql + qo[j.query], (uint32_t)(qo[j.query + 1] - qo[j.query]), sl + so[j.subject],
-                           (uint32_t)(so[j.subject + 1] - so[j.subject]), (uint32_t)j.qa, (uint32_t)j.sa, xd, slot);
+                           (uint32_t)(so[j.subject + 1] - so[j.subject]), (uint32_t)j.qa, (uint32_t)j.sa, xd, mat);
   drg_segment r;
   r.q_start = g.q_start;
   r.s_start = g.s_start;
