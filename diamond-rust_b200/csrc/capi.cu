@@ -408,8 +408,8 @@ int drg_extend_span_batch(drg_ctx* c, const uint8_t* ql, const uint64_t* qo, uin
   DevArr<uint32_t> dops(ooff + 1);
   DevArr<uint64_t> doff(n + 1);
   DevArr<int64_t> cnt(2);
-  DevArr<unsigned long long> cells(3);  // evaluated, lane, issued cells
-  DRG_CUDA(cudaMemsetAsync(cells.p, 0, 3 * sizeof(unsigned long long), c->stream));
+  DevArr<unsigned long long> cells(4);  // evaluated, lane, issued cells, transposed bands
+  DRG_CUDA(cudaMemsetAsync(cells.p, 0, 4 * sizeof(unsigned long long), c->stream));
   if (n) {
     DRG_CUDA(cudaMemcpyAsync(db_.p, hb.data(), n * sizeof(Band), cudaMemcpyHostToDevice, c->stream));
     DRG_CUDA(cudaMemsetAsync(dout.p, 0, n * sizeof(ExactOut), c->stream));
@@ -489,17 +489,20 @@ int drg_extend_span_scores(drg_ctx* c, const uint8_t* ql, const uint64_t* qo, ui
   DevArr<Band> db_(n);
   DevArr<int32_t> ds(n);
   DevArr<int64_t> cnt(2);
-  DevArr<unsigned long long> cells(3);  // evaluated, lane, issued cells
-  DRG_CUDA(cudaMemsetAsync(cells.p, 0, 3 * sizeof(unsigned long long), c->stream));
+  DevArr<unsigned long long> cells(4);  // evaluated, lane, issued cells, transposed bands
+  DRG_CUDA(cudaMemsetAsync(cells.p, 0, 4 * sizeof(unsigned long long), c->stream));
   if (n) DRG_CUDA(cudaMemcpyAsync(db_.p, hb.data(), n * sizeof(Band), cudaMemcpyHostToDevice, c->stream));
   drg_run_stats st{};
   run_bands(c, db_.p, n, qs.view(), ss.view(), sc, false, ds.p, nullptr, nullptr, nullptr, nullptr, nullptr, st, cnt.p,
             cells.p);
   if (n) DRG_CUDA(cudaMemcpyAsync(scores, ds.p, n * 4, cudaMemcpyDeviceToHost, c->stream));
-  unsigned long long cg = 0;
-  DRG_CUDA(cudaMemcpyAsync(&cg, cells.p, 8, cudaMemcpyDeviceToHost, c->stream));
+  unsigned long long cg[4] = {0, 0, 0, 0};
+  DRG_CUDA(cudaMemcpyAsync(cg, cells.p, sizeof(cg), cudaMemcpyDeviceToHost, c->stream));
   sync(c);
-  st.dp_cells_gpu = cg;
+  st.dp_cells_gpu = cg[0];
+  st.dp_cells_lane = cg[1];
+  st.dp_cells_issued = cg[2];
+  st.sw_transposed_bands = cg[3];
   if (stats) *stats = st;
   API_END(c)
 }

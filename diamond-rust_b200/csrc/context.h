@@ -31,7 +31,8 @@ struct drg_ctx {
   drg::DevBuf tband, task_size, task_off, trace, rev, ex_bands, ops_off, trace_out, task_max;
   drg::DevBuf sw_tasks_u, task_key, task_key_s, task_val, task_val_s, best_row, band_jobs_u, band_jobs, sw_rows, sw_rows_s,
       sw_keys_r, sw_order_r;
-  drg::DevBuf bj_key, bj_key_s, bj_val, bj_val_s, bj_size, bj_off, bj_max, ops_cnt, ops_coff, ops_compact, verdict;
+  drg::DevBuf bj_key, bj_key_s, bj_val, bj_val_s, bj_size, bj_off, bj_max, ops_cnt, ops_coff, ops_compact, verdict,
+      tr_count;
   drg::HostBuf h_stage;
   cudaEvent_t ev[16] = {};
   drg_run_stats last{};

@@ -135,7 +135,8 @@ struct SwTask {        // one warp: up to 32 bands sharing a query window
   uint32_t n_strips;   // 16-row strips to run
   uint32_t width;      // widest band of the task, W_max = d1 - d0 + 1
   uint32_t w_min;      // narrowest band of the task
-  uint64_t trace_off;  // trace mode: first uint2 of the task's trace
+  uint32_t transposed; // 1: rows are the subject, columns the query window (diagonals negated)
+  uint32_t pad;
 };
 // Trace-pass result of one band: where its nibbles are and its first maximum.
 struct TraceBand {
@@ -202,6 +203,7 @@ struct SwWalkArgs {
   uint8_t* rev;             // per band: n + m bytes at ops_off
   uint32_t* ops;
   ExactOut* out;
+  int exact_below;  // bands whose best is below this were written by the exact kernel
   int8_t scores625[628];
 };
 // Width classes of the packed kernel by the widest band of a warp (the shared

@@ -114,7 +114,29 @@ __host__ __device__ __forceinline__ int sw_class_of(uint32_t w) {
   return w <= (uint32_t)kSwC0 ? 0 : (w <= (uint32_t)kSwC1 ? 1 : (w <= (uint32_t)kSwC2 ? 2 : 3));
 }
 
-constexpr uint64_t kWideKey = 1ull << 63;
+// Score-pass sort key, radix-sorted over bits kKeyLo..63:
+//   63 wide band (one warp per band, after every packed-kernel band),
+//   61 transposed band, 24..60 group (target << 16 | window start, or the
+//   subject of a transposed band), 13..23 width.  Not computed here: ~0.
+// (Medium bands share warps with the narrow bands of their group: giving
+// them warps of their own left most of those warps' lanes idle.)
+constexpr uint64_t kWideKey = 1ull << 63, kTransposedKey = 1ull << 61;
+constexpr int kGroupShift = 24, kWidthShift = 13, kKeyLo = 13;
+
+// DP rows [rs, re] of a band with at least one in-matrix cell: rows are the
+// query window (d = i - j in [d0, d1]) or, transposed, the subject (the
+// diagonals become [-d1, -d0] and the columns are the query window).
+__host__ __device__ __forceinline__ void band_rows(const Band& b, int64_t m, bool transposed, int64_t* rs,
+                                                   int64_t* re) {
+  const int64_t n = b.n;
+  if (!transposed) {
+    *rs = b.d0 + 1 > 1 ? b.d0 + 1 : 1;
+    *re = m + b.d1 < n ? m + b.d1 : n;
+  } else {
+    *rs = -(int64_t)b.d1 + 1 > 1 ? -(int64_t)b.d1 + 1 : 1;
+    *re = n - b.d0 < m ? n - b.d0 : m;
+  }
+}
 
 // Number of sorted keys below `bound`.
 __global__ void k_count_below(const uint64_t* keys, uint64_t n, uint64_t bound, int64_t* out) {
@@ -127,30 +149,61 @@ __global__ void k_count_below(const uint64_t* keys, uint64_t n, uint64_t bound, 
   *out = (int64_t)lo;
 }
 
-// Classify bands for the packed kernel and build its two sort keys:
-//  key  (target, window start, width) << 16, or ~0 for the exact kernel;
-//  rows (first-row strip bucket, last row), the last row descending in odd
-//       buckets, so that bands next to each other in (key, rows) order cover
-//       nearly the same rows.
-__global__ void k_sw_keys(const Band* bands, uint64_t n, const uint64_t* s_offsets, int max_score,
-                          uint64_t* keys, uint32_t* rows, uint32_t* order) {
+// Which kernel a band goes to: the packed kernel (fast), its wide-band
+// variant (wide), and whether the band has fewer strips transposed.
+struct SwRoute {
+  bool fast, wide, tr;
+  int64_t rs, re, ts, te;
+};
+__device__ __forceinline__ SwRoute sw_route(const Band& b, const uint64_t* s_offsets, int max_score) {
+  SwRoute r;
+  const int64_t W = (int64_t)b.d1 - b.d0 + 1;
+  const int64_t m = (int64_t)(s_offsets[b.subject + 1] - s_offsets[b.subject]);
+  band_rows(b, m, false, &r.rs, &r.re);
+  band_rows(b, m, true, &r.ts, &r.te);
+  const int64_t mn = m < (int64_t)b.n ? m : (int64_t)b.n;
+  r.fast = W >= kSwMinWidth && W <= kSwMaxWidth && (int64_t)max_score * mn <= 32000 && r.rs <= r.re &&
+           b.target < (1u << 21) && b.q0 < 65536 && r.re < 65536;
+  r.wide = r.fast && W >= kSwBandMinWidth;
+  // narrow bands only: a medium band (W > 136) in a subject's warps would
+  // make its narrow lanes wait on its width
+  r.tr = r.fast && W <= kSwC0 && r.ts <= r.te && r.te < 65536 && (r.te - r.ts + 16) / 16 < (r.re - r.rs + 16) / 16;
+  return r;
+}
+// Bands per subject that would run with fewer strips transposed; each such
+// band draws a ticket (its arrival order, which varies from run to run: the
+// grouping of bands into warps does not change any score).
+__global__ void k_sw_tr_count(const Band* bands, uint64_t n, const uint64_t* s_offsets, int max_score,
+                              uint32_t* count, uint32_t* ticket) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
-  Band b = bands[i];
-  int64_t W = (int64_t)b.d1 - b.d0 + 1;
-  int64_t m = (int64_t)(s_offsets[b.subject + 1] - s_offsets[b.subject]);
-  int64_t rs = b.d0 + 1 > 1 ? b.d0 + 1 : 1;
-  int64_t re = m + b.d1 < (int64_t)b.n ? m + b.d1 : (int64_t)b.n;
-  int64_t mn = m < (int64_t)b.n ? m : (int64_t)b.n;
-  bool fast = W >= kSwMinWidth && W <= kSwMaxWidth && (int64_t)max_score * mn <= 32000 && rs <= re &&
-              b.target < (1u << 21) && b.q0 < 65536 && re < 65536;
-  // wide bands: after every narrow band, before the exact kernel's
-  const bool wide = fast && W >= kSwBandMinWidth;
-  keys[i] = !fast ? ~0ull
-                  : wide ? (kWideKey | ((uint64_t)W << 16))
-                         : ((uint64_t)b.target << 43) | ((uint64_t)b.q0 << 27) | ((uint64_t)W << 16);
-  const uint32_t bucket = fast ? (uint32_t)(rs >> 4) : 0xFFFFu;
-  const uint32_t last = fast ? (uint32_t)re : 0u;
+  const Band b = bands[i];
+  ticket[i] = sw_route(b, s_offsets, max_score).tr ? atomicAdd(count + b.subject, 1u) : 0xFFFFFFFFu;
+}
+
+// The two sort keys of the score pass: the key above, and rows (first-row
+// strip bucket, last row, the last row descending in odd buckets).  Bands are
+// sorted by rows, then stably by key, so that bands next to each other cover
+// nearly the same rows.
+// rows[i] holds band i's ticket from k_sw_tr_count on entry.
+__global__ void k_sw_keys(const Band* bands, uint64_t n, const uint64_t* s_offsets, int max_score,
+                          const uint32_t* tr_count, uint64_t* keys, uint32_t* rows, uint32_t* order) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Band b = bands[i];
+  const uint64_t W = (uint64_t)(b.d1 - b.d0 + 1);
+  const SwRoute r = sw_route(b, s_offsets, max_score);
+  // A subject's transposed bands form warps of their own: only whole warps
+  // of them are transposed, the rest stay with their query windows.
+  const bool tr = r.tr && tr_count && rows[i] < (tr_count[b.subject] & ~31u);
+  const int64_t rs = tr ? r.ts : r.rs, re = tr ? r.te : r.re;
+  const uint64_t group = tr ? (kTransposedKey | ((uint64_t)b.subject << kGroupShift))
+                            : ((((uint64_t)b.target << 16) | b.q0) << kGroupShift);
+  keys[i] = !r.fast ? ~0ull
+                    : r.wide ? (kWideKey | (W << kWidthShift))
+                             : (group | (W << kWidthShift));
+  const uint32_t bucket = r.fast ? (uint32_t)(rs >> 4) : 0xFFFFu;
+  const uint32_t last = r.fast ? (uint32_t)re : 0u;
   rows[i] = (bucket << 16) | ((bucket & 1) ? 0xFFFFu - last : last);
   order[i] = (uint32_t)i;
 }
@@ -165,7 +218,7 @@ __device__ __forceinline__ int64_t band_first_row(const Band& b) { return b.d0 +
 __global__ void k_sw_group_start(const uint64_t* keys, uint64_t n, uint32_t* gstart) {
   uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (s >= n) return;
-  gstart[s] = (s == 0 || (keys[s] >> 27) != (keys[s - 1] >> 27)) ? (uint32_t)s : 0u;
+  gstart[s] = (s == 0 || (keys[s] >> kGroupShift) != (keys[s - 1] >> kGroupShift)) ? (uint32_t)s : 0u;
 }
 __global__ void k_sw_task_flags(const uint32_t* gstart, uint64_t n, uint8_t* f) {
   uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
@@ -178,19 +231,20 @@ __global__ void k_sw_fill_tasks(const uint32_t* starts, uint64_t n_tasks, const 
   uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (t >= n_tasks) return;
   uint32_t s = starts[t];
-  uint64_t grp = keys[s] >> 27;
+  const uint64_t grp = keys[s] >> kGroupShift;
+  const bool transposed = (keys[s] & kTransposedKey) != 0;
   uint32_t cnt = 0;
   int64_t row_first = INT64_MAX, row_last = 0;
   uint32_t wmin = 0xFFFFFFFFu, wmax = 0;
   uint64_t lane_cells = 0;
-  while (cnt < 32 && s + cnt < n_fast && (keys[s + cnt] >> 27) == grp) {
+  while (cnt < 32 && s + cnt < n_fast && (keys[s + cnt] >> kGroupShift) == grp) {
     const uint64_t key = keys[s + cnt];
     const Band b = bands[order[s + cnt]];
     int64_t m = (int64_t)(s_offsets[b.subject + 1] - s_offsets[b.subject]);
-    int64_t re = m + b.d1 < (int64_t)b.n ? m + b.d1 : (int64_t)b.n;
-    if (row_limit && b.pad > 0 && (int64_t)b.pad < re) re = b.pad;  // traceback: rows up to the best
-    const int64_t rs = band_first_row(b);
-    const uint32_t w = (uint32_t)((key >> 16) & 0x7FF);
+    int64_t rs, re;
+    band_rows(b, m, transposed, &rs, &re);
+    if (row_limit && !transposed && b.pad > 0 && (int64_t)b.pad < re) re = b.pad;  // rows up to the best
+    const uint32_t w = (uint32_t)((key >> kWidthShift) & 0x7FF);
     if (re > row_last) row_last = re;
     if (rs < row_first) row_first = rs;
     if (w < wmin) wmin = w;
@@ -206,14 +260,18 @@ __global__ void k_sw_fill_tasks(const uint32_t* starts, uint64_t n_tasks, const 
   k.n_strips = (uint32_t)((row_last - row_first + 16) / 16);
   k.width = wmax;
   k.w_min = wmin;
-  k.trace_off = 0;
+  k.transposed = transposed ? 1u : 0u;
+  k.pad = 0;
   tasks[t] = k;
   const uint64_t steps = (uint64_t)k.n_strips * (wmax + 16ull);
   const int cls = sw_class_of(wmax);
   sort_key[t] = ((uint64_t)cls << 60) | ((~steps) & ((1ull << 60) - 1));  // class, then longest first
   sort_val[t] = (uint32_t)t;
   if (trace_size) trace_size[t] = steps * 32ull;
-  if (cells_gpu) atomicAdd(cells_gpu + 1, (unsigned long long)lane_cells);  // evaluated cells: counted by k_sw
+  if (cells_gpu) {
+    atomicAdd(cells_gpu + 1, (unsigned long long)lane_cells);  // evaluated cells: counted by k_sw
+    if (transposed) atomicAdd(cells_gpu + 3, (unsigned long long)cnt);
+  }
 }
 
 __global__ void k_gather_tasks(const SwTask* in, const uint32_t* idx, uint64_t n, SwTask* out) {
@@ -301,14 +359,17 @@ __global__ void k_set_band_trace_off(SwBandJob* jobs, const uint64_t* off, uint6
   if (k < n) jobs[k].trace_off = off[k];
 }
 
-// Bands the packed kernel did not take, or whose best is below 12.
+// Bands the packed kernel did not take, or whose best is not above the
+// matrix's largest score (exact_below = that + 1): only then can a cell the
+// packed kernels skip (the reference's clamped column past row m + d1) hold
+// the best.
 __global__ void k_exact_flags(const uint32_t* order, uint64_t n_fast, uint64_t n, const int32_t* score,
-                              const TraceBand* tband, uint8_t* f) {
+                              const TraceBand* tband, int exact_below, uint8_t* f) {
   uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (s >= n) return;
   uint32_t i = order[s];
   int v = tband ? tband[i].score : score[i];
-  f[s] = (s >= n_fast || v < 12) ? 1 : 0;
+  f[s] = (s >= n_fast || v < exact_below) ? 1 : 0;
 }
 
 __global__ void k_gather_positions(const uint32_t* pos, const uint32_t* order, uint64_t n, const Band* bands,
@@ -353,7 +414,7 @@ __global__ void k_gather_bands(const uint32_t* idx, uint64_t n, const Band* band
 // The banded DP of n_bands bands (any order).  The packed kernel takes the
 // bands whose width it supports (by width class) and whose best cannot
 // overflow 16 bits; the exact kernel takes the rest and every band whose
-// packed best is below 12.
+// packed best is not above the matrix's largest score.
 //  score mode (trace == false): scores[i] = best score (0 = None).
 //  trace mode: out[i] and the band's ops at h_ops_off[i] in ops (n + m slots
 //  per band), the same records the exact kernel produces.
@@ -433,8 +494,19 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
   uint32_t* rows_s = c->sw_rows_s.as<uint32_t>(n_bands);
   uint64_t* swk_r = c->sw_keys_r.as<uint64_t>(n_bands);
   uint32_t* swo_r = c->sw_order_r.as<uint32_t>(n_bands);
+  // the score pass may transpose bands; the traceback runs them as they are
+  uint32_t* tr_count = nullptr;
+  if (!trace) {
+    const uint64_t n_subjects = s.h_offsets->size() - 1;
+    tr_count = c->tr_count.as<uint32_t>(n_subjects);
+    DRG_CUDA(cudaMemsetAsync(tr_count, 0, n_subjects * sizeof(uint32_t), c->stream));
+    count_launch();
+    k_sw_tr_count<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(bc, n_bands, s.offsets, scr.max_score, tr_count,
+                                                                  rows);
+  }
   count_launch();
-  k_sw_keys<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(bc, n_bands, s.offsets, scr.max_score, swk, rows, swo);
+  k_sw_keys<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(bc, n_bands, s.offsets, scr.max_score, tr_count, swk,
+                                                           rows, swo);
   // rows first, then a stable sort by (target, window, width)
   cub_call(c, [&](void* t, size_t& b) {
     return cub::DeviceRadixSort::SortPairs(t, b, rows, rows_s, swo, swo_r, (int64_t)n_bands, 0, 32, c->stream);
@@ -442,7 +514,7 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
   count_launch();
   k_gather_keys<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(swk, swo_r, n_bands, swk_r);
   cub_call(c, [&](void* t, size_t& b) {
-    return cub::DeviceRadixSort::SortPairs(t, b, swk_r, swks, swo_r, swos, (int64_t)n_bands, 16, 64, c->stream);
+    return cub::DeviceRadixSort::SortPairs(t, b, swk_r, swks, swo_r, swos, (int64_t)n_bands, kKeyLo, 64, c->stream);
   });
   const uint64_t n_fast = (uint64_t)count_valid(c, swks, n_bands, d_count);
   TraceBand* tb = nullptr;
@@ -476,6 +548,7 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
     wa.rev = c->rev.as<uint8_t>((*h_ops_off)[n_bands] + 16);
     wa.ops = ops;
     wa.out = out;
+    wa.exact_below = scr.max_score + 1;
     std::memcpy(wa.scores625, scr.scores, 625);
     launch_sw_walk(wa, c->stream);
     DRG_CUDA(cudaEventSynchronize(e1));
@@ -609,7 +682,8 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
   }
   // the exact kernel for the bands the packed kernel did not settle
   count_launch();
-  k_exact_flags<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(swos, n_fast, n_bands, scores, tb, flags);
+  k_exact_flags<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(swos, n_fast, n_bands, scores, tb,
+                                                                scr.max_score + 1, flags);
   uint32_t* ex_pos = c->sel_idx.as<uint32_t>(n_bands + 1);
   const uint64_t n_ex = select_indices(c, flags, n_bands, ex_pos, d_count);
   st.exact_bands += n_ex;
@@ -677,6 +751,7 @@ struct Search {
   // device scratch for counters
   int64_t* d_count = nullptr;
   // [0] xdrops [1] cells_ref [2] computed [3] cells_gpu [4] lane cells [5] issued cells
+  // [6] transposed bands
   unsigned long long* d_counters = nullptr;
 
   void configure(const drg_search_config* cfg) {
@@ -1166,9 +1241,9 @@ void Search::run(drg_result* out) {
   Timer total(c);
   total.start();
   std::memset(out, 0, sizeof(*out));
-  d_count = c->counters.as<int64_t>(8);
+  d_count = c->counters.as<int64_t>(9);
   d_counters = reinterpret_cast<unsigned long long*>(d_count + 2);
-  DRG_CUDA(cudaMemsetAsync(d_count, 0, 8 * sizeof(int64_t), c->stream));
+  DRG_CUDA(cudaMemsetAsync(d_count, 0, 9 * sizeof(int64_t), c->stream));
   if (q->n == 0 || db->n == 0) {
     out->n_targets = q->n;
     out->target_offsets = (uint64_t*)std::calloc(q->n + 1, sizeof(uint64_t));
@@ -1188,7 +1263,7 @@ void Search::run(drg_result* out) {
     for (auto [c0, c1] : split_chunks(db->n, index_chunks)) chunk(cid++, c0, c1, n_runs);
   }
   finish(out);
-  unsigned long long cnt[6];
+  unsigned long long cnt[7];
   DRG_CUDA(cudaMemcpyAsync(cnt, d_counters, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
   DRG_CUDA(cudaStreamSynchronize(c->stream));
   st.xdrops = cnt[0];
@@ -1197,6 +1272,7 @@ void Search::run(drg_result* out) {
   st.dp_cells_gpu = cnt[3];
   st.dp_cells_lane = cnt[4];
   st.dp_cells_issued = cnt[5];
+  st.sw_transposed_bands = cnt[6];
   st.ms_total = total.stop();
   st.kernel_launches = kernel_launch_count() - launches0;
   out->stats = st;

@@ -6,7 +6,7 @@
 // row-major maximum, trace bits and the traceback walk are the reference's.
 // It runs on the HSPs that survive the E-value gate and the per-query cut,
 // and on the rare bands the packed score kernel does not take (width < 17,
-// possible 16-bit overflow, best score below 12).
+// possible 16-bit overflow, best score not above the matrix's largest).
 #include "kernels.h"
 
 namespace drg {

@@ -24,8 +24,11 @@
 // below 2^15 (bands that could exceed it are not given to this kernel).
 // Cells with j < 0, j > m or rows past the query read a sentinel residue
 // scoring -64; they can neither raise the maximum above the true band maximum
-// (when that is >= 12; smaller results are recomputed exactly) nor feed an
-// in-band cell.  Cells left or right of the band in the first/last 16 steps of
+// nor feed an in-band cell.  Rows past m + d1 are not computed: the reference
+// keeps one cell per such row, clamped to column m, whose H is at most
+// max(largest matrix score, band best - open), so a packed best above the
+// matrix's largest score is the reference's; smaller results are recomputed
+// exactly.  Cells left or right of the band in the first/last 16 steps of
 // a strip are masked: their H does not count and they pass -inf-like E/F.
 //
 // Trace mode also writes, per cell, the reference's trace nibble
@@ -170,11 +173,19 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS >= 2 ? 3 : 1) k_sw(SwScoreAr
   const uint32_t bidx = a.order[task.first + (active ? lane : 0)];
   const Band band = a.bands[bidx];
   const int Wl = band.d1 - band.d0 + 1;  // this lane's width
-  const uint8_t* q = a.q_letters + a.q_offsets[band.target] + band.q0;
-  const int n = (int)band.n;
+  // Rows are the query window and columns the subject, or (a transposed
+  // task, whose lanes share the subject) rows the subject and columns the
+  // window with the diagonals negated: the same cells, so the same best.
+  const bool tr = task.transposed != 0;
+  const uint8_t* qw = a.q_letters + a.q_offsets[band.target] + band.q0;
+  const uint8_t* sj = a.s_letters + a.s_offsets[band.subject];
+  const int m_s = (int)(a.s_offsets[band.subject + 1] - a.s_offsets[band.subject]);
+  const uint8_t* q = tr ? sj : qw;  // row letters
+  const int n = tr ? m_s : (int)band.n;
+  const int d1 = tr ? -band.d0 : band.d1;
   Lane L;
-  L.s = a.s_letters + a.s_offsets[band.subject];
-  L.m = (int)(a.s_offsets[band.subject + 1] - a.s_offsets[band.subject]);
+  L.s = tr ? qw : sj;  // column letters
+  L.m = tr ? (int)band.n : m_s;
   const uint32_t noc2 = (uint32_t)(uint16_t)(-(a.gap_open + a.gap_extend)) * 0x10001u;
   const uint32_t nge2 = (uint32_t)(uint16_t)(-a.gap_extend) * 0x10001u;
   // the row above the first strip is row 0 of the reference: H = 0, and its
@@ -191,18 +202,22 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS >= 2 ? 3 : 1) k_sw(SwScoreAr
   uint64_t steps_done = 0;  // column steps run (all strips)
   for (uint32_t k = 0; k < task.n_strips; ++k) {
     const int i0 = (int)task.row_first + (int)(k * kRows);
-    // strip profile: prof[res * stride + r] = S(q[i0 + r - 1], res)
+    // strip profile: prof[res * stride + r] = S(query letter, subject letter)
+    // of row i0 + r against column residue res
     __syncwarp();
     for (int e = lane; e < 26 * kRows; e += 32) {
       int res = e >> 4, r = e & 15;
       int i = i0 + r;
       int v;
       if (res == 25 || i > n) v = kSentinelScore;
-      else v = mat[(int)min((uint32_t)q[i - 1], 24u) * 25 + res];
+      else {
+        const int row = (int)min((uint32_t)q[i - 1], 24u);
+        v = tr ? mat[res * 25 + row] : mat[row * 25 + res];
+      }
       prof[res * kProfStride + r] = (uint8_t)(int8_t)v;
     }
     __syncwarp();
-    L.jbase = i0 - band.d1;
+    L.jbase = i0 - d1;
 #pragma unroll
     for (int p = 0; p < kPairs; ++p) {
       R.H[p] = 0;
@@ -309,6 +324,9 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS >= 2 ? 3 : 1) k_sw(SwScoreAr
   }
   if (!active) return;
   a.score[bidx] = best;
+  // transposed: the best cell's subject row i' <= best_i sits on query row
+  // i' + d (d in [d0, d1]), so best_i + d1 bounds the reference's best row
+  if (tr && best_i > 0) best_i = min((int)band.n, best_i + band.d1);
   if (a.best_row) a.best_row[bidx] = best_i;
 }
 
@@ -328,13 +346,13 @@ __global__ void k_sw_walk(SwWalkArgs a) {
   R.identities = R.positives = R.mismatches = R.gap_openings = R.gaps = R.length = 0;
   R.n_ops = 0;
   R.cells = 0;
-  if (tb.score < 12) return;  // not traced here: the exact kernel writes this band
+  if (tb.score < a.exact_below) return;  // not traced here: the exact kernel writes this band
   const uint8_t* q = a.q_letters + a.q_offsets[b.target] + b.q0;
   const uint8_t* s = a.s_letters + a.s_offsets[b.subject];
   const int64_t m = (int64_t)(a.s_offsets[b.subject + 1] - a.s_offsets[b.subject]);
   const int64_t d0 = b.d0, d1 = b.d1, W = tb.width, rf = tb.row_first;
   if (tb.best_i < 1 || tb.best_i > (int64_t)b.n || tb.best_j < 1 || tb.best_j > m) {
-    R.score = -1;  // cannot happen for a best >= 12; reported to the host as an internal error
+    R.score = -1;  // cannot happen for a best this high; reported to the host as an internal error
     a.out[t] = R;
     return;
   }

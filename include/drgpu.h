@@ -109,6 +109,7 @@ typedef struct {
   double ms_sw_wide;               /* device time of their launch (concurrent with the classes) */
   uint64_t dp_cells_issued;        /* score kernel: warps x column steps x 16 x 32, idle lanes included */
   uint64_t index_hits;             /* index chunks whose sorted reference seeds came from the db's cache */
+  uint64_t sw_transposed_bands;    /* score kernel: bands run with the subject as rows */
 } drg_run_stats;
 
 /* search::run result: per-target HSP lists, target_offsets[n_targets+1]. */

@@ -209,6 +209,51 @@ def test_packed_scores_on_search_like_bands(ctx, orc):
         assert int(g) == (e[0] if e else 0), j
 
 
+def test_packed_scores_transposed_short_subjects(ctx, orc):
+    """Bands on short subjects from long queries run with the subject as rows
+    (fewer strips); a subject needs a warp's worth of such bands.  Widths mix
+    narrow and medium (137..272) bands in one warp."""
+    r = rng(123)
+    queries = [rand_seq(r, int(L)) for L in r.integers(400, 1200, size=9)]
+    subjects, jobs = [], []
+    for k in range(3):
+        m = int(r.integers(40, 140))
+        base = queries[k][:m].copy() if k == 0 else rand_seq(r, m)
+        subjects.append(synth.mutate(r, base, 0.3) if k == 0 else base)
+        for t in range(60):
+            qi = t % len(queries)
+            n = len(queries[qi])
+            half = int(r.choice([12, 16, 30, 40, 64, 80, 100]))
+            d = int(r.integers(-m + 1, n))
+            jobs.append((qi, k, d - half, d + half))
+    # one subject with too few bands to be worth transposing
+    subjects.append(rand_seq(r, 50))
+    jobs += [(q, 3, -20, 20) for q in range(5)]
+    scores, st = ctx.extend_span_scores(queries, subjects, jobs)
+    exp = oracle_spans(orc, queries, subjects, jobs)
+    for j, g, e in zip(jobs, scores, exp):
+        assert int(g) == (e[0] if e else 0), j
+    assert st["sw_transposed_bands"] >= 64
+
+
+@pytest.mark.parametrize("matrix", ["BLOSUM45", "BLOSUM50", "BLOSUM80", "BLOSUM90", "PAM30", "PAM70", "PAM250"])
+def test_packed_scores_other_matrices(ctx, orc, matrix):
+    """The clamped column past row m + d1 (gapped.rs:86-92) can hold up to the
+    matrix's largest score; packed bests up to that are recomputed exactly."""
+    r = rng(7 + len(matrix))
+    queries, subjects, jobs = span_cases(31 + len(matrix), 150, max_len=500)
+    # C/C then W/W in the clamped column: in-band best 9..13, clamped cells up to 15/17
+    queries.append(orc.encode("C" + "A" * 24 + "W" * 10 + "A" * 100))
+    subjects.append(orc.encode("C" * 19 + "W"))
+    jobs.append((len(queries) - 1, len(subjects) - 1, -5, 5))
+    scores, _ = ctx.extend_span_scores(queries, subjects, jobs, matrix=matrix)
+    exp = [orc.extend_span(queries[j[0]], subjects[j[1]], j[2], j[3], matrix=matrix)[0] for j in jobs]
+    for j, g, e in zip(jobs, scores, exp):
+        assert int(g) == (e[0] if e else 0), (matrix, j)
+    got = ctx.extend_span(queries[-1:], subjects[-1:], [(0, 0, -5, 5)], matrix=matrix)
+    assert got == [exp[-1]]
+
+
 def test_extend_span_edge_cases(ctx, orc):
     W = np.full(3100, 17, np.uint8)  # W/W scores 11: best 34100 does not fit 16 bits
     cases = [
