@@ -14,7 +14,7 @@ void upload_seed_params(const ShapeTable& shapes, const SeedParams& p, int slot,
 void launch_letter_owner(const uint64_t* offsets, uint64_t n_seqs, uint64_t letter_lo, uint64_t letter_hi,
                          uint32_t* out, cudaStream_t st);
 // Enumerate seeds of letters [letter_lo, letter_hi) for shapes [0, n_shapes):
-// keys[(g - letter_lo) * n_shapes + s] = request << request_shift |
+// keys[s * (letter_hi - letter_lo) + g - letter_lo] = request << request_shift |
 // s << shape_shift | key (shifts from the search's SeedParams), or ~0 when no
 // seed.  request (per sequence, optional) tags query seeds with the request
 // their target belongs to, so that the join cap counts the query occurrences
