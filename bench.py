@@ -57,6 +57,8 @@ def parse():
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     p.add_argument("--no-serve", action="store_true", help="skip the serving stream (profiling runs)")
+    p.add_argument("--no-blastx", action="store_true", help="skip the blastx leg (profiling runs)")
+    p.add_argument("--blastx-reads", type=int, default=20000, help="reads in the blastx leg")
     p.add_argument("--serve-requests", type=int, default=100, help="requests in the serving stream")
     p.add_argument("--queries", type=int, default=None,
                    help="search only the first N queries (a smaller case for ncu captures; not a bench line)")
@@ -215,6 +217,63 @@ def serve_stream(w, device, n_requests):
     return out
 
 
+def blastx_leg(ctx, steps, warmup, n_reads, cpu_sample, with_cpu):
+    """blastx (--fast) end to end through the C ABI: reads from host memory,
+    six-frame translation and ORF masking on the device
+    (drg_batch_create_blastx), search, merge_frames, results on the host.
+    Reads: 150-300 nt, 30 % reverse-translated DB fragments, the rest random."""
+    import numpy as np
+    import drgpu
+    from drgpu import synth
+    w = synth.read_workload(n_reads=n_reads, n_db=20000, seed_offset=0)
+    dl, do = drgpu.concat(w.db)
+    db = drgpu.ResidentDb(ctx, dl, do)
+    cfg = drgpu.make_config(sensitivity="fast")
+    nt_bytes = sum(len(r) for r in w.reads)
+
+    def one():
+        t0 = time.perf_counter()
+        b = drgpu.blastx_batch(ctx, w.reads)
+        try:
+            _, st, n_hsps = drgpu.search_resident(ctx, db, b, cfg, want_lists=False, merge_queries=len(w.reads))
+        finally:
+            b.close()
+        return time.perf_counter() - t0, st, n_hsps, len(b.query)
+
+    for _ in range(warmup):
+        one()
+    total, frames, hsps, search_ms = 0.0, 0, 0, 0.0
+    for _ in range(steps):
+        dt, st, hsps, frames = one()
+        total += dt
+        search_ms += st["ms_total"]
+    out = {"workload": f"{n_reads} reads (150-300 nt, 30 % reverse-translated DB fragments) x 20,000-sequence "
+                       f"synthetic DB, blastx --fast, BLOSUM62 11/1, e 1e-3, k 25", "reads_per_s": n_reads * steps / total,
+           "ms_per_step": 1000.0 * total / steps, "search_ms_per_step": search_ms / steps, "frames": frames,
+           "hsps": hsps, "h2d_nt_bytes_per_step": nt_bytes,
+           "what": "wall time per step: reads uploaded, translated on the GPU, searched, merged per read"}
+    if with_cpu:
+        import pyoracle
+        sample = w.reads[:cpu_sample]
+        t0 = time.perf_counter()
+        frames_o, q_o, f_o = [], [], []
+        for qi, r in enumerate(sample):
+            m = pyoracle.min_orf_len(len(r))
+            for f, fr in enumerate(pyoracle.six_frames(r)):
+                fr = pyoracle.mask_short_orfs(fr, m)
+                if (fr < 23).any():
+                    frames_o.append(fr)
+                    q_o.append(qi)
+                    f_o.append(f)
+        pyoracle.search(w.db, frames_o, sensitivity="fast", t_query=np.array(q_o), t_frame=np.array(f_o),
+                        merge=True, n_queries=len(sample), threads=os.cpu_count() or 1)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": len(sample) / dt, "unit": "reads/s", "cores": os.cpu_count() or 1,
+                               "kind": "port", "sample": f"first {len(sample)} reads as their own batch, {dt:.1f} s"}
+    db.close()
+    return out
+
+
 def cpu_sample_run(w, n_sample, threads):
     import pyoracle
     qs = w.queries[:n_sample]
@@ -343,6 +402,12 @@ def main():
     if not args.no_serve:
         serving = serve_stream(w, local, args.serve_requests)
 
+    # ---- blastx (config-4 shaped, scaled) ------------------------------------
+    blastx = None
+    if not args.no_blastx:
+        blastx = blastx_leg(ctx, args.steps, max(1, args.warmup), args.blastx_reads, 2000,
+                            rank == 0 and world == 1 and not args.no_cpu)
+
     # ---- CPU baseline and sample parity (rank 0, N = 1) ---------------------
     cpu = None
     parity = None
@@ -391,6 +456,7 @@ def main():
             "e2e": e2e,
             "serving": serving,
             "index_resident": index_resident,
+            "blastx": blastx,
             "gpu_launches": int(launches),
             "cpu_baseline": cpu,
             "parity_sample": parity,

@@ -550,6 +550,56 @@ int drg_batch_create_requests(drg_ctx* c, const uint8_t* letters, const uint64_t
   API_END(c)
 }
 
+int drg_batch_create_blastx(drg_ctx* c, const uint8_t* nt, const uint64_t* nt_offsets, uint64_t n_reads,
+                            int64_t min_orf, drg_batch** out) {
+  if (!c || !nt_offsets || !out || (!nt && nt_offsets[n_reads] > 0)) return DRG_ERR_INVALID;
+  API_BEGIN(c)
+  *out = make_batch_translated(c, nt, nt_offsets, n_reads, min_orf);
+  API_END(c)
+}
+
+int drg_translate_reads(drg_ctx* c, const uint8_t* nt, const uint64_t* nt_offsets, uint64_t n_reads,
+                        int64_t min_orf, uint8_t** letters, uint64_t** offsets, uint32_t** query, uint8_t** frame,
+                        uint64_t* n_targets) {
+  if (!c || !nt_offsets || !letters || !offsets || !query || !frame || !n_targets ||
+      (!nt && nt_offsets[n_reads] > 0))
+    return DRG_ERR_INVALID;
+  API_BEGIN(c)
+  HostFrames h;
+  drg_batch* b = make_batch_translated(c, nt, nt_offsets, n_reads, min_orf, &h);
+  free_batch(b);
+  const uint64_t n = h.query.size();
+  *letters = (uint8_t*)std::malloc(h.letters.size() + 1);
+  *offsets = (uint64_t*)std::malloc((n + 1) * sizeof(uint64_t));
+  *query = (uint32_t*)std::malloc((n + 1) * sizeof(uint32_t));
+  *frame = (uint8_t*)std::malloc(n + 1);
+  if (!*letters || !*offsets || !*query || !*frame) {
+    std::free(*letters);
+    std::free(*offsets);
+    std::free(*query);
+    std::free(*frame);
+    *letters = nullptr;
+    *offsets = nullptr;
+    *query = nullptr;
+    *frame = nullptr;
+    throw Error(DRG_ERR_OOM, "host allocation failed");
+  }
+  if (!h.letters.empty()) std::memcpy(*letters, h.letters.data(), h.letters.size());
+  std::memcpy(*offsets, h.offsets.data(), (n + 1) * sizeof(uint64_t));
+  if (n) std::memcpy(*query, h.query.data(), n * sizeof(uint32_t));
+  if (n) std::memcpy(*frame, h.frame.data(), n);
+  *n_targets = n;
+  API_END(c)
+}
+
+int drg_batch_targets(const drg_batch* b, uint64_t* n_targets, uint32_t* query, uint8_t* frame) {
+  if (!b || !n_targets) return DRG_ERR_INVALID;
+  *n_targets = b->n;
+  if (query && b->n) std::memcpy(query, b->query.data(), b->n * sizeof(uint32_t));
+  if (frame && b->n) std::memcpy(frame, b->frame.data(), b->n);
+  return DRG_OK;
+}
+
 void drg_batch_destroy(drg_batch* b) {
   if (b) cudaSetDevice(b->ctx->device);
   free_batch(b);

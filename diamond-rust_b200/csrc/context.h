@@ -33,6 +33,9 @@ struct drg_ctx {
       sw_keys_r, sw_order_r;
   drg::DevBuf bj_key, bj_key_s, bj_val, bj_val_s, bj_size, bj_off, bj_max, ops_cnt, ops_coff, ops_compact, verdict,
       tr_count;
+  // blastx front end
+  drg::DevBuf x_nt, x_nt_off, x_len, x_scratch_off, x_scratch, x_keep, x_kept_len, x_kept_index, x_kept_off,
+      x_query, x_frame;
   drg::HostBuf h_stage;
   cudaEvent_t ev[16] = {};
   drg_run_stats last{};
@@ -82,6 +85,16 @@ void search(drg_ctx* ctx, const drg_db* db, const drg_batch* b, const drg_search
 drg_db* make_db(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offsets, uint64_t n);
 drg_batch* make_batch(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offsets, const uint32_t* query,
                       const uint8_t* frame, uint64_t n, const uint32_t* request = nullptr);
+// blastx targets translated on the device from host reads; with `host`, the
+// frames are also returned (letters, offsets, query index, frame).
+struct HostFrames {
+  std::vector<uint8_t> letters;
+  std::vector<uint64_t> offsets;
+  std::vector<uint32_t> query;
+  std::vector<uint8_t> frame;
+};
+drg_batch* make_batch_translated(drg_ctx* ctx, const uint8_t* nt, const uint64_t* nt_offsets, uint64_t n_reads,
+                                 int64_t min_orf, HostFrames* host = nullptr);
 void free_db(drg_db* db);
 void free_batch(drg_batch* b);
 }  // namespace drg

@@ -277,27 +277,46 @@ int cmd_blast(const std::vector<std::string>& a, bool translated) {  // workflow
       throw std::runtime_error("unsupported matrix or gap costs: " + o.matrix + " " + std::to_string(o.gap_open) +
                                "/" + std::to_string(o.gap_extend));
   }
-  // targets: translated frames (blastx) or encoded residues (blastp)
+  drg_ctx* ctx = nullptr;
+  check(nullptr, drg_ctx_create(0, &ctx));
+  struct CtxGuard {
+    drg_ctx*& c;
+    ~CtxGuard() {
+      if (c) drg_ctx_destroy(c);
+    }
+  } ctx_guard{ctx};
+  const uint8_t empty = 0;
+  // targets: translated frames (blastx, on the GPU) or encoded residues (blastp)
   std::vector<std::vector<uint8_t>> t_letters;
   std::vector<uint32_t> t_query;
   std::vector<uint8_t> t_frame;
   std::vector<std::array<long long, 6>> target_of(records.size());
-  for (size_t qi = 0; qi < records.size(); ++qi) {
-    target_of[qi].fill(-1);
-    if (translated) {
-      const size_t min_orf = min_orf_len(records[qi].raw.size(), o.min_orf);
-      auto frames = six_frames(records[qi].raw);
-      for (int f = 0; f < 6; ++f) {
-        mask_short_orfs(frames[f], min_orf);
-        size_t real = 0;
-        for (uint8_t l : frames[f]) real += l < kXLetter;
-        if (real == 0) continue;
-        target_of[qi][f] = (long long)t_letters.size();
-        t_letters.push_back(std::move(frames[f]));
-        t_query.push_back((uint32_t)qi);
-        t_frame.push_back((uint8_t)f);
-      }
-    } else {
+  for (auto& t : target_of) t.fill(-1);
+  if (translated) {  // workflow.rs:112-127
+    std::vector<uint8_t> nt;
+    std::vector<uint64_t> no(1, 0);
+    for (const auto& r : records) {
+      nt.insert(nt.end(), r.raw.begin(), r.raw.end());
+      no.push_back(nt.size());
+    }
+    uint8_t *L = nullptr, *F = nullptr;
+    uint64_t* O = nullptr;
+    uint32_t* Q = nullptr;
+    uint64_t n = 0;
+    check(ctx, drg_translate_reads(ctx, nt.empty() ? &empty : nt.data(), no.data(), records.size(), o.min_orf, &L,
+                                   &O, &Q, &F, &n));
+    for (uint64_t t = 0; t < n; ++t) {
+      target_of[Q[t]][F[t]] = (long long)t;
+      t_letters.emplace_back(L + O[t], L + O[t + 1]);
+      t_query.push_back(Q[t]);
+      t_frame.push_back(F[t]);
+    }
+    drg_free(L);
+    drg_free(O);
+    drg_free(Q);
+    drg_free(F);
+  } else {
+    for (size_t qi = 0; qi < records.size(); ++qi) {
       auto l = encode_residues(records[qi].raw);
       if (l.empty()) continue;
       target_of[qi][0] = (long long)t_letters.size();
@@ -326,19 +345,13 @@ int cmd_blast(const std::vector<std::string>& a, bool translated) {  // workflow
   cfg.has_seed_cut = o.has_seed_cut;
   cfg.seed_cut = o.seed_cut;
   cfg.threads = (uint32_t)o.threads;
-  drg_ctx* ctx = nullptr;
-  check(nullptr, drg_ctx_create(0, &ctx));
   drg_result res{};
   const uint8_t* dl = db.data.data() + db.letters_start;
-  const uint8_t empty = 0;
   const int rc = drg_search_run(ctx, db.letters ? dl : &empty, dbo.data(), db.n, tl.empty() ? &empty : tl.data(),
                                 to.data(), t_query.data(), t_frame.data(), t_letters.size(), &cfg, &res);
-  if (rc != DRG_OK) {
-    std::string msg = drg_last_error(ctx);
-    drg_ctx_destroy(ctx);
-    throw std::runtime_error("GPU search failed: " + msg);
-  }
+  if (rc != DRG_OK) throw std::runtime_error("GPU search failed: " + std::string(drg_last_error(ctx)));
   drg_ctx_destroy(ctx);
+  ctx = nullptr;
   if (drg_merge_frames(&res, records.size(), t_query.data(), o.max_hsps, o.max_target_seqs) != DRG_OK) {
     drg_result_free(&res);
     throw std::runtime_error("merge_frames failed");

@@ -8,78 +8,6 @@
 namespace drg {
 namespace host {
 
-// ---- translate.rs ----------------------------------------------------------------
-namespace {
-// The standard genetic code, codons indexed by bases in T, C, A, G order.
-const char kCodon[65] = "FFLLSSSSYY**CC*WLLLLPPPPHHQQRRRRIIIMTTTTNNKKSSRRVVVVAAAADDEEGGGG";
-
-int base_index(char b) {
-  switch (b) {
-    case 'T': case 't': case 'U': case 'u': return 0;
-    case 'C': case 'c': return 1;
-    case 'A': case 'a': return 2;
-    case 'G': case 'g': return 3;
-    default: return 4;
-  }
-}
-char complement_base(char b) {
-  switch (b) {
-    case 'A': return 'T';
-    case 'T': return 'A';
-    case 'C': return 'G';
-    case 'G': return 'C';
-    case 'U': return 'A';
-    case 'R': return 'Y';
-    case 'Y': return 'R';
-    case 'K': return 'M';
-    case 'M': return 'K';
-    case 'B': return 'V';
-    case 'V': return 'B';
-    case 'D': return 'H';
-    case 'H': return 'D';
-    default: return b;  // S, W, N and anything else map to themselves
-  }
-}
-}  // namespace
-
-std::vector<uint8_t> translate_frame(const std::string& nt, size_t offset) {
-  std::vector<uint8_t> out;
-  if (nt.size() > offset) out.reserve((nt.size() - offset) / 3);
-  for (size_t i = offset; i + 3 <= nt.size(); i += 3) {
-    const int a = base_index(nt[i]), b = base_index(nt[i + 1]), c = base_index(nt[i + 2]);
-    out.push_back(a > 3 || b > 3 || c > 3 ? kXLetter : encode_letter((uint8_t)kCodon[a * 16 + b * 4 + c]));
-  }
-  return out;
-}
-
-std::vector<std::vector<uint8_t>> six_frames(const std::string& nt) {
-  std::string rc(nt.size(), ' ');
-  for (size_t i = 0; i < nt.size(); ++i) rc[i] = complement_base(nt[nt.size() - 1 - i]);
-  std::vector<std::vector<uint8_t>> f;
-  f.reserve(6);
-  for (size_t o = 0; o < 3; ++o) f.push_back(translate_frame(nt, o));
-  for (size_t o = 0; o < 3; ++o) f.push_back(translate_frame(rc, o));
-  return f;
-}
-
-void mask_short_orfs(std::vector<uint8_t>& frame, size_t min_len) {
-  if (min_len <= 1) return;
-  size_t begin = 0;
-  for (size_t i = 0; i < frame.size(); ++i) {
-    if (frame[i] != kStopLetter) continue;
-    if (i - begin < min_len)
-      for (size_t k = begin; k < i; ++k) frame[k] = kXLetter;
-    begin = i + 1;
-  }
-  if (frame.size() - begin < min_len)
-    for (size_t k = begin; k < frame.size(); ++k) frame[k] = kXLetter;
-}
-
-size_t min_orf_len(size_t dna_len, long long user) {
-  if (user >= 0) return (size_t)user;
-  return dna_len < 30 ? 1 : (dna_len < 100 ? 20 : 40);
-}
-
 // ---- output.rs ----------------------------------------------------------------------
 namespace {
 const char* kFieldNames[] = {"qseqid", "qlen", "sseqid", "slen", "qstart", "qend", "sstart", "send", "qseq",

@@ -1,5 +1,6 @@
-// blastx front end (translate.rs) and BLAST tabular output (output.rs,
-// hsp.rs:84-241) of the drop-in command line.
+// BLAST tabular output (output.rs, hsp.rs:84-241) of the drop-in command
+// line.  (The blastx front end, translate.rs, runs on the device:
+// drg_translate_reads.)
 #pragma once
 #include <cstdint>
 #include <string>
@@ -10,12 +11,6 @@
 
 namespace drg {
 namespace host {
-
-// ---- translate.rs:9-137 ------------------------------------------------------
-std::vector<uint8_t> translate_frame(const std::string& nt, size_t offset);
-std::vector<std::vector<uint8_t>> six_frames(const std::string& nt);
-void mask_short_orfs(std::vector<uint8_t>& frame, size_t min_len);
-size_t min_orf_len(size_t dna_len, long long user);  // user < 0: the default
 
 // ---- output.rs -----------------------------------------------------------------
 enum Field : int {

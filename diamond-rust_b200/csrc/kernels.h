@@ -67,6 +67,32 @@ struct JoinExpandArgs {
 };
 void launch_join_expand(const JoinExpandArgs& a, cudaStream_t st);
 
+// ---- blastx front end (translate.cu) ----------------------------------------
+// Per (read, frame) entry i = 6 * read + frame; arrays of 6 * n_reads + 1
+// entries, the last one the scans' total.
+struct TranslateArgs {
+  const uint8_t* nt;            // reads, upper-cased bytes back to back
+  const uint64_t* nt_off;       // n_reads + 1
+  uint64_t n_reads;
+  int64_t min_orf;              // >= 0: for every read; < 0: translate::min_orf_len of each read
+  uint8_t* scratch;             // frames before compaction
+  const uint64_t* scratch_off;  // exclusive scan of the frame lengths
+  uint32_t* keep;               // 1: the frame has a letter below X after masking
+  uint64_t* kept_len;           // its length when kept, else 0
+  const uint32_t* kept_index;   // exclusive scan of keep: the target index
+  const uint64_t* kept_off;     // exclusive scan of kept_len: the target's first letter
+  uint8_t* out;                 // kept frames back to back
+  uint64_t* out_off;            // n_targets + 1
+  uint32_t* out_query;          // read of each target
+  uint8_t* out_frame;           // frame 0-5 of each target
+};
+// len[i] = codons of frame i ((L - offset) / 3), len[6 * n_reads] = 0.
+void launch_frame_lengths(const uint64_t* nt_off, uint64_t n_reads, uint64_t* len, cudaStream_t st);
+// Translation, ORF masking, keep flags (fills scratch, keep, kept_len).
+void launch_translate_frames(const TranslateArgs& a, cudaStream_t st);
+// Kept frames into out / out_off / out_query / out_frame.
+void launch_compact_frames(const TranslateArgs& a, cudaStream_t st);
+
 // ---- ungapped (ungapped_kernels.cu) -----------------------------------------
 // Scores (25x25, int8) in constant memory for X-drop and the band stage.
 void upload_score_matrix(const int8_t* scores625, int slot, cudaStream_t st);

@@ -1373,6 +1373,80 @@ drg_batch* make_batch(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offs
   return b;
 }
 
+drg_batch* make_batch_translated(drg_ctx* ctx, const uint8_t* nt, const uint64_t* nt_off, uint64_t n_reads,
+                                 int64_t min_orf, HostFrames* host) {
+  const uint64_t n_nt = nt_off[n_reads];
+  for (uint64_t i = 0; i < n_reads; ++i)
+    if (nt_off[i + 1] < nt_off[i]) throw Error(DRG_ERR_INVALID, "read offsets must be non-decreasing");
+  if (6 * n_reads > 0xFFFFFFF0ull) throw Error(DRG_ERR_INVALID, "too many reads in one batch");
+  drg_ctx* c = ctx;
+  const uint64_t n6 = 6 * n_reads;
+  uint8_t* d_nt = c->x_nt.as<uint8_t>(n_nt + 16);
+  uint64_t* d_off = c->x_nt_off.as<uint64_t>(n_reads + 1);
+  if (n_nt) DRG_CUDA(cudaMemcpyAsync(d_nt, nt, n_nt, cudaMemcpyHostToDevice, c->stream));
+  DRG_CUDA(cudaMemcpyAsync(d_off, nt_off, (n_reads + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
+  uint64_t* len = c->x_len.as<uint64_t>(n6 + 1);
+  uint64_t* soff = c->x_scratch_off.as<uint64_t>(n6 + 1);
+  launch_frame_lengths(d_off, n_reads, len, c->stream);
+  cub_call(c, [&](void* t, size_t& b) {
+    return cub::DeviceScan::ExclusiveSum(t, b, len, soff, (int64_t)n6 + 1, c->stream);
+  });
+  const uint64_t n_scratch = fetch(c, soff + n6);
+  TranslateArgs a{};
+  a.nt = d_nt;
+  a.nt_off = d_off;
+  a.n_reads = n_reads;
+  a.min_orf = min_orf;
+  a.scratch = c->x_scratch.as<uint8_t>(n_scratch + 16);
+  a.scratch_off = soff;
+  a.keep = c->x_keep.as<uint32_t>(n6 + 1);
+  a.kept_len = c->x_kept_len.as<uint64_t>(n6 + 1);
+  uint32_t* kidx = c->x_kept_index.as<uint32_t>(n6 + 1);
+  uint64_t* koff = c->x_kept_off.as<uint64_t>(n6 + 1);
+  a.kept_index = kidx;
+  a.kept_off = koff;
+  launch_translate_frames(a, c->stream);
+  cub_call(c, [&](void* t, size_t& b) {
+    return cub::DeviceScan::ExclusiveSum(t, b, a.keep, kidx, (int64_t)n6 + 1, c->stream);
+  });
+  cub_call(c, [&](void* t, size_t& b) {
+    return cub::DeviceScan::ExclusiveSum(t, b, a.kept_len, koff, (int64_t)n6 + 1, c->stream);
+  });
+  const uint64_t n = fetch(c, kidx + n6);
+  const uint64_t total = fetch(c, koff + n6);
+  drg_batch* b = new drg_batch();
+  b->ctx = ctx;
+  b->n = n;
+  b->total = total;
+  try {
+    pool_alloc(ctx, &b->letters, total + 64);
+    pool_alloc(ctx, &b->offsets, (n + 1) * sizeof(uint64_t));
+    pool_alloc(ctx, &b->owner, (total + 1) * sizeof(uint32_t));
+    DRG_CUDA(cudaMemsetAsync(b->letters + total, 25, 64, ctx->stream));
+    a.out = b->letters;
+    a.out_off = b->offsets;
+    a.out_query = c->x_query.as<uint32_t>(n + 1);
+    a.out_frame = c->x_frame.as<uint8_t>(n + 1);
+    launch_compact_frames(a, c->stream);
+    launch_letter_owner(b->offsets, n, 0, total, b->owner, ctx->stream);
+    fetch_n(c, b->h_offsets, b->offsets, n + 1);
+    fetch_n(c, b->query, a.out_query, n);
+    fetch_n(c, b->frame, a.out_frame, n);
+    for (uint64_t i = 0; i < n; ++i)
+      b->max_len = std::max<uint32_t>(b->max_len, (uint32_t)(b->h_offsets[i + 1] - b->h_offsets[i]));
+    if (host) {
+      fetch_n(c, host->letters, b->letters, total);
+      host->offsets = b->h_offsets;
+      host->query = b->query;
+      host->frame = b->frame;
+    }
+  } catch (...) {
+    free_batch(b);
+    throw;
+  }
+  return b;
+}
+
 void free_db(drg_db* d) {
   if (!d) return;
   d->cache.reset();

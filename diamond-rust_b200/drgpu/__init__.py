@@ -136,6 +136,10 @@ _SIGNATURES = {
     "drg_db_create": (C.c_int, [C.c_void_p, _u8p, _u64p, C.c_uint64, _P(C.c_void_p)]),
     "drg_db_destroy": (None, [C.c_void_p]),
     "drg_db_set_index_budget": (C.c_int, [C.c_void_p, C.c_uint64]),
+    "drg_batch_create_blastx": (C.c_int, [C.c_void_p, _u8p, _u64p, C.c_uint64, C.c_int64, _P(C.c_void_p)]),
+    "drg_translate_reads": (C.c_int, [C.c_void_p, _u8p, _u64p, C.c_uint64, C.c_int64, _P(_P(C.c_uint8)),
+                                      _P(_P(C.c_uint64)), _P(_P(C.c_uint32)), _P(_P(C.c_uint8)), _P(C.c_uint64)]),
+    "drg_batch_targets": (C.c_int, [C.c_void_p, _P(C.c_uint64), C.c_void_p, C.c_void_p]),
     "drg_db_index_stats": (C.c_int, [C.c_void_p, C.c_void_p]),
     "drg_batch_create": (C.c_int, [C.c_void_p, _u8p, _u64p, _u32p, _u8p, C.c_uint64, _P(C.c_void_p)]),
     "drg_batch_create_requests": (C.c_int, [C.c_void_p, _u8p, _u64p, _u32p, _u8p, _u32p, C.c_uint64,
@@ -409,6 +413,29 @@ class Context:
         self.lib.drg_result_free(C.byref(res))
         return n_hsps, n_ops, stats
 
+    def translate_reads(self, reads, min_orf=-1):
+        """blastx front end on the device: the kept frames of each read as
+        (list of letter arrays, read index per frame, frame 0-5 per frame)."""
+        nl, no = _reads_buffers(reads)
+        nlp, nop = _ptr(nl, C.c_uint8), _ptr(no, C.c_uint64)
+        L, O, Q, F = (C.POINTER(C.c_uint8)(), C.POINTER(C.c_uint64)(), C.POINTER(C.c_uint32)(),
+                      C.POINTER(C.c_uint8)())
+        n = C.c_uint64()
+        self._check(self.lib.drg_translate_reads(self.h, nlp, nop, len(no) - 1, int(min_orf), C.byref(L),
+                                                 C.byref(O), C.byref(Q), C.byref(F), C.byref(n)))
+        try:
+            k = n.value
+            offs = np.ctypeslib.as_array(O, shape=(k + 1,)).copy()
+            total = int(offs[-1])
+            letters = np.ctypeslib.as_array(L, shape=(max(total, 1),))[:total].copy()
+            query = np.ctypeslib.as_array(Q, shape=(max(k, 1),))[:k].copy()
+            frame = np.ctypeslib.as_array(F, shape=(max(k, 1),))[:k].copy()
+        finally:
+            for p in (L, O, Q, F):
+                self.lib.drg_free(C.cast(p, C.c_void_p))
+        frames = [letters[offs[i]:offs[i + 1]] for i in range(k)]
+        return frames, query, frame
+
     def probe_int_peak(self):
         ops, mhz = C.c_double(), C.c_double()
         self._check(self.lib.drg_probe_int_peak(self.h, C.byref(ops), C.byref(mhz)))
@@ -475,10 +502,45 @@ class ResidentBatch:
             self.h = None
 
 
-def search_resident(ctx: Context, db: ResidentDb, batch: ResidentBatch, config: SearchConfig, want_lists=True):
+def _reads_buffers(reads):
+    """Nucleotide reads (str or bytes) as one byte buffer with offsets."""
+    raw = [r.encode() if isinstance(r, str) else bytes(r) for r in reads]
+    offs = np.zeros(len(raw) + 1, np.uint64)
+    offs[1:] = np.cumsum([len(r) for r in raw]) if raw else []
+    buf = np.frombuffer(b"".join(raw) + b"\0", dtype=np.uint8).copy()
+    return buf, offs
+
+
+def blastx_batch(ctx: Context, reads, min_orf=-1):
+    """The reads' kept frames, translated on the device, as a resident batch
+    (drg_batch_create_blastx); .query / .frame hold each target's read and frame."""
+    nl, no = _reads_buffers(reads)
+    h = C.c_void_p()
+    ctx._check(ctx.lib.drg_batch_create_blastx(ctx.h, _ptr(nl, C.c_uint8), _ptr(no, C.c_uint64), len(no) - 1,
+                                               int(min_orf), C.byref(h)))
+    b = ResidentBatch.__new__(ResidentBatch)
+    b.ctx, b.h = ctx, h
+    n = C.c_uint64()
+    ctx._check(ctx.lib.drg_batch_targets(h, C.byref(n), None, None))
+    b.query = np.zeros(max(n.value, 1), np.uint32)
+    b.frame = np.zeros(max(n.value, 1), np.uint8)
+    ctx._check(ctx.lib.drg_batch_targets(h, C.byref(n), b.query.ctypes.data_as(C.c_void_p),
+                                         b.frame.ctypes.data_as(C.c_void_p)))
+    b.query, b.frame = b.query[:n.value], b.frame[:n.value]
+    return b
+
+
+def search_resident(ctx: Context, db: ResidentDb, batch: ResidentBatch, config: SearchConfig, want_lists=True,
+                    merge_queries=None):
+    """merge_queries = n: the frames' lists merged per query (drg_merge_frames,
+    search::merge_frames), by the batch's query index of each target."""
     res = Result()
     ctx._check(ctx.lib.drg_search_batch(ctx.h, db.h, batch.h, C.byref(config), C.byref(res)))
     try:
+        if merge_queries is not None:
+            tq = np.ascontiguousarray(batch.query, dtype=np.uint32)
+            ctx._check(ctx.lib.drg_merge_frames(C.byref(res), merge_queries, _ptr(tq, C.c_uint32), config.max_hsps,
+                                                config.max_target_seqs))
         lists = _result_lists(res) if want_lists else None
         return lists, res.stats.as_dict(), int(res.n_hsps)
     finally:

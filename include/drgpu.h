@@ -225,6 +225,28 @@ int drg_batch_create_requests(drg_ctx* ctx, const uint8_t* letters, const uint64
                               uint64_t n_targets, drg_batch** out);
 void drg_batch_destroy(drg_batch* b);
 
+/* blastx front end on the device (translate.rs:54-137 six_frames /
+ * mask_short_orfs / min_orf_len, workflow.rs:112-127): the six frames of each
+ * read (0-2 forward at offsets 0-2, 3-5 the reverse complement), stop-free
+ * stretches shorter than the minimum ORF length masked with X, frames without
+ * a letter below X dropped.  nt holds the reads' upper-cased bytes back to
+ * back (FASTA records' raw sequence), nt_offsets[n_reads + 1].  min_orf >= 0
+ * applies to every read; < 0 uses min_orf_len of each read's length.
+ * The kept frames, in (read, frame) order, become a target batch resident in
+ * device memory: query index = read, frame = 0-5 (for drg_search_batch, then
+ * drg_merge_frames with the read count). */
+int drg_batch_create_blastx(drg_ctx* ctx, const uint8_t* nt, const uint64_t* nt_offsets, uint64_t n_reads,
+                            int64_t min_orf, drg_batch** out);
+/* The same translation, returned to the host: letters, offsets[n_targets + 1],
+ * the read and the frame of each target (each freed with drg_free). */
+int drg_translate_reads(drg_ctx* ctx, const uint8_t* nt, const uint64_t* nt_offsets, uint64_t n_reads,
+                        int64_t min_orf, uint8_t** letters, uint64_t** offsets, uint32_t** query, uint8_t** frame,
+                        uint64_t* n_targets);
+/* A resident batch's targets: their count, and (when not null, n_targets
+ * entries each) the query index and frame of each (drg_merge_frames takes
+ * the query indices). */
+int drg_batch_targets(const drg_batch* b, uint64_t* n_targets, uint32_t* query, uint8_t* frame);
+
 /* search::run over resident inputs.  Results are per-target HSP lists, each
  * in the reference's order (best target first, search.rs:262-270). */
 int drg_search_batch(drg_ctx* ctx, const drg_db* db, const drg_batch* batch, const drg_search_config* cfg,
