@@ -98,14 +98,21 @@ class ClockSampler:
         self.device = device
         self.proc = None
         self.lines = []
+        self.skip = 0  # lines sampled before the timed region
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader",
-                                          "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                          "-lms", "50", "-i", str(self.device)], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # the timed region starts once the sampler is producing (a short
+            # region would otherwise end before nvidia-smi's first line)
+            t0 = time.perf_counter()
+            while not self.lines and time.perf_counter() - t0 < 3.0 and self.proc.poll() is None:
+                time.sleep(0.01)
+            self.skip = len(self.lines)
         except OSError:
             self.proc = None
         return self
@@ -125,7 +132,7 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in self.lines[self.skip:]:
             parts = [x.strip() for x in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -447,6 +454,7 @@ def main():
                                                          "ms_sw", "ms_sw_kernel", "ms_select", "ms_trace",
                                                          "ms_trace_kernel", "ms_host")},
             "sw_wide": {"bands": int(s0["sw_wide_bands"]), "ms": round(s0["ms_sw_wide"], 3)},
+            "sw_transposed_bands": int(s0["sw_transposed_bands"]),
             "sw_classes": {"width_max": [136, 272, 544, 1700], "warps": s0["sw_class_tasks"],
                            "longest_warp_steps": s0["sw_class_max_steps"],
                            "ms": [round(x, 3) for x in s0["ms_sw_class"]]},
