@@ -58,6 +58,7 @@ def parse():
     p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     p.add_argument("--no-serve", action="store_true", help="skip the serving stream (profiling runs)")
     p.add_argument("--no-blastx", action="store_true", help="skip the blastx leg (profiling runs)")
+    p.add_argument("--no-very-sensitive", action="store_true", help="skip the very-sensitive leg")
     p.add_argument("--blastx-reads", type=int, default=20000, help="reads in the blastx leg")
     p.add_argument("--serve-requests", type=int, default=100, help="requests in the serving stream")
     p.add_argument("--queries", type=int, default=None,
@@ -85,6 +86,16 @@ def config_desc(w):
         "sensitivity": SENS,
         "l2": "flushed between timed steps (256 MiB write)",
     }
+
+
+def measured_peaks():
+    """The pool's measured peaks (HBM copy GB/s, ...), or the fallback figures."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0, "fallback": True}
 
 
 class ClockSampler:
@@ -365,6 +376,43 @@ def main():
     gcups = cells_ref / (sw_ms / 1000.0) / 1e9 if sw_ms > 0 else 0.0
     launches = sum(s["kernel_launches"] for s in steps)
 
+    # ---- seed enumeration + sort + join (HBM-bound): algorithmic bytes per
+    # search = the letters read once per shape, each seed entry written and
+    # read once as 8 bytes, each hit written once as 16 bytes
+    sl = steps[-1]
+    S = int(sl["seed_shapes"])
+    seed_bytes = (S * (int(do[-1]) + int(to[-1])) + 16 * (int(sl["ref_seeds"]) + int(sl["query_seeds"]))
+                  + 16 * int(sl["hits"]))
+    seed_ms = sum(s["ms_seed"] + s["ms_join"] + s["ms_sort"] for s in steps) / len(steps)
+    hbm_peak = measured_peaks().get("hbm_gbs")
+    seed_stage = {"bound": "hbm", "ms": seed_ms, "algorithmic_bytes": seed_bytes,
+                  "achieved_gbs": seed_bytes / (seed_ms / 1000.0) / 1e9 if seed_ms > 0 else None,
+                  "peak_gbs": hbm_peak, "frac": (seed_bytes / (seed_ms / 1000.0) / 1e9 / hbm_peak)
+                  if hbm_peak and seed_ms > 0 else None,
+                  "peak_source": "hbm_gbs of fallback" if measured_peaks().get("fallback")
+                  else "MEASURED_PEAKS.json hbm_gbs (of measured)",
+                  "what": "seed enumeration, radix sorts and the join of one search (stages seed + join + sort, "
+                          "device time incl. the host round trips that size each launch)"}
+
+    # ---- very-sensitive (config 2's second preset), resident
+    vs = None
+    if not args.no_very_sensitive:
+        vcfg = drgpu.make_config(sensitivity="very-sensitive", index_chunks=1)
+        for _ in range(max(1, args.warmup)):
+            drgpu.search_resident(ctx, db, batch, vcfg, want_lists=False)
+        vsteps = []
+        barrier_sync(world)
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            vsteps.append(drgpu.search_resident(ctx, db, batch, vcfg, want_lists=False)[1])
+        barrier_sync(world)
+        vms = max_over_ranks(sum(s["ms_total"] for s in vsteps), world)
+        vsw = sum(s["ms_sw_kernel"] for s in vsteps) / len(vsteps)
+        vs = {"value": world * len(w.queries) * args.steps / (vms / 1000.0), "unit": "queries/s",
+              "ms_per_step": vms / args.steps, "gcups": sum(s["dp_cells_ref"] for s in vsteps) / len(vsteps)
+              / (vsw / 1000.0) / 1e9 if vsw > 0 else None, "hsps": int(vsteps[-1]["hsps"])}
+
     # ---- resident seed index: the DB's sorted reference seeds kept in HBM
     # across searches (built by the first, untimed search), not part of value
     idb = drgpu.ResidentDb(ctx, dl, do, index_budget=16 << 30)
@@ -464,6 +512,8 @@ def main():
             "e2e": e2e,
             "serving": serving,
             "index_resident": index_resident,
+            "very_sensitive": vs,
+            "seed_stage": seed_stage,
             "blastx": blastx,
             "gpu_launches": int(launches),
             "cpu_baseline": cpu,

@@ -526,7 +526,7 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
     // traceback: one warp per band (few, long bands)
     const BandJobs bj = make_band_jobs(c, swos, swks, n_fast, bc, s.offsets, true);
     SwBandArgs ba = band_args(bc, bj, qs, s, scr);
-    ba.trace = c->trace.as<uint2>(bj.trace_words);
+    ba.trace = c->trace.as<uint2>(bj.trace_words + 8);  // the walk reads 8-word windows
     ba.tband = tb;
     const int max_w = bj.max_width;
     cudaEvent_t e0, e1;
@@ -1273,6 +1273,7 @@ void Search::run(drg_result* out) {
   st.dp_cells_lane = cnt[4];
   st.dp_cells_issued = cnt[5];
   st.sw_transposed_bands = cnt[6];
+  st.seed_shapes = shapes.size();
   st.ms_total = total.stop();
   st.kernel_launches = kernel_launch_count() - launches0;
   out->stats = st;

@@ -332,8 +332,16 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS >= 2 ? 3 : 1) k_sw(SwScoreAr
 
 // Traceback of one band through the nibbles of the trace pass, in the
 // reference's order and with its stopping rules (gapped.rs:205-279).
-__global__ void k_sw_walk(SwWalkArgs a) {
+constexpr int kWalkThreads = 64;
+constexpr int kWalkWindow = 8;  // trace words a walker holds
+
+__global__ void __launch_bounds__(kWalkThreads) k_sw_walk(SwWalkArgs a) {
   __shared__ int8_t mat[625];  // lanes look up unrelated pairs: shared, not parameter space
+  // Each walker keeps a window of 8 consecutive trace words (word x of
+  // thread t at [x][t]).  A diagonal run steps to the next lower word, so one
+  // window load (four 16-byte loads issued together) serves up to 7 steps
+  // instead of one dependent load per step.
+  __shared__ uint2 win[kWalkWindow][kWalkThreads];
   for (int i = threadIdx.x; i < 625; i += blockDim.x) mat[i] = a.scores625[i];
   __syncthreads();
   const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
@@ -364,6 +372,7 @@ __global__ void k_sw_walk(SwWalkArgs a) {
   int state = 0;
   int64_t i = tb.best_i, j = tb.best_j;
   bool in_gap = false;
+  int64_t wb = -kWalkWindow;  // first word of the window (even: 16-byte aligned loads)
   while (i > 0 && j > 0) {
     int64_t lo = i - d1, hi = i - d0;
     lo = lo < 0 ? 0 : (lo > m ? m : lo);
@@ -372,7 +381,26 @@ __global__ void k_sw_walk(SwWalkArgs a) {
     const int64_t k = (i - rf) >> 4, r = (i - rf) & 15;
     const int64_t c = j - (rf + 16 * k - d1);
     const int64_t it = c + (r >= 8 ? 1 : 0);
-    const uint2 w = a.trace[tb.trace_off + (uint64_t)(k * (W + 16) + it) * (uint64_t)tb.stride];
+    const uint64_t g = tb.trace_off + (uint64_t)(k * (W + 16) + it) * (uint64_t)tb.stride;
+    uint2 w;
+    if (tb.stride == 1) {
+      if ((int64_t)g < wb || (int64_t)g >= wb + kWalkWindow) {
+        wb = (int64_t)g >= 6 ? (((int64_t)g - 6) & ~(int64_t)1) : 0;
+        const uint4* src = reinterpret_cast<const uint4*>(a.trace + wb);
+        const uint4 v0 = src[0], v1 = src[1], v2 = src[2], v3 = src[3];
+        win[0][threadIdx.x] = make_uint2(v0.x, v0.y);
+        win[1][threadIdx.x] = make_uint2(v0.z, v0.w);
+        win[2][threadIdx.x] = make_uint2(v1.x, v1.y);
+        win[3][threadIdx.x] = make_uint2(v1.z, v1.w);
+        win[4][threadIdx.x] = make_uint2(v2.x, v2.y);
+        win[5][threadIdx.x] = make_uint2(v2.z, v2.w);
+        win[6][threadIdx.x] = make_uint2(v3.x, v3.y);
+        win[7][threadIdx.x] = make_uint2(v3.z, v3.w);
+      }
+      w = win[g - wb][threadIdx.x];
+    } else {
+      w = a.trace[g];
+    }
     const uint32_t p = (uint32_t)(r & 7);
     const uint32_t byte = ((p < 4 ? w.x : w.y) >> (8 * (p & 3))) & 0xFFu;
     const uint32_t nib = r >= 8 ? byte >> 4 : byte & 0xFu;
@@ -469,7 +497,7 @@ void launch_sw_class(const SwScoreArgs& a, int cls, cudaStream_t st) {
 void launch_sw_walk(const SwWalkArgs& a, cudaStream_t st) {
   if (a.n_bands == 0) return;
   count_launch();
-  k_sw_walk<<<ceil_div(a.n_bands, 64), 64, 0, st>>>(a);
+  k_sw_walk<<<ceil_div(a.n_bands, kWalkThreads), kWalkThreads, 0, st>>>(a);
   DRG_CUDA(cudaGetLastError());
 }
 

@@ -88,7 +88,8 @@ class RunStats(C.Structure):
                 ("sw_class_tasks", C.c_uint64 * 4), ("sw_class_max_steps", C.c_uint64 * 4),
                 ("ms_sw_class", C.c_double * 4), ("ms_trace_kernel", C.c_double), ("dp_cells_lane", C.c_uint64),
                 ("sw_wide_bands", C.c_uint64), ("ms_sw_wide", C.c_double), ("dp_cells_issued", C.c_uint64),
-                ("index_hits", C.c_uint64), ("sw_transposed_bands", C.c_uint64)]
+                ("index_hits", C.c_uint64), ("sw_transposed_bands", C.c_uint64),
+                ("seed_shapes", C.c_uint64)]
 
     def as_dict(self):
         d = {}

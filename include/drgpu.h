@@ -110,6 +110,7 @@ typedef struct {
   uint64_t dp_cells_issued;        /* score kernel: warps x column steps x 16 x 32, idle lanes included */
   uint64_t index_hits;             /* index chunks whose sorted reference seeds came from the db's cache */
   uint64_t sw_transposed_bands;    /* score kernel: bands run with the subject as rows */
+  uint64_t seed_shapes;            /* shapes of the preset (seeds per letter enumerated) */
 } drg_run_stats;
 
 /* search::run result: per-target HSP lists, target_offsets[n_targets+1]. */
