@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "host/pool.h"
 #include "index_cache.h"
 #include "drgpu.h"
 #include "host/presets.h"
@@ -39,6 +40,7 @@ struct drg_ctx {
   drg::HostBuf h_stage;
   cudaEvent_t ev[16] = {};
   drg_run_stats last{};
+  std::unique_ptr<drg::host::Pool> host_pool;  // CPU-side steps of a search, created on first use
 };
 
 struct drg_db {

@@ -196,6 +196,21 @@ struct SwBandJob {
   uint32_t pad;
   uint64_t trace_off;  // trace mode: first uint2 of the band's nibbles
 };
+struct ExactOut;
+// Where a traced band's walk writes (per band t: ops at ops_off[t], n + m
+// slots; rev the same bytes as scratch; out[t] the record).
+struct WalkEnv {
+  const uint2* trace;
+  const uint8_t* q_letters;
+  const uint64_t* q_offsets;
+  const uint8_t* s_letters;
+  const uint64_t* s_offsets;
+  const uint64_t* ops_off;
+  uint8_t* rev;
+  uint32_t* ops;
+  ExactOut* out;
+  int exact_below;  // bands whose best is below this are left to the exact kernel
+};
 struct SwBandArgs {
   const Band* bands;
   const SwBandJob* jobs;
@@ -209,6 +224,7 @@ struct SwBandArgs {
   int32_t* best_row;  // score mode: first DP row holding the best
   uint2* trace;       // trace mode: nibbles, strip k's step c at trace_off + k (W + 16) + c
   TraceBand* tband;   // trace mode: per band
+  WalkEnv walk;       // trace mode: each band is walked right after its DP
   uint32_t xbuf_words;  // set by the launcher
   int8_t scores625[628];
 };
@@ -216,22 +232,6 @@ size_t sw_band_smem(int max_width);
 void launch_sw_band(SwBandArgs a, int max_width, bool trace, cudaStream_t st);
 
 struct ExactOut;
-struct SwWalkArgs {
-  const Band* bands;
-  const TraceBand* tband;
-  uint64_t n_bands;
-  const uint2* trace;
-  const uint8_t* q_letters;
-  const uint64_t* q_offsets;
-  const uint8_t* s_letters;
-  const uint64_t* s_offsets;
-  const uint64_t* ops_off;  // per band: first op slot (n + m slots each)
-  uint8_t* rev;             // per band: n + m bytes at ops_off
-  uint32_t* ops;
-  ExactOut* out;
-  int exact_below;  // bands whose best is below this were written by the exact kernel
-  int8_t scores625[628];
-};
 // Width classes of the packed kernel by the widest band of a warp (the shared
 // ring holds W + 1 words per thread); each fits 3 blocks per SM but the last.
 constexpr int kSwMinWidth = 17;   // narrower bands use the exact kernel
@@ -242,7 +242,6 @@ constexpr int kSwBandMinWidth = kSwC1 + 1;  // score pass: wider bands run one w
 constexpr int kSwClasses = 4;
 int sw_width_class(int width);  // 0..3, or -1 for the exact kernel
 void launch_sw_class(const SwScoreArgs& a, int cls, cudaStream_t st);  // score mode
-void launch_sw_walk(const SwWalkArgs& a, cudaStream_t st);
 
 // ---- exact DP with traceback (sw_exact.cu) ----------------------------------
 struct ExactJob {

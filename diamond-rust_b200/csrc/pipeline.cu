@@ -15,6 +15,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <thread>
 #include <cmath>
 #include <cstring>
 #include <numeric>
@@ -533,24 +534,20 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
     DRG_CUDA(cudaEventCreate(&e0));
     DRG_CUDA(cudaEventCreate(&e1));
     DRG_CUDA(cudaEventRecord(e0, c->stream));
+    // each band's walk (gapped.rs:205-279) runs in the band kernel right
+    // after its DP
+    ba.walk.trace = ba.trace;
+    ba.walk.q_letters = qs.letters;
+    ba.walk.q_offsets = qs.offsets;
+    ba.walk.s_letters = s.letters;
+    ba.walk.s_offsets = s.offsets;
+    ba.walk.ops_off = d_ops_off;
+    ba.walk.rev = c->rev.as<uint8_t>((*h_ops_off)[n_bands] + 16);
+    ba.walk.ops = ops;
+    ba.walk.out = out;
+    ba.walk.exact_below = scr.max_score + 1;
     launch_sw_band(ba, max_w, true, c->stream);
     DRG_CUDA(cudaEventRecord(e1, c->stream));
-    SwWalkArgs wa{};
-    wa.bands = bc;
-    wa.tband = tb;
-    wa.n_bands = n_bands;
-    wa.trace = ba.trace;
-    wa.q_letters = qs.letters;
-    wa.q_offsets = qs.offsets;
-    wa.s_letters = s.letters;
-    wa.s_offsets = s.offsets;
-    wa.ops_off = d_ops_off;
-    wa.rev = c->rev.as<uint8_t>((*h_ops_off)[n_bands] + 16);
-    wa.ops = ops;
-    wa.out = out;
-    wa.exact_below = scr.max_score + 1;
-    std::memcpy(wa.scores625, scr.scores, 625);
-    launch_sw_walk(wa, c->stream);
     DRG_CUDA(cudaEventSynchronize(e1));
     float ms = 0;
     DRG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
@@ -746,6 +743,7 @@ struct Search {
   uint64_t index_chunks = 1;
   double evalue = 1e-3;
   uint64_t max_hsps = 1, max_targets = 25;
+  uint64_t host_threads = 0;  // 0: all of the context's host threads
   drg_run_stats st{};
   std::vector<Candidate> cands;
   // device scratch for counters
@@ -767,6 +765,7 @@ struct Search {
     evalue = cfg->evalue;
     max_hsps = std::max<uint32_t>(cfg->max_hsps, 1);
     max_targets = std::max<uint32_t>(cfg->max_target_seqs, 1);
+    host_threads = cfg->threads;
     if ((int)shapes.size() > kMaxShapes) throw Error(DRG_ERR_INVALID, "too many seed shapes");
     ShapeTable t{};
     t.n = (int)shapes.size();
@@ -1085,6 +1084,25 @@ int cmp_cand(const Candidate& a, const Candidate& b) {  // cmp_hsp, search.rs:27
 
 void Search::finish(drg_result* out) {
   auto t0 = std::chrono::steady_clock::now();
+  // The exact host E-values (glibc libm, like the reference) of every
+  // candidate, on the context's host threads: a pure function of (score,
+  // qlen, slen), used below in the reference's order.
+  std::vector<double> ev(cands.size(), 0.0);
+  {
+    if (!c->host_pool) {
+      const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+      c->host_pool.reset(new host::Pool(std::min(hw - 1, 15u)));
+    }
+    c->host_pool->parallel_for(cands.size(), 256, host_threads, [&](uint64_t lo, uint64_t hi) {
+      for (uint64_t k = lo; k < hi; ++k) {
+        const Candidate& cd = cands[k];
+        if (cd.score <= 0) continue;
+        const uint64_t qlen = q->h_offsets[cd.band.target + 1] - q->h_offsets[cd.band.target];
+        const uint64_t slen = db->h_offsets[cd.band.subject + 1] - db->h_offsets[cd.band.subject];
+        ev[k] = sc.evalue(cd.score, qlen, slen, db->total);
+      }
+    });
+  }
   // exact statistics and the walk of undecided pairs
   std::vector<Candidate> kept;
   kept.reserve(cands.size());
@@ -1094,17 +1112,15 @@ void Search::finish(drg_result* out) {
     uint64_t nkept = 0;
     for (size_t k = i; k < j; ++k) {
       Candidate cd = cands[k];
-      const uint64_t qlen = q->h_offsets[cd.band.target + 1] - q->h_offsets[cd.band.target];
-      const uint64_t slen = db->h_offsets[cd.band.subject + 1] - db->h_offsets[cd.band.subject];
       if (cd.state == 2) {
-        cd.evalue = sc.evalue(cd.score, qlen, slen, db->total);
+        cd.evalue = ev[k];
         cd.bits = sc.bit_score(cd.score);
         kept.push_back(cd);
         ++nkept;
       } else {  // undecided: continue the reference's walk exactly
         if (nkept >= max_hsps) continue;
         if (cd.score <= 0) continue;
-        double e = sc.evalue(cd.score, qlen, slen, db->total);
+        const double e = ev[k];
         if (e <= evalue) {
           cd.evalue = e;
           cd.bits = sc.bit_score(cd.score);

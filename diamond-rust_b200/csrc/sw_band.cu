@@ -19,6 +19,7 @@
 // nibbles with a unit lane stride.
 #include "kernels.h"
 #include "sw_common.cuh"
+#include "sw_walk.cuh"
 
 namespace drg {
 
@@ -241,6 +242,9 @@ __global__ void __launch_bounds__(kBandWarps * 32) k_sw_band(SwBandArgs a) {
     tb.best_j = best_j;
     tb.stride = 1;  // consecutive column steps
     a.tband[job.band] = tb;
+    // the walk, while the SM's other warps run DP; the warp's exchange
+    // buffer (free now) holds its 8-word trace window
+    walk_band(a.walk, job.band, band, tb, mat, reinterpret_cast<uint2*>(xbuf), 1);
   }
 }
 

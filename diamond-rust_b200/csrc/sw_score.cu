@@ -1,6 +1,5 @@
-// Banded affine Smith-Waterman (gapped.rs:67-280) for many bands that share a
-// query window: the score pass of the E-value gate and the traceback of the
-// HSPs that survive it.
+// Banded affine Smith-Waterman (gapped.rs:67-203) for many bands that share a
+// query window (or a subject, transposed): the score pass of the E-value gate.
 //
 // Mapping (inter-task): one thread = one band; one warp = up to 32 bands of
 // the same query window and width W, so the query profile is shared per warp.
@@ -31,10 +30,8 @@
 // exactly.  Cells left or right of the band in the first/last 16 steps of
 // a strip are masked: their H does not count and they pass -inf-like E/F.
 //
-// Trace mode also writes, per cell, the reference's trace nibble
-// (choice | e_ext << 2 | f_ext << 3, gapped.rs:171-188) into a lane-interleaved
-// buffer and tracks the first row-major maximum; a walk kernel then follows
-// the reference's traceback (gapped.rs:205-279) through those nibbles.
+// The traceback of the HSPs that pass the gate runs in sw_band.cu (one warp
+// per band) and sw_walk.cuh.
 #include "kernels.h"
 #include "sw_common.cuh"
 
@@ -330,136 +327,6 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS >= 2 ? 3 : 1) k_sw(SwScoreAr
   if (a.best_row) a.best_row[bidx] = best_i;
 }
 
-// Traceback of one band through the nibbles of the trace pass, in the
-// reference's order and with its stopping rules (gapped.rs:205-279).
-constexpr int kWalkThreads = 64;
-constexpr int kWalkWindow = 8;  // trace words a walker holds
-
-__global__ void __launch_bounds__(kWalkThreads) k_sw_walk(SwWalkArgs a) {
-  __shared__ int8_t mat[625];  // lanes look up unrelated pairs: shared, not parameter space
-  // Each walker keeps a window of 8 consecutive trace words (word x of
-  // thread t at [x][t]).  A diagonal run steps to the next lower word, so one
-  // window load (four 16-byte loads issued together) serves up to 7 steps
-  // instead of one dependent load per step.
-  __shared__ uint2 win[kWalkWindow][kWalkThreads];
-  for (int i = threadIdx.x; i < 625; i += blockDim.x) mat[i] = a.scores625[i];
-  __syncthreads();
-  const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (t >= a.n_bands) return;
-  const Band b = a.bands[t];
-  const TraceBand tb = a.tband[t];
-  ExactOut R;
-  R.score = 0;
-  R.q_begin = R.q_end = R.s_begin = R.s_end = 0;
-  R.identities = R.positives = R.mismatches = R.gap_openings = R.gaps = R.length = 0;
-  R.n_ops = 0;
-  R.cells = 0;
-  if (tb.score < a.exact_below) return;  // not traced here: the exact kernel writes this band
-  const uint8_t* q = a.q_letters + a.q_offsets[b.target] + b.q0;
-  const uint8_t* s = a.s_letters + a.s_offsets[b.subject];
-  const int64_t m = (int64_t)(a.s_offsets[b.subject + 1] - a.s_offsets[b.subject]);
-  const int64_t d0 = b.d0, d1 = b.d1, W = tb.width, rf = tb.row_first;
-  if (tb.best_i < 1 || tb.best_i > (int64_t)b.n || tb.best_j < 1 || tb.best_j > m) {
-    R.score = -1;  // cannot happen for a best this high; reported to the host as an internal error
-    a.out[t] = R;
-    return;
-  }
-  R.score = tb.score;
-  R.q_end = (uint32_t)tb.best_i;
-  R.s_end = (uint32_t)tb.best_j;
-  uint8_t* rev = a.rev + a.ops_off[t];
-  uint32_t nrev = 0;
-  int state = 0;
-  int64_t i = tb.best_i, j = tb.best_j;
-  bool in_gap = false;
-  int64_t wb = -kWalkWindow;  // first word of the window (even: 16-byte aligned loads)
-  while (i > 0 && j > 0) {
-    int64_t lo = i - d1, hi = i - d0;
-    lo = lo < 0 ? 0 : (lo > m ? m : lo);
-    hi = hi < 0 ? 0 : (hi > m ? m : hi);
-    if (j < lo || j > hi || i < rf) break;
-    const int64_t k = (i - rf) >> 4, r = (i - rf) & 15;
-    const int64_t c = j - (rf + 16 * k - d1);
-    const int64_t it = c + (r >= 8 ? 1 : 0);
-    const uint64_t g = tb.trace_off + (uint64_t)(k * (W + 16) + it) * (uint64_t)tb.stride;
-    uint2 w;
-    if (tb.stride == 1) {
-      if ((int64_t)g < wb || (int64_t)g >= wb + kWalkWindow) {
-        wb = (int64_t)g >= 6 ? (((int64_t)g - 6) & ~(int64_t)1) : 0;
-        const uint4* src = reinterpret_cast<const uint4*>(a.trace + wb);
-        const uint4 v0 = src[0], v1 = src[1], v2 = src[2], v3 = src[3];
-        win[0][threadIdx.x] = make_uint2(v0.x, v0.y);
-        win[1][threadIdx.x] = make_uint2(v0.z, v0.w);
-        win[2][threadIdx.x] = make_uint2(v1.x, v1.y);
-        win[3][threadIdx.x] = make_uint2(v1.z, v1.w);
-        win[4][threadIdx.x] = make_uint2(v2.x, v2.y);
-        win[5][threadIdx.x] = make_uint2(v2.z, v2.w);
-        win[6][threadIdx.x] = make_uint2(v3.x, v3.y);
-        win[7][threadIdx.x] = make_uint2(v3.z, v3.w);
-      }
-      w = win[g - wb][threadIdx.x];
-    } else {
-      w = a.trace[g];
-    }
-    const uint32_t p = (uint32_t)(r & 7);
-    const uint32_t byte = ((p < 4 ? w.x : w.y) >> (8 * (p & 3))) & 0xFFu;
-    const uint32_t nib = r >= 8 ? byte >> 4 : byte & 0xFu;
-    if (state == 0) {
-      const uint32_t ch = nib & 3;
-      if (ch == 0) break;
-      if (ch == 1) {
-        const uint32_t x = q[i - 1], y = s[j - 1];
-        R.length++;
-        if (x == y) R.identities++;
-        else R.mismatches++;
-        if (mat[(x < 24 ? x : 24) * 25 + (y < 24 ? y : 24)] > 0) R.positives++;
-        rev[nrev++] = 0;
-        in_gap = false;
-        --i;
-        --j;
-      } else {
-        state = ch == 2 ? 1 : 2;
-      }
-    } else if (state == 1) {
-      R.length++;
-      R.gaps++;
-      if (!in_gap) {
-        R.gap_openings++;
-        in_gap = true;
-      }
-      rev[nrev++] = 1;
-      if (((nib >> 2) & 1) == 0) state = 0;
-      --i;
-    } else {
-      R.length++;
-      R.gaps++;
-      if (!in_gap) {
-        R.gap_openings++;
-        in_gap = true;
-      }
-      rev[nrev++] = 2;
-      if (((nib >> 3) & 1) == 0) state = 0;
-      --j;
-    }
-  }
-  R.q_begin = (uint32_t)i;
-  R.s_begin = (uint32_t)j;
-  uint32_t* o = a.ops + a.ops_off[t];
-  uint32_t nops = 0;
-  int64_t x = (int64_t)nrev - 1;
-  while (x >= 0) {
-    const uint32_t op = rev[x];
-    uint32_t cnt = 0;
-    while (x >= 0 && rev[x] == op) {
-      ++cnt;
-      --x;
-    }
-    o[nops++] = (cnt << 2) | op;
-  }
-  R.n_ops = nops;
-  a.out[t] = R;
-}
-
 template <int WARPS>
 void launch_class(const SwScoreArgs& a, int max_width, cudaStream_t st) {
   if (a.task_hi <= a.task_lo) return;
@@ -494,11 +361,5 @@ void launch_sw_class(const SwScoreArgs& a, int cls, cudaStream_t st) {
   }
 }
 
-void launch_sw_walk(const SwWalkArgs& a, cudaStream_t st) {
-  if (a.n_bands == 0) return;
-  count_launch();
-  k_sw_walk<<<ceil_div(a.n_bands, kWalkThreads), kWalkThreads, 0, st>>>(a);
-  DRG_CUDA(cudaGetLastError());
-}
 
 }  // namespace drg
