@@ -230,6 +230,17 @@ struct SwBandArgs {
 };
 size_t sw_band_smem(int max_width);
 void launch_sw_band(SwBandArgs a, int max_width, bool trace, cudaStream_t st);
+// Bands by width: route 0 (W <= 134), 1 (<= 271), 2 (<= 559) run in groups
+// of 8, 16, 32 lanes with rotating strips; route 3 (wider) in the block
+// kernel.  The traceback pass's few bands keep a warp each (route 2 up to
+// W 559): with several bands per warp too few warps remain to hide the
+// step's dependency chain.  max_width matters for route 3 only.
+__host__ __device__ inline int sw_band_route(int width, bool trace) {
+  if (width > 559) return 3;
+  if (trace) return 2;
+  return width <= 134 ? 0 : (width <= 271 ? 1 : 2);
+}
+void launch_sw_band_route(const SwBandArgs& a, int route, int max_width, bool trace, cudaStream_t st);
 
 struct ExactOut;
 // Width classes of the packed kernel by the widest band of a warp (the shared

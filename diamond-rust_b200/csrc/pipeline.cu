@@ -319,8 +319,8 @@ __global__ void k_compact_ops(const uint32_t* ops, const uint64_t* ops_off, cons
 // Jobs of the one-warp-per-band kernel for the first n bands of the sorted
 // order: rows [rs, re] (re limited to the best row when known), longest first.
 __global__ void k_band_jobs(const uint32_t* order, const uint64_t* keys, uint64_t n, const Band* bands,
-                            const uint64_t* s_offsets, SwBandJob* jobs, uint64_t* sort_key, uint32_t* sort_val,
-                            unsigned long long* max_width) {
+                            const uint64_t* s_offsets, bool trace, SwBandJob* jobs, uint64_t* sort_key,
+                            uint32_t* sort_val, unsigned long long* max_width) {
   uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (k >= n) return;
   const uint32_t i = order[k];
@@ -338,11 +338,13 @@ __global__ void k_band_jobs(const uint32_t* order, const uint64_t* keys, uint64_
   j.pad = W;
   j.trace_off = 0;
   jobs[k] = j;
-  const uint64_t blocks = (j.n_strips + 31) / 32;
-  const uint64_t cost = blocks * (W + 16ull) + (uint64_t)(j.n_strips - 1) * 18ull;
-  sort_key[k] = ~cost;  // longest first
+  // by kernel route (sw_band_route), then longest first
+  const int route = sw_band_route((int)W, trace);
+  const uint64_t cost = (uint64_t)(j.n_strips - 1) * 19ull + W + 16ull;
+  sort_key[k] = ((uint64_t)route << 60) | ((~cost) & ((1ull << 60) - 1));
   sort_val[k] = (uint32_t)k;
   atomicMax(max_width, (unsigned long long)W);
+  atomicAdd(max_width + 1 + route, 1ull);
 }
 __global__ void k_gather_band_jobs(const SwBandJob* in, const uint32_t* idx, uint64_t n, SwBandJob* out,
                                    uint64_t* size) {
@@ -428,6 +430,7 @@ struct BandJobs {
   uint64_t n = 0;
   int max_width = 0;
   uint64_t trace_words = 0;
+  uint64_t route_lo[5] = {0, 0, 0, 0, 0};  // jobs [route_lo[r], route_lo[r + 1]) take route r
 };
 BandJobs make_band_jobs(drg_ctx* c, const uint32_t* order, const uint64_t* keys, uint64_t n, const Band* bc,
                         const uint64_t* s_offsets, bool trace) {
@@ -440,10 +443,11 @@ BandJobs make_band_jobs(drg_ctx* c, const uint32_t* order, const uint64_t* keys,
   uint64_t* key_s = c->bj_key_s.as<uint64_t>(n);
   uint32_t* val = c->bj_val.as<uint32_t>(n);
   uint32_t* val_s = c->bj_val_s.as<uint32_t>(n);
-  unsigned long long* dmaxw = c->bj_max.as<unsigned long long>(1);
-  DRG_CUDA(cudaMemsetAsync(dmaxw, 0, sizeof(unsigned long long), c->stream));
+  unsigned long long* dmaxw = c->bj_max.as<unsigned long long>(5);  // max width, jobs per route
+  DRG_CUDA(cudaMemsetAsync(dmaxw, 0, 5 * sizeof(unsigned long long), c->stream));
   count_launch();
-  k_band_jobs<<<ceil_div(n, 256), 256, 0, c->stream>>>(order, keys, n, bc, s_offsets, jobs_u, key, val, dmaxw);
+  k_band_jobs<<<ceil_div(n, 256), 256, 0, c->stream>>>(order, keys, n, bc, s_offsets, trace, jobs_u, key, val,
+                                                       dmaxw);
   cub_call(c, [&](void* t, size_t& b) {
     return cub::DeviceRadixSort::SortPairs(t, b, key, key_s, val, val_s, (int64_t)n, 0, 64, c->stream);
   });
@@ -459,8 +463,21 @@ BandJobs make_band_jobs(drg_ctx* c, const uint32_t* order, const uint64_t* keys,
     k_set_band_trace_off<<<ceil_div(n, 256), 256, 0, c->stream>>>(r.jobs, off, n);
     r.trace_words = fetch(c, off + n);
   }
-  r.max_width = (int)fetch(c, dmaxw);
+  unsigned long long h[5];
+  DRG_CUDA(cudaMemcpyAsync(h, dmaxw, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  DRG_CUDA(cudaStreamSynchronize(c->stream));
+  r.max_width = (int)h[0];
+  for (int k = 0; k < 4; ++k) r.route_lo[k + 1] = r.route_lo[k] + h[1 + k];
   return r;
+}
+
+// The band kernels of jobs bj, one launch per route.
+void launch_band_routes(SwBandArgs ba, const BandJobs& bj, bool trace, cudaStream_t st) {
+  for (int k = 0; k < 4; ++k) {
+    ba.lo = bj.route_lo[k];
+    ba.hi = bj.route_lo[k + 1];
+    launch_sw_band_route(ba, k, bj.max_width, trace, st);
+  }
 }
 
 SwBandArgs band_args(const Band* bc, const BandJobs& bj, const DevSeqs& qs, const DevSeqs& s, const Scoring& scr) {
@@ -529,7 +546,6 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
     SwBandArgs ba = band_args(bc, bj, qs, s, scr);
     ba.trace = c->trace.as<uint2>(bj.trace_words + 8);  // the walk reads 8-word windows
     ba.tband = tb;
-    const int max_w = bj.max_width;
     cudaEvent_t e0, e1;
     DRG_CUDA(cudaEventCreate(&e0));
     DRG_CUDA(cudaEventCreate(&e1));
@@ -546,7 +562,7 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
     ba.walk.ops = ops;
     ba.walk.out = out;
     ba.walk.exact_below = scr.max_score + 1;
-    launch_sw_band(ba, max_w, true, c->stream);
+    launch_band_routes(ba, bj, true, c->stream);
     DRG_CUDA(cudaEventRecord(e1, c->stream));
     DRG_CUDA(cudaEventSynchronize(e1));
     float ms = 0;
@@ -653,7 +669,7 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
       SwBandArgs ba = band_args(bc, wide, qs, s, scr);
       ba.score = scores;
       ba.best_row = best_row;
-      launch_sw_band(ba, wide.max_width, false, c->side);
+      launch_band_routes(ba, wide, false, c->side);
       st.sw_launches += 1;
     }
     DRG_CUDA(cudaEventRecord(ev[wide1], c->side));

@@ -248,7 +248,199 @@ __global__ void __launch_bounds__(kBandWarps * 32) k_sw_band(SwBandArgs a) {
   }
 }
 
+// ---- rotating strips: G lanes per band, several bands per warp --------------
+//
+// One band needs about (W + 16) / 18 lanes at a time: strip s + 1 can start 18
+// steps after strip s (the lag above) and a strip lasts W + 16 steps.  So a
+// warp holds 32 / G bands, G lanes each, and lane l of a group runs strips l,
+// l + G, l + 2G, ...: strip s starts at group time Lag * s on lane s mod G,
+// and takes the row above from lane (s - 1) mod G by a shuffle.  Lag is 18
+// (or 19 for 8-lane groups of widths 128-134) under two conditions on the
+// width: a lane's strips do not overlap (W + 16 <= G * Lag), and a strip
+// has passed its last column (and sends -inf) before its lane starts the
+// next strip while its successor still reads it (W - 1 <= (G - 1) * Lag).
+// Routes: G = 8 for W <= 134, 16 for W <= 271, 32 for W <= 559; wider bands
+// use the block kernel above.
+constexpr int kRotWarps = 4;
+
+template <int G>
+__device__ __forceinline__ int rot_lag(int w_max) {
+  return (G == 8 && w_max > 127) ? kLag + 1 : kLag;
+}
+
+template <int G, bool TR>
+__global__ void __launch_bounds__(kRotWarps * 32) k_sw_rot(SwBandArgs a) {
+  constexpr int NG = 32 / G;  // bands per warp
+  extern __shared__ __align__(16) uint8_t smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int grp = lane / G, gl = lane % G;
+  int8_t* mat = reinterpret_cast<int8_t*>(smem);
+  for (int i = threadIdx.x; i < 625; i += blockDim.x) mat[i] = a.scores625[i];
+  __syncthreads();
+  uint8_t* prof_base = smem + 640 + (size_t)(warp * 32) * kLaneProf;  // lane x's profile at x * kLaneProf
+  uint8_t* prof = prof_base + (size_t)lane * kLaneProf;
+  uint2* win = reinterpret_cast<uint2*>(smem + 640 + (size_t)kRotWarps * 32 * kLaneProf) +
+               (size_t)(warp * NG + grp) * kWalkWindow;  // the group's walk window
+  const uint64_t t = a.lo + ((uint64_t)blockIdx.x * kRotWarps + warp) * NG + grp;
+  const bool has_job = t < a.hi;
+  SwBandJob job{};
+  Band band{};
+  if (has_job) {
+    job = a.jobs[t];
+    band = a.bands[job.band];
+  }
+  const int W = has_job ? band.d1 - band.d0 + 1 : 0;
+  const int steps = W + kRows;
+  const int S = has_job ? (int)job.n_strips : 0;
+  const int lag = rot_lag<G>(__reduce_max_sync(0xFFFFFFFFu, W));
+  const int t_group = S > 0 ? lag * (S - 1) + steps : 0;
+  const int t_end = __reduce_max_sync(0xFFFFFFFFu, t_group);
+  const uint8_t* q = has_job ? a.q_letters + a.q_offsets[band.target] + band.q0 : a.q_letters;
+  const int n = has_job ? (int)band.n : 0;
+  Lane L;
+  L.s = has_job ? a.s_letters + a.s_offsets[band.subject] : a.s_letters;
+  L.m = has_job ? (int)(a.s_offsets[band.subject + 1] - a.s_offsets[band.subject]) : 0;
+  const uint32_t noc2 = (uint32_t)(uint16_t)(-(a.gap_open + a.gap_extend)) * 0x10001u;
+  const uint32_t nge2 = (uint32_t)(uint16_t)(-a.gap_extend) * 0x10001u;
+  const int src = grp * G + (gl + G - 1) % G;  // the lane of the previous strip
+  int best = 0, best_i = 0, best_j = 0;
+  Regs<TR> R;
+  int s = gl;            // this lane's current (or next) strip
+  int c = -lag * gl;     // its column: strip s starts at group time lag * s
+  int i0 = 0;
+  uint2* tr = nullptr;
+  uint32_t rw_prev = 0xC0000000u, out_prev = kNeg2, out_prev2 = kNeg2;
+  int ph = 0, s0 = 0;  // group time modulo lag; the strip starting at the next multiple
+  // the query letters of strip s0's rows, loaded one strip ahead of the
+  // profile they feed (the loads' latency then hides behind lag steps)
+  uint32_t qr[kRows];
+  auto load_rows = [&](int sk) {
+    const int ib = (int)job.row_first + kRows * sk;
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) {
+      const int i = ib + r;
+      qr[r] = (sk >= S || i > n) ? 255u : (uint32_t)min((uint32_t)q[i - 1], 24u);
+    }
+  };
+  load_rows(0);
+  for (int T = 0; T < t_end; ++T) {
+    // The strip starting now (group time lag * s0) gets its profile from the
+    // whole group: lane x of the group fills residues x, x + G, ...
+    if (ph == 0) {
+      if (s0 < S) {
+        uint8_t* dst = prof_base + (size_t)(grp * G + s0 % G) * kLaneProf;
+        for (int res = gl; res < 26; res += G) {
+#pragma unroll
+          for (int r4 = 0; r4 < 4; ++r4) {
+            uint32_t w = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              const uint32_t r = qr[r4 * 4 + k];
+              const int v = (res == 25 || r == 255u) ? kSentinelScore : mat[r * 25 + res];
+              w |= ((uint32_t)(uint8_t)(int8_t)v) << (8 * k);
+            }
+            *reinterpret_cast<uint32_t*>(dst + res * kRows + r4 * 4) = w;
+          }
+        }
+      }
+      ++s0;
+      load_rows(s0);
+      __syncwarp();
+    }
+    if (++ph == lag) ph = 0;
+    // the row above at this lane's column: the previous strip's word, or
+    // row 0 of the reference for the band's first strip
+    uint32_t rw = __shfl_sync(0xFFFFFFFFu, lag == kLag ? out_prev : out_prev2, src);
+    if (s == 0) rw = c < W - 1 ? 0xC0000000u : kNeg2;
+    uint32_t out = kNeg2;  // a lane between strips passes -inf
+    if (s < S && c >= 0 && c < steps) {
+      if (c == 0) {
+        i0 = (int)job.row_first + kRows * s;
+        L.jbase = i0 - band.d1;
+        if (TR) tr = a.trace + job.trace_off + (uint64_t)s * steps;
+#pragma unroll
+        for (int p = 0; p < kPairs; ++p) {
+          R.H[p] = 0;
+          R.Hm[p] = kNeg2;
+          R.F[p] = kNeg2;
+          R.rowmax[p] = 0;
+          if (TR) R.rowcol[p] = 0;
+        }
+        R.E7 = kNeg2;
+        R.htop_old = s == 0 ? 0u : (rw_prev & 0xFFFFu);
+        R.res_prev = subject_residue(L, L.jbase - 2);
+      }
+      const uint32_t cc2 = (uint32_t)c * 0x10001u;
+      const uint32_t cw2 = (uint32_t)(uint16_t)(c - W) * 0x10001u;
+      out = band_step<TR>(R, L, c, cc2, cw2, prof, rw, noc2, nge2, TR ? tr + c : nullptr);
+      if (c == steps - 1) {
+#pragma unroll
+        for (int r = 0; r < kRows; ++r) {
+          const int v = r < kPairs ? lo16(R.rowmax[r]) : hi16(R.rowmax[r - kPairs]);
+          if (v > best) {
+            best = v;
+            best_i = i0 + r;
+            if (TR) best_j = L.jbase + (r < kPairs ? lo16(R.rowcol[r]) : hi16(R.rowcol[r - kPairs]));
+          }
+        }
+      }
+    }
+    rw_prev = rw;
+    out_prev2 = out_prev;
+    out_prev = out;
+    if (++c == G * lag) {  // this lane's next strip
+      c = 0;
+      s += G;
+    }
+  }
+  __syncwarp();
+  // first row-major maximum over the group: highest score, then lowest row
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) {
+    const int ob = __shfl_xor_sync(0xFFFFFFFFu, best, o);
+    const int oi = __shfl_xor_sync(0xFFFFFFFFu, best_i, o);
+    const int oj = __shfl_xor_sync(0xFFFFFFFFu, best_j, o);
+    if (ob > best || (ob == best && ob > 0 && oi < best_i)) {
+      best = ob;
+      best_i = oi;
+      best_j = oj;
+    }
+  }
+  if (best == 0) best_i = best_j = 0;
+  if (gl != 0 || !has_job) return;
+  if (!TR) {
+    a.score[job.band] = best;
+    if (a.best_row) a.best_row[job.band] = best_i;
+  } else {
+    TraceBand tb;
+    tb.trace_off = job.trace_off;
+    tb.row_first = job.row_first;
+    tb.width = (uint32_t)W;
+    tb.score = best;
+    tb.best_i = best_i;
+    tb.best_j = best_j;
+    tb.stride = 1;
+    a.tband[job.band] = tb;
+    walk_band(a.walk, job.band, band, tb, mat, win, 1);
+  }
+}
+
 }  // namespace
+
+template <int G, bool TR>
+void launch_rot(const SwBandArgs& a, cudaStream_t st) {
+  constexpr int NG = 32 / G;
+  const size_t smem = 640 + (size_t)kRotWarps * 32 * kLaneProf + (size_t)kRotWarps * NG * kWalkWindow * 8;
+  static bool configured = false;
+  if (!configured) {
+    DRG_CUDA(cudaFuncSetAttribute(k_sw_rot<G, TR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    configured = true;
+  }
+  const int blocks = ceil_div((long long)(a.hi - a.lo), kRotWarps * NG);
+  count_launch();
+  k_sw_rot<G, TR><<<blocks, kRotWarps * 32, smem, st>>>(a);
+  DRG_CUDA(cudaGetLastError());
+}
 
 size_t sw_band_smem(int max_width) {
   const size_t xwords = (size_t)(max_width + kRows + 2) & ~(size_t)1;
@@ -270,6 +462,16 @@ void launch_sw_band(SwBandArgs a, int max_width, bool trace, cudaStream_t st) {
   if (trace) k_sw_band<true><<<blocks, kBandWarps * 32, smem, st>>>(a);
   else k_sw_band<false><<<blocks, kBandWarps * 32, smem, st>>>(a);
   DRG_CUDA(cudaGetLastError());
+}
+
+void launch_sw_band_route(const SwBandArgs& a, int route, int max_width, bool trace, cudaStream_t st) {
+  if (a.hi <= a.lo) return;
+  switch (route) {
+    case 0: trace ? launch_rot<8, true>(a, st) : launch_rot<8, false>(a, st); break;
+    case 1: trace ? launch_rot<16, true>(a, st) : launch_rot<16, false>(a, st); break;
+    case 2: trace ? launch_rot<32, true>(a, st) : launch_rot<32, false>(a, st); break;
+    default: launch_sw_band(a, max_width, trace, st); break;
+  }
 }
 
 }  // namespace drg
