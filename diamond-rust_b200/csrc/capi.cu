@@ -50,6 +50,7 @@ namespace {
 // Device copy of a sequence set with its letter -> sequence map.
 struct Seqs {
   uint8_t* letters = nullptr;
+  uint8_t* score_letters = nullptr;  // clamped to 24 for the DP kernels, when some code is above 24
   uint64_t* offsets = nullptr;
   uint32_t* owner = nullptr;
   std::vector<uint64_t> h_offsets;
@@ -58,6 +59,7 @@ struct Seqs {
   Seqs(const Seqs&) = delete;
   ~Seqs() {
     cudaFree(letters);
+    cudaFree(score_letters);
     cudaFree(offsets);
     cudaFree(owner);
   }
@@ -74,8 +76,13 @@ struct Seqs {
     if (total) DRG_CUDA(cudaMemcpyAsync(letters, l, total, cudaMemcpyHostToDevice, c->stream));
     DRG_CUDA(cudaMemcpyAsync(offsets, off, (n + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
     launch_letter_owner(offsets, n, 0, total, owner, c->stream);
+    if (letters_above_24(c, letters, total)) {
+      DRG_CUDA(cudaMalloc(&score_letters, total + 64));
+      DRG_CUDA(cudaMemsetAsync(score_letters + total, 25, 64, c->stream));
+      launch_clamp_letters(letters, total, score_letters, c->stream);
+    }
   }
-  DevSeqs view() const { return DevSeqs{letters, offsets, &h_offsets}; }
+  DevSeqs view() const { return DevSeqs{letters, offsets, &h_offsets, score_letters}; }
 };
 
 template <typename T>

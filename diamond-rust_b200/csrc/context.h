@@ -33,7 +33,7 @@ struct drg_ctx {
   drg::DevBuf sw_tasks_u, task_key, task_key_s, task_val, task_val_s, best_row, band_jobs_u, band_jobs, sw_rows, sw_rows_s,
       sw_keys_r, sw_order_r;
   drg::DevBuf bj_key, bj_key_s, bj_val, bj_val_s, bj_size, bj_off, bj_max, ops_cnt, ops_coff, ops_compact, verdict,
-      tr_count;
+      tr_count, letter_check;
   // blastx front end
   drg::DevBuf x_nt, x_nt_off, x_len, x_scratch_off, x_scratch, x_keep, x_kept_len, x_kept_index, x_kept_off,
       x_query, x_frame;
@@ -46,6 +46,7 @@ struct drg_ctx {
 struct drg_db {
   drg_ctx* ctx = nullptr;
   uint8_t* letters = nullptr;   // device, 16 bytes of slack after the end
+  uint8_t* score_letters = nullptr;  // device: letters clamped to 24, only when some code is above 24
   uint64_t* offsets = nullptr;  // device, n + 1
   uint32_t* owner = nullptr;    // device: letter -> sequence
   std::vector<uint64_t> h_offsets;
@@ -57,6 +58,7 @@ struct drg_db {
 struct drg_batch {
   drg_ctx* ctx = nullptr;
   uint8_t* letters = nullptr;
+  uint8_t* score_letters = nullptr;  // device: letters clamped to 24, only when some code is above 24
   uint64_t* offsets = nullptr;
   uint32_t* owner = nullptr;
   uint32_t* request = nullptr;  // device: request of each target (null: one request)
@@ -75,6 +77,9 @@ struct DevSeqs {
   const uint8_t* letters;
   const uint64_t* offsets;
   const std::vector<uint64_t>* h_offsets;
+  const uint8_t* score_letters = nullptr;  // letters clamped to 24, when some code is above 24
+  // what the DP kernels read: they index residue profiles by the code
+  const uint8_t* dp_letters() const { return score_letters ? score_letters : letters; }
 };
 struct ExactOut;
 void run_bands(drg_ctx* c, const Band* bands, uint64_t n_bands, const DevSeqs& q, const DevSeqs& s,
@@ -83,6 +88,8 @@ void run_bands(drg_ctx* c, const Band* bands, uint64_t n_bands, const DevSeqs& q
                int64_t* d_count, unsigned long long* cells_gpu);
 // Whole-path search over resident inputs (pipeline.cu).
 void search(drg_ctx* ctx, const drg_db* db, const drg_batch* b, const drg_search_config* cfg, drg_result* out);
+// Whether n device letters hold a code above 24; syncs the context's stream.
+bool letters_above_24(drg_ctx* ctx, const uint8_t* d_letters, uint64_t n);
 // Device residency helpers.
 drg_db* make_db(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offsets, uint64_t n);
 drg_batch* make_batch(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offsets, const uint32_t* query,

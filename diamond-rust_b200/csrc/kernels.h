@@ -13,6 +13,10 @@ void upload_seed_params(const ShapeTable& shapes, const SeedParams& p, int slot,
 // seq index of every letter: out[g] = i with offsets[i] <= g < offsets[i+1].
 void launch_letter_owner(const uint64_t* offsets, uint64_t n_seqs, uint64_t letter_lo, uint64_t letter_hi,
                          uint32_t* out, cudaStream_t st);
+// *bad = 1 when a letter code of letters[0, n) is above 24 (0 otherwise).
+void launch_check_letters(const uint8_t* letters, uint64_t n, unsigned int* bad, cudaStream_t st);
+// out[i] = min(in[i], 24): the codes the score tables see.
+void launch_clamp_letters(const uint8_t* in, uint64_t n, uint8_t* out, cudaStream_t st);
 // Enumerate seeds of letters [letter_lo, letter_hi) for shapes [0, n_shapes):
 // keys[s * (letter_hi - letter_lo) + g - letter_lo] = request << request_shift |
 // s << shape_shift | key (shifts from the search's SeedParams), or ~0 when no

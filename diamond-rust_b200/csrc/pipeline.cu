@@ -486,9 +486,9 @@ SwBandArgs band_args(const Band* bc, const BandJobs& bj, const DevSeqs& qs, cons
   ba.jobs = bj.jobs;
   ba.lo = 0;
   ba.hi = bj.n;
-  ba.q_letters = qs.letters;
+  ba.q_letters = qs.dp_letters();
   ba.q_offsets = qs.offsets;
-  ba.s_letters = s.letters;
+  ba.s_letters = s.dp_letters();
   ba.s_offsets = s.offsets;
   ba.gap_open = scr.gap_open;
   ba.gap_extend = scr.gap_extend;
@@ -630,9 +630,9 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
     sa.bands = bc;
     sa.order = swos;
     sa.tasks = tasks;
-    sa.q_letters = qs.letters;
+    sa.q_letters = qs.dp_letters();
     sa.q_offsets = qs.offsets;
-    sa.s_letters = s.letters;
+    sa.s_letters = s.dp_letters();
     sa.s_offsets = s.offsets;
     sa.gap_open = scr.gap_open;
     sa.gap_extend = scr.gap_extend;
@@ -1031,8 +1031,8 @@ void Search::chunk(uint64_t chunk_id, uint64_t c0, uint64_t c1, uint64_t n_runs)
   // ---- banded SW scores
   tm.start();
   int32_t* scores = c->scores.as<int32_t>(n_bands);
-  DevSeqs qs{q->letters, q->offsets, &q->h_offsets};
-  DevSeqs ss{db->letters, db->offsets, &db->h_offsets};
+  DevSeqs qs{q->letters, q->offsets, &q->h_offsets, q->score_letters};
+  DevSeqs ss{db->letters, db->offsets, &db->h_offsets, db->score_letters};
   int32_t* best_row = c->best_row.as<int32_t>(n_bands);
   run_bands(c, bc, n_bands, qs, ss, sc, false, scores, best_row, nullptr, nullptr, nullptr, nullptr, st, d_count,
             d_counters + 3);
@@ -1198,8 +1198,8 @@ void Search::finish(drg_result* out) {
     uint32_t* dops = c->exact_ops.as<uint32_t>(ops_off[nj] + 1);
     DRG_CUDA(cudaMemcpyAsync(db_, sb.data(), nj * sizeof(Band), cudaMemcpyHostToDevice, c->stream));
     DRG_CUDA(cudaMemcpyAsync(doff, ops_off.data(), (nj + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
-    DevSeqs qs{q->letters, q->offsets, &q->h_offsets};
-    DevSeqs ss{db->letters, db->offsets, &db->h_offsets};
+    DevSeqs qs{q->letters, q->offsets, &q->h_offsets, q->score_letters};
+    DevSeqs ss{db->letters, db->offsets, &db->h_offsets, db->score_letters};
     run_bands(c, db_, nj, qs, ss, sc, true, nullptr, nullptr, dout, dops, doff, &ops_off, st, d_count,
               nullptr);
     // only the ops the alignments use come back (each band has n + m slots)
@@ -1333,6 +1333,24 @@ static void pool_free(drg_ctx* ctx, void* p) {
   if (p) cudaFreeAsync(p, ctx->stream);
 }
 
+bool letters_above_24(drg_ctx* c, const uint8_t* d_letters, uint64_t n) {
+  unsigned int* bad = c->letter_check.as<unsigned int>(1);
+  launch_check_letters(d_letters, n, bad, c->stream);
+  return fetch(c, bad) != 0;
+}
+
+// Letter codes above 24 score as 24 (matrix.rs:164-168) while identities
+// compare the codes themselves (hsp.rs:46-56): the DP kernels then read a
+// clamped copy, everything else the letters as given.
+template <typename Obj>
+static void clamp_for_dp(drg_ctx* ctx, Obj* o) {
+  if (!letters_above_24(ctx, o->letters, o->total)) return;
+  pool_alloc(ctx, &o->score_letters, o->total + 64);
+  DRG_CUDA(cudaMemsetAsync(o->score_letters + o->total, 25, 64, ctx->stream));
+  launch_clamp_letters(o->letters, o->total, o->score_letters, ctx->stream);
+  DRG_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
 drg_db* make_db(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offsets, uint64_t n) {
   drg_db* d = new drg_db();
   d->ctx = ctx;
@@ -1356,7 +1374,7 @@ drg_db* make_db(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offsets, u
       DRG_CUDA(cudaMemcpyAsync(d->letters, letters, d->total, cudaMemcpyHostToDevice, ctx->stream));
     DRG_CUDA(cudaMemcpyAsync(d->offsets, offsets, (n + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, ctx->stream));
     launch_letter_owner(d->offsets, n, 0, d->total, d->owner, ctx->stream);
-    DRG_CUDA(cudaStreamSynchronize(ctx->stream));
+    clamp_for_dp(ctx, d);
   } catch (...) {
     free_db(d);
     throw;
@@ -1398,7 +1416,7 @@ drg_batch* make_batch(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offs
       pool_alloc(ctx, &b->request, n * sizeof(uint32_t));
       DRG_CUDA(cudaMemcpyAsync(b->request, request, n * sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
     }
-    DRG_CUDA(cudaStreamSynchronize(ctx->stream));
+    clamp_for_dp(ctx, b);
   } catch (...) {
     free_batch(b);
     throw;
@@ -1484,6 +1502,7 @@ void free_db(drg_db* d) {
   if (!d) return;
   d->cache.reset();
   pool_free(d->ctx, d->letters);
+  pool_free(d->ctx, d->score_letters);
   pool_free(d->ctx, d->offsets);
   pool_free(d->ctx, d->owner);
   delete d;
@@ -1492,6 +1511,7 @@ void free_db(drg_db* d) {
 void free_batch(drg_batch* b) {
   if (!b) return;
   pool_free(b->ctx, b->letters);
+  pool_free(b->ctx, b->score_letters);
   pool_free(b->ctx, b->offsets);
   pool_free(b->ctx, b->owner);
   pool_free(b->ctx, b->request);

@@ -41,6 +41,43 @@ __global__ void k_letter_owner(const uint64_t* __restrict__ offsets, uint64_t n_
   out[g - lo] = (uint32_t)a;
 }
 
+// Letter codes above 24 score as 24 (matrix.rs:164-168 clamps both indices)
+// but would index past the packed kernels' 26-row residue profiles: any such
+// byte sets *bad, and the DP kernels then read a clamped copy.  Sixteen
+// letters per thread (the buffers are 256-byte aligned), four at a time.
+__global__ void k_check_letters(const uint8_t* __restrict__ letters, uint64_t n, unsigned int* __restrict__ bad) {
+  const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  bool b = false;
+  if (16 * t + 16 <= n) {
+    const uint4 w = reinterpret_cast<const uint4*>(letters)[t];
+    b = (__vcmpgtu4(w.x, 0x18181818u) | __vcmpgtu4(w.y, 0x18181818u) | __vcmpgtu4(w.z, 0x18181818u) |
+         __vcmpgtu4(w.w, 0x18181818u)) != 0;
+  } else {
+    for (uint64_t i = 16 * t; i < n; ++i) b |= letters[i] > 24;
+  }
+  if (__any_sync(0xFFFFFFFFu, b) && (threadIdx.x & 31) == 0) atomicOr(bad, 1u);
+}
+
+__global__ void k_clamp_letters(const uint8_t* __restrict__ in, uint64_t n, uint8_t* __restrict__ out) {
+  const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i < n) out[i] = in[i] < 24 ? in[i] : 24;
+}
+
+void launch_clamp_letters(const uint8_t* in, uint64_t n, uint8_t* out, cudaStream_t st) {
+  if (n == 0) return;
+  count_launch();
+  k_clamp_letters<<<ceil_div((long long)n, 256), 256, 0, st>>>(in, n, out);
+  DRG_CUDA(cudaGetLastError());
+}
+
+void launch_check_letters(const uint8_t* letters, uint64_t n, unsigned int* bad, cudaStream_t st) {
+  DRG_CUDA(cudaMemsetAsync(bad, 0, sizeof(unsigned int), st));
+  if (n == 0) return;
+  count_launch();
+  k_check_letters<<<ceil_div(ceil_div((long long)n, 16), 256), 256, 0, st>>>(letters, n, bad);
+  DRG_CUDA(cudaGetLastError());
+}
+
 void launch_letter_owner(const uint64_t* offsets, uint64_t n_seqs, uint64_t lo, uint64_t hi, uint32_t* out,
                          cudaStream_t st) {
   if (hi <= lo || n_seqs == 0) return;

@@ -97,3 +97,16 @@ def test_resident_search_equals_host_search(ctx):
     finally:
         b.close()
         db.close()
+
+
+def test_search_with_letter_codes_above_24(ctx, orc):
+    """Letter codes above 24 in the database and the queries: seeds skip them,
+    scores treat them as 24, identities compare them as they are."""
+    w = small(2, 20, 300, seed=9)
+    r = np.random.Generator(np.random.PCG64(9))
+    for seq in list(w.db) + list(w.queries):
+        mask = r.random(len(seq)) < 0.03
+        seq[mask] = r.choice(np.array([25, 31, 128, 255], np.uint8), size=int(mask.sum()))
+    got, exp, _, _ = run_both(ctx, orc, w, sensitivity="sensitive")
+    assert got == exp
+    assert sum(len(x) for x in exp) > 0

@@ -254,6 +254,30 @@ def test_packed_scores_other_matrices(ctx, orc, matrix):
     assert got == [exp[-1]]
 
 
+def test_letter_codes_above_24(ctx, orc):
+    """Codes above 24 score as 24 (matrix.rs:164-168 clamps both indices) but
+    count as identities only when equal (hsp.rs:46-56); the packed kernels
+    read a clamped copy of the letters, the walk the letters as given."""
+    r = rng(404)
+    queries, subjects, jobs = [], [], []
+    for k in range(60):
+        q = rand_seq(r, int(r.integers(40, 400)))
+        s = synth.mutate(r, q, 0.7) if k % 2 else rand_seq(r, int(r.integers(40, 400)))
+        for seq in (q, s):
+            mask = r.random(len(seq)) < 0.05
+            seq[mask] = r.choice(np.array([24, 25, 26, 30, 99, 200, 255], np.uint8), size=int(mask.sum()))
+        queries.append(q)
+        subjects.append(s)
+        half = int(r.choice([12, 30, 64, 100, 200]))
+        d = int(r.integers(-20, 20))
+        jobs.append((k, k, d - half, d + half))
+    got = ctx.extend_span(queries, subjects, jobs)
+    exp = oracle_spans(orc, queries, subjects, jobs)
+    assert got == exp
+    scores, _ = ctx.extend_span_scores(queries, subjects, jobs)
+    assert [int(x) for x in scores] == [e[0] if e else 0 for e in exp]
+
+
 def test_extend_span_edge_cases(ctx, orc):
     W = np.full(3100, 17, np.uint8)  # W/W scores 11: best 34100 does not fit 16 bits
     cases = [
