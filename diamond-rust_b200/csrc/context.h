@@ -63,7 +63,6 @@ struct drg_batch {
   uint32_t* owner = nullptr;
   uint32_t* request = nullptr;  // device: request of each target (null: one request)
   std::vector<uint64_t> h_offsets;
-  std::vector<uint8_t> h_letters;
   std::vector<uint32_t> query;
   std::vector<uint8_t> frame;
   uint64_t n = 0, total = 0;

@@ -1389,7 +1389,6 @@ drg_batch* make_batch(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offs
   b->n = n;
   b->h_offsets.assign(offsets, offsets + n + 1);
   b->total = offsets[n];
-  b->h_letters.assign(letters, letters + b->total);
   b->query.resize(n);
   b->frame.resize(n);
   for (uint64_t i = 0; i < n; ++i) {
