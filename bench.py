@@ -59,6 +59,7 @@ def parse():
     p.add_argument("--no-serve", action="store_true", help="skip the serving stream (profiling runs)")
     p.add_argument("--no-blastx", action="store_true", help="skip the blastx leg (profiling runs)")
     p.add_argument("--no-very-sensitive", action="store_true", help="skip the very-sensitive leg")
+    p.add_argument("--no-batching", action="store_true", help="skip the batched-vs-plain leg")
     p.add_argument("--blastx-reads", type=int, default=20000, help="reads in the blastx leg")
     p.add_argument("--serve-requests", type=int, default=100, help="requests in the serving stream")
     p.add_argument("--queries", type=int, default=None,
@@ -233,6 +234,55 @@ def serve_stream(w, device, n_requests):
                 srv.close()
             out[name + tag] = serve.latency_summary(finished, span)
     return out
+
+
+def batching_leg(ctx, n_queries=400, n_db=50000):
+    """Config-3 shaped, scaled (400 queries, lognormal mean 350, 20-2000 aa,
+    10 % with 1-20 planted homologs, against 50,000 sequences; --sensitive,
+    index chunks 4, the seed index resident).  plain: one search per query;
+    batched: one search of all queries, each its own request (per-request join
+    accounting), so that both give the same HSPs.  Wall time host to host."""
+    import numpy as np
+    import drgpu
+    from drgpu import synth
+    w = synth.workload(3, n_queries=n_queries, n_db=n_db, seed_offset=0)
+    dl, do = drgpu.concat(w.db)
+    db = drgpu.ResidentDb(ctx, dl, do, index_budget=16 << 30)
+    cfg = drgpu.make_config(sensitivity="sensitive", index_chunks=4)
+    tl, to = drgpu.concat(w.queries)
+
+    def batched():
+        b = drgpu.ResidentBatch(ctx, tl, to, request=np.arange(len(w.queries), dtype=np.uint32))
+        try:
+            return drgpu.search_resident(ctx, db, b, cfg)[0]
+        finally:
+            b.close()
+
+    def plain():
+        out = []
+        for q in w.queries:
+            ql, qo = drgpu.concat([q])
+            b = drgpu.ResidentBatch(ctx, ql, qo)
+            try:
+                out.append(drgpu.search_resident(ctx, db, b, cfg)[0][0])
+            finally:
+                b.close()
+        return out
+
+    batched()  # builds the index entries
+    t0 = time.perf_counter()
+    lb = batched()
+    tb = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    lp = plain()
+    tp = time.perf_counter() - t0
+    same = [[h.key()[1:] for h in x] for x in lb] == [[h.key()[1:] for h in x] for x in lp]
+    db.close()
+    return {"workload": f"{n_queries} queries (config-3 generator) x {n_db:,}-sequence DB ({int(do[-1]):,} aa), "
+                        "blastp --sensitive, index chunks 4, seed index resident",
+            "plain_queries_per_s": n_queries / tp, "batched_queries_per_s": n_queries / tb,
+            "batched_over_plain": tp / tb, "identical_hsps": same,
+            "hsps": sum(len(x) for x in lb)}
 
 
 def blastx_leg(ctx, steps, warmup, n_reads, cpu_sample, with_cpu):
@@ -457,6 +507,11 @@ def main():
     if not args.no_serve:
         serving = serve_stream(w, local, args.serve_requests)
 
+    # ---- batched vs plain (config-3 shaped, scaled) --------------------------
+    batching = None
+    if not args.no_batching:
+        batching = batching_leg(ctx)
+
     # ---- blastx (config-4 shaped, scaled) ------------------------------------
     blastx = None
     if not args.no_blastx:
@@ -515,6 +570,7 @@ def main():
             "very_sensitive": vs,
             "seed_stage": seed_stage,
             "blastx": blastx,
+            "batching": batching,
             "gpu_launches": int(launches),
             "cpu_baseline": cpu,
             "parity_sample": parity,
