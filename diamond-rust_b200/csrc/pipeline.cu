@@ -843,7 +843,18 @@ struct Search {
 
   void run(drg_result* out);
   void query_seeds(uint64_t* n_runs);
-  void chunk(uint64_t chunk_id, uint64_t c0, uint64_t c1, uint64_t n_runs);
+  // The join of index chunk [c0, c1): its hits are appended to acc.
+  void join_chunk(uint64_t c0, uint64_t c1, uint64_t n_runs);
+  // X-drop, bands, score pass and gate over the accumulated hits.
+  void process_hits(uint64_t pass_id);
+  // Hits of the chunks joined since the last process_hits (device, from the
+  // context's pool; grows keeping its contents).
+  uint64_t* acc = nullptr;
+  uint64_t acc_n = 0, acc_cap = 0;
+  void acc_reserve(uint64_t n);
+  ~Search() {
+    if (acc) cudaFreeAsync(acc, c->stream);
+  }
   void finish(drg_result* out);
 };
 
@@ -878,7 +889,23 @@ void Search::query_seeds(uint64_t* n_runs_out) {
   *n_runs_out = n_runs;
 }
 
-void Search::chunk(uint64_t chunk_id, uint64_t c0, uint64_t c1, uint64_t n_runs) {
+// Chunks are joined one by one (the join cap counts reference occurrences
+// per chunk, search.rs:127-131), but a subject lives in one chunk, so the
+// stages after the join treat every (target, subject) pair on its own: the
+// hits of all chunks go through them in one pass (up to a hit budget), which
+// saves a pass of fixed launch and sync costs per chunk.
+void Search::acc_reserve(uint64_t n) {
+  if (n <= acc_cap) return;
+  const uint64_t cap = std::max<uint64_t>(n, 2 * acc_cap);
+  uint64_t* p = nullptr;
+  DRG_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p), cap * sizeof(uint64_t), c->pool, c->stream));
+  if (acc_n) DRG_CUDA(cudaMemcpyAsync(p, acc, acc_n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, c->stream));
+  if (acc) DRG_CUDA(cudaFreeAsync(acc, c->stream));
+  acc = p;
+  acc_cap = cap;
+}
+
+void Search::join_chunk(uint64_t c0, uint64_t c1, uint64_t n_runs) {
   Timer tm(c);
   const int S = (int)shapes.size();
   const uint64_t lo = db->h_offsets[c0], hi = db->h_offsets[c1];
@@ -925,7 +952,8 @@ void Search::chunk(uint64_t chunk_id, uint64_t c0, uint64_t c1, uint64_t n_runs)
   const uint64_t n_hits = fetch(c, roff + n_runs);
   st.hits += n_hits;
   const HitKeyLayout L = layout();
-  uint64_t* hk = c->hits.as<uint64_t>(n_hits);
+  acc_reserve(acc_n + n_hits);
+  uint64_t* hk = acc + acc_n;
   if (n_hits > 0) {
     JoinExpandArgs ja{};
     ja.run_hit_off = roff;
@@ -944,8 +972,17 @@ void Search::chunk(uint64_t chunk_id, uint64_t c0, uint64_t c1, uint64_t n_runs)
     ja.hit_keys = hk;
     launch_join_expand(ja, c->stream);
   }
+  acc_n += n_hits;
   st.ms_join += tm.stop();
+}
+
+void Search::process_hits(uint64_t pass_id) {
+  Timer tm(c);
+  const uint64_t n_hits = acc_n;
+  acc_n = 0;
   if (n_hits == 0) return;
+  const HitKeyLayout L = layout();
+  const uint64_t* hk = acc;
   // ---- sort + unique hits
   tm.start();
   uint64_t* hs = c->hits_s.as<uint64_t>(n_hits);
@@ -1081,7 +1118,7 @@ void Search::chunk(uint64_t chunk_id, uint64_t c0, uint64_t c1, uint64_t n_runs)
       cd.band = hb[k];
       cd.score = hs_[k];
       cd.state = hst[k];
-      cd.pair_key = (chunk_id << 32) | hb[k].pair;
+      cd.pair_key = (pass_id << 32) | hb[k].pair;
       cd.evalue = 0;
       cd.bits = 0;
       cands.push_back(cd);
@@ -1291,8 +1328,13 @@ void Search::run(drg_result* out) {
   query_seeds(&n_runs);
   st.ms_seed = tm.stop();
   if (n_runs > 0) {
-    uint64_t cid = 0;
-    for (auto [c0, c1] : split_chunks(db->n, index_chunks)) chunk(cid++, c0, c1, n_runs);
+    constexpr uint64_t kHitPassBudget = 1ull << 28;  // hits held before the stages after the join run
+    uint64_t pass = 0;
+    for (auto [c0, c1] : split_chunks(db->n, index_chunks)) {
+      join_chunk(c0, c1, n_runs);
+      if (acc_n >= kHitPassBudget) process_hits(pass++);
+    }
+    process_hits(pass++);
   }
   finish(out);
   unsigned long long cnt[7];
