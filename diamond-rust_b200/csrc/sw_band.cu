@@ -1,8 +1,11 @@
-// Banded affine Smith-Waterman (gapped.rs:67-280) with one warp per band:
-// the traceback pass of the HSPs that survive the E-value gate, whose few,
-// long bands leave an inter-band warp nearly empty.
+// Banded affine Smith-Waterman (gapped.rs:67-280) with lanes of a warp on
+// one band: the wide bands of the score pass and the traceback pass of the
+// HSPs that survive the E-value gate, whose few, long bands leave an
+// inter-band warp nearly empty.  Two mappings: the block kernel (k_sw_band,
+// below) and rotating strips (k_sw_rot, further down), which the launcher
+// picks by width.
 //
-// Mapping (intra-band, systolic): lane l runs strip 32b + l of the band (16
+// Block kernel (intra-band, systolic): lane l runs strip 32b + l of the band (16
 // DP rows, the same s16x2 pair layout and column recurrence as the packed
 // inter-band kernel) in block b of 32 strips.  Strip k + 1 at relative column
 // c needs the (H, E) of strip k's last row at strip k's relative column c + 16,
@@ -15,8 +18,9 @@
 // lane at run time.
 //
 // Results (trace nibbles, score, first row-major maximum) equal the packed
-// inter-band kernel's and hence the reference's; the walk kernel reads the
-// nibbles with a unit lane stride.
+// inter-band kernel's and hence the reference's; in trace mode each band is
+// walked (sw_walk.cuh) right after its DP, through nibbles laid out with a
+// unit stride between column steps.
 #include "kernels.h"
 #include "sw_common.cuh"
 #include "sw_walk.cuh"
