@@ -10,6 +10,7 @@ SeedIndex::~SeedIndex() {
   cudaGetDevice(&cur);
   if (cur != device) cudaSetDevice(device);
   cudaFree(keys);
+  cudaFree(keys32);
   cudaFree(vals);
   if (cur != device) cudaSetDevice(cur);
 }
@@ -47,9 +48,10 @@ std::shared_ptr<SeedIndex> IndexCache::find(const std::string& key) {
   return nullptr;
 }
 
-std::shared_ptr<SeedIndex> IndexCache::insert(const std::string& key, const uint64_t* keys, const uint32_t* vals,
-                                              uint64_t n, cudaStream_t stream) {
-  const uint64_t bytes = n * (sizeof(uint64_t) + sizeof(uint32_t));
+std::shared_ptr<SeedIndex> IndexCache::insert(const std::string& key, const uint64_t* keys, const uint32_t* keys32,
+                                              const uint32_t* vals, uint64_t n, cudaStream_t stream) {
+  const uint64_t key_bytes = keys ? sizeof(uint64_t) : sizeof(uint32_t);
+  const uint64_t bytes = n * (key_bytes + sizeof(uint32_t));
   {
     std::lock_guard<std::mutex> g(mu_);
     if (bytes > budget_ || bytes == 0) return nullptr;
@@ -61,12 +63,13 @@ std::shared_ptr<SeedIndex> IndexCache::insert(const std::string& key, const uint
   e->device = device_;
   e->n = n;
   e->bytes = bytes;
-  if (cudaMalloc(&e->keys, n * sizeof(uint64_t)) != cudaSuccess ||
-      cudaMalloc(&e->vals, n * sizeof(uint32_t)) != cudaSuccess) {
+  void** kp = keys ? reinterpret_cast<void**>(&e->keys) : reinterpret_cast<void**>(&e->keys32);
+  if (cudaMalloc(kp, n * key_bytes) != cudaSuccess || cudaMalloc(&e->vals, n * sizeof(uint32_t)) != cudaSuccess) {
     cudaGetLastError();  // out of memory: the search goes on without caching
     return nullptr;
   }
-  DRG_CUDA(cudaMemcpyAsync(e->keys, keys, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, stream));
+  DRG_CUDA(cudaMemcpyAsync(*kp, keys ? static_cast<const void*>(keys) : static_cast<const void*>(keys32),
+                           n * key_bytes, cudaMemcpyDeviceToDevice, stream));
   DRG_CUDA(cudaMemcpyAsync(e->vals, vals, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream));
   DRG_CUDA(cudaStreamSynchronize(stream));  // other contexts read it from their own streams
   std::list<std::shared_ptr<SeedIndex>> dropped;  // released after the lock (declared first)

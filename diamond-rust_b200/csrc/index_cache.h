@@ -19,11 +19,13 @@
 namespace drg {
 
 // Sorted reference seeds of one index chunk under one seed configuration:
-// keys[0, n) ascending, vals the packed (sequence, position) entries.
+// keys[0, n) ascending (or keys32, when the seed key fits 32 bits), vals
+// their letter indices.
 struct SeedIndex {
   std::string key;
   int device = 0;
   uint64_t* keys = nullptr;
+  uint32_t* keys32 = nullptr;
   uint32_t* vals = nullptr;
   uint64_t n = 0;
   uint64_t bytes = 0;
@@ -42,9 +44,10 @@ class IndexCache {
   // The entry under `key`, most recently used from now on; null on a miss.
   std::shared_ptr<SeedIndex> find(const std::string& key);
   // Copies n sorted seeds (device arrays, ready once `stream` reaches this
-  // point) into a new entry; returns null when the budget cannot hold it.
-  std::shared_ptr<SeedIndex> insert(const std::string& key, const uint64_t* keys, const uint32_t* vals, uint64_t n,
-                                    cudaStream_t stream);
+  // point; 64-bit keys or 32-bit keys32, the other null) into a new entry;
+  // returns null when the budget cannot hold it.
+  std::shared_ptr<SeedIndex> insert(const std::string& key, const uint64_t* keys, const uint32_t* keys32,
+                                    const uint32_t* vals, uint64_t n, cudaStream_t stream);
   struct Stats {
     uint64_t entries, bytes, hits, misses, evictions;
   };

@@ -26,6 +26,10 @@ void launch_clamp_letters(const uint8_t* in, uint64_t n, uint8_t* out, cudaStrea
 void launch_seed_enum(const uint8_t* letters, const uint64_t* offsets, const uint32_t* owner, uint64_t letter_lo,
                       uint64_t letter_hi, int n_shapes, uint64_t* keys, uint32_t* vals, int slot, cudaStream_t st,
                       const uint32_t* request = nullptr);
+// The same with 32-bit keys, for a seed key of at most 32 bits and no
+// request; "no seed" is 0xFFFFFFFF.
+void launch_seed_enum(const uint8_t* letters, const uint64_t* offsets, const uint32_t* owner, uint64_t letter_lo,
+                      uint64_t letter_hi, int n_shapes, uint32_t* keys, uint32_t* vals, int slot, cudaStream_t st);
 constexpr uint64_t kNoSeed = ~0ull;
 constexpr uint32_t kMaxRequests = 65535;  // request ids of one batch
 
@@ -34,6 +38,9 @@ constexpr uint32_t kMaxRequests = 65535;  // request ids of one batch
 // under the expansion cap.
 void launch_join_count(const uint64_t* run_keys, const uint32_t* run_counts, uint64_t n_runs,
                        const uint64_t* ref_keys, uint64_t n_ref, uint64_t max_expand, uint32_t* run_rlo,
+                       uint32_t* run_rcount, uint64_t* run_hits, uint64_t key_mask, cudaStream_t st);
+void launch_join_count(const uint64_t* run_keys, const uint32_t* run_counts, uint64_t n_runs,
+                       const uint32_t* ref_keys, uint64_t n_ref, uint64_t max_expand, uint32_t* run_rlo,
                        uint32_t* run_rcount, uint64_t* run_hits, uint64_t key_mask, cudaStream_t st);
 
 // Layout of the packed 64-bit hit key (target, subject, diag + doff, spos).

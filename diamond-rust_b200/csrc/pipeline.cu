@@ -84,21 +84,23 @@ struct Timer {
   }
 };
 
-__global__ void k_count_valid(const uint64_t* keys, uint64_t n, int64_t* out) {
-  // number of keys before the first kNoSeed (keys sorted ascending)
+template <typename K>
+__global__ void k_count_valid(const K* keys, uint64_t n, int64_t* out) {
+  // number of keys before the first "no seed" (all ones; keys sorted ascending)
   uint64_t lo = 0, hi = n;
   while (lo < hi) {
     uint64_t m = (lo + hi) >> 1;
-    if (keys[m] < kNoSeed) lo = m + 1;
+    if (keys[m] < (K)kNoSeed) lo = m + 1;
     else hi = m;
   }
   *out = (int64_t)lo;
 }
 
-int64_t count_valid(drg_ctx* c, const uint64_t* keys, uint64_t n, int64_t* d_tmp) {
+template <typename K>
+int64_t count_valid(drg_ctx* c, const K* keys, uint64_t n, int64_t* d_tmp) {
   if (n == 0) return 0;
   count_launch();
-  k_count_valid<<<1, 1, 0, c->stream>>>(keys, n, d_tmp);
+  k_count_valid<K><<<1, 1, 0, c->stream>>>(keys, n, d_tmp);
   DRG_CUDA(cudaGetLastError());
   return fetch(c, d_tmp);
 }
@@ -915,35 +917,55 @@ void Search::join_chunk(uint64_t c0, uint64_t c1, uint64_t n_runs) {
   IndexCache* cache = db->cache && db->cache->budget() > 0 ? db->cache.get() : nullptr;
   const std::string ikey = cache ? index_key(c0, c1) : std::string();
   std::shared_ptr<SeedIndex> held = cache ? cache->find(ikey) : nullptr;  // kept until the join has read it
-  const uint64_t* keys_s;
+  // A seed key of at most 32 bits is sorted as a 32-bit key: 8 bytes per
+  // entry and pass instead of 12.
+  const bool key32 = seed_key_bits <= 32;
+  const uint64_t* keys_s = nullptr;
+  const uint32_t* keys32_s = nullptr;
   const uint32_t* vals_s;
   int64_t nr;
   if (held) {
     keys_s = held->keys;
+    keys32_s = held->keys32;
     vals_s = held->vals;
     nr = (int64_t)held->n;
     st.index_hits += 1;
   } else {
-    uint64_t* keys = c->r_keys.as<uint64_t>(N);
     uint32_t* vals = c->r_vals.as<uint32_t>(N);
-    uint64_t* ks = c->r_keys_s.as<uint64_t>(N);
     uint32_t* vs = c->r_vals_s.as<uint32_t>(N);
-    launch_seed_enum(db->letters, db->offsets, db->owner + lo, lo, hi, S, keys, vals, c->slot, c->stream);
-    cub_call(c, [&](void* t, size_t& b) {
-      return cub::DeviceRadixSort::SortPairs(t, b, keys, ks, vals, vs, (int64_t)N, 0, seed_key_bits, c->stream);
-    });
-    nr = count_valid(c, ks, N, d_count);
-    keys_s = ks;
+    if (key32) {
+      uint32_t* keys = c->r_keys.as<uint32_t>(N);
+      uint32_t* ks = c->r_keys_s.as<uint32_t>(N);
+      launch_seed_enum(db->letters, db->offsets, db->owner + lo, lo, hi, S, keys, vals, c->slot, c->stream);
+      cub_call(c, [&](void* t, size_t& b) {
+        return cub::DeviceRadixSort::SortPairs(t, b, keys, ks, vals, vs, (int64_t)N, 0, seed_key_bits, c->stream);
+      });
+      nr = count_valid(c, ks, N, d_count);
+      keys32_s = ks;
+    } else {
+      uint64_t* keys = c->r_keys.as<uint64_t>(N);
+      uint64_t* ks = c->r_keys_s.as<uint64_t>(N);
+      launch_seed_enum(db->letters, db->offsets, db->owner + lo, lo, hi, S, keys, vals, c->slot, c->stream);
+      cub_call(c, [&](void* t, size_t& b) {
+        return cub::DeviceRadixSort::SortPairs(t, b, keys, ks, vals, vs, (int64_t)N, 0, seed_key_bits, c->stream);
+      });
+      nr = count_valid(c, ks, N, d_count);
+      keys_s = ks;
+    }
     vals_s = vs;
-    if (cache) held = cache->insert(ikey, ks, vs, (uint64_t)nr, c->stream);
+    if (cache) held = cache->insert(ikey, keys_s, keys32_s, vs, (uint64_t)nr, c->stream);
   }
   st.ref_seeds += (uint64_t)nr;
   uint32_t* rlo = c->run_rlo.as<uint32_t>(n_runs + 1);
   uint32_t* rcnt = c->run_rcount.as<uint32_t>(n_runs + 1);
   uint64_t* rhits = c->run_hits.as<uint64_t>(n_runs + 1);
   uint64_t* roff = c->run_hit_off.as<uint64_t>(n_runs + 1);
-  launch_join_count(c->run_keys.as<uint64_t>(0), c->run_counts.as<uint32_t>(0), n_runs, keys_s, (uint64_t)nr, 4096,
-                    rlo, rcnt, rhits, (1ull << seed_key_bits) - 1, c->stream);
+  if (keys32_s)
+    launch_join_count(c->run_keys.as<uint64_t>(0), c->run_counts.as<uint32_t>(0), n_runs, keys32_s, (uint64_t)nr,
+                      4096, rlo, rcnt, rhits, (1ull << seed_key_bits) - 1, c->stream);
+  else
+    launch_join_count(c->run_keys.as<uint64_t>(0), c->run_counts.as<uint32_t>(0), n_runs, keys_s, (uint64_t)nr, 4096,
+                      rlo, rcnt, rhits, (1ull << seed_key_bits) - 1, c->stream);
   count_launch();
   k_set_u64<<<1, 1, 0, c->stream>>>(rhits + n_runs, 0);
   cub_call(c, [&](void* t, size_t& b) {

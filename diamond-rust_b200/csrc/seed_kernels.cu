@@ -124,9 +124,12 @@ __device__ __forceinline__ bool seed_at(const uint8_t* __restrict__ p, int s, in
   return true;
 }
 
+// K = uint32_t: the caller guarantees that the seed key (with the request,
+// if any) fits 32 bits; "no seed" is then 0xFFFFFFFF.
+template <typename K>
 __global__ void k_seed_enum(const uint8_t* __restrict__ letters, const uint64_t* __restrict__ offsets,
                             const uint32_t* __restrict__ owner, uint64_t lo, uint64_t hi, int n_shapes,
-                            uint64_t* __restrict__ keys, uint32_t* __restrict__ vals,
+                            K* __restrict__ keys, uint32_t* __restrict__ vals,
                             const uint32_t* __restrict__ request, int slot) {
   __shared__ uint8_t bucket[32];
   __shared__ double lnfact[33];
@@ -144,7 +147,7 @@ __global__ void k_seed_enum(const uint8_t* __restrict__ letters, const uint64_t*
   for (int s = 0; s < n_shapes; ++s) {
     uint64_t key = 0;
     const bool ok = g + c_shapes[slot].span[s] <= end && seed_at(letters + g, s, slot, bucket, lnfact, &key);
-    keys[s * L + i] = ok ? req | ((uint64_t)s << sp.shape_shift) | key : kNoSeed;
+    keys[s * L + i] = ok ? (K)(req | ((uint64_t)s << sp.shape_shift) | key) : (K)kNoSeed;
     vals[s * L + i] = (uint32_t)g;
   }
 }
@@ -154,13 +157,23 @@ void launch_seed_enum(const uint8_t* letters, const uint64_t* offsets, const uin
                       const uint32_t* request) {
   if (hi <= lo || n_shapes == 0) return;
   count_launch();
-  k_seed_enum<<<ceil_div(hi - lo, 256), 256, 0, st>>>(letters, offsets, owner, lo, hi, n_shapes, keys, vals, request,
-                                                     slot);
+  k_seed_enum<uint64_t><<<ceil_div(hi - lo, 256), 256, 0, st>>>(letters, offsets, owner, lo, hi, n_shapes, keys,
+                                                               vals, request, slot);
   DRG_CUDA(cudaGetLastError());
 }
 
+void launch_seed_enum(const uint8_t* letters, const uint64_t* offsets, const uint32_t* owner, uint64_t lo,
+                      uint64_t hi, int n_shapes, uint32_t* keys, uint32_t* vals, int slot, cudaStream_t st) {
+  if (hi <= lo || n_shapes == 0) return;
+  count_launch();
+  k_seed_enum<uint32_t><<<ceil_div(hi - lo, 256), 256, 0, st>>>(letters, offsets, owner, lo, hi, n_shapes, keys,
+                                                               vals, nullptr, slot);
+  DRG_CUDA(cudaGetLastError());
+}
+
+template <typename K>
 __global__ void k_join_count(const uint64_t* __restrict__ run_keys, const uint32_t* __restrict__ run_counts,
-                             uint64_t n_runs, const uint64_t* __restrict__ ref_keys, uint64_t n_ref,
+                             uint64_t n_runs, const K* __restrict__ ref_keys, uint64_t n_ref,
                              uint64_t max_expand, uint32_t* __restrict__ run_rlo, uint32_t* __restrict__ run_rcount,
                              uint64_t* __restrict__ run_hits, uint64_t key_mask) {
   uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
@@ -169,14 +182,14 @@ __global__ void k_join_count(const uint64_t* __restrict__ run_keys, const uint32
   uint64_t a = 0, b = n_ref;
   while (a < b) {  // lower bound
     uint64_t m = (a + b) >> 1;
-    if (ref_keys[m] < key) a = m + 1;
+    if ((uint64_t)ref_keys[m] < key) a = m + 1;
     else b = m;
   }
   uint64_t lo = a;
   b = n_ref;
   while (a < b) {  // upper bound
     uint64_t m = (a + b) >> 1;
-    if (ref_keys[m] <= key) a = m + 1;
+    if ((uint64_t)ref_keys[m] <= key) a = m + 1;
     else b = m;
   }
   uint64_t rc = a - lo;
@@ -186,14 +199,27 @@ __global__ void k_join_count(const uint64_t* __restrict__ run_keys, const uint32
   run_hits[u] = (rc > 0 && qc * rc <= max_expand) ? qc * rc : 0;
 }
 
+template <typename K>
+void join_count(const uint64_t* run_keys, const uint32_t* run_counts, uint64_t n_runs, const K* ref_keys,
+                uint64_t n_ref, uint64_t max_expand, uint32_t* run_rlo, uint32_t* run_rcount, uint64_t* run_hits,
+                uint64_t key_mask, cudaStream_t st) {
+  if (n_runs == 0) return;
+  count_launch();
+  k_join_count<K><<<ceil_div(n_runs, 256), 256, 0, st>>>(run_keys, run_counts, n_runs, ref_keys, n_ref, max_expand,
+                                                         run_rlo, run_rcount, run_hits, key_mask);
+  DRG_CUDA(cudaGetLastError());
+}
+
 void launch_join_count(const uint64_t* run_keys, const uint32_t* run_counts, uint64_t n_runs,
                        const uint64_t* ref_keys, uint64_t n_ref, uint64_t max_expand, uint32_t* run_rlo,
                        uint32_t* run_rcount, uint64_t* run_hits, uint64_t key_mask, cudaStream_t st) {
-  if (n_runs == 0) return;
-  count_launch();
-  k_join_count<<<ceil_div(n_runs, 256), 256, 0, st>>>(run_keys, run_counts, n_runs, ref_keys, n_ref, max_expand,
-                                                      run_rlo, run_rcount, run_hits, key_mask);
-  DRG_CUDA(cudaGetLastError());
+  join_count(run_keys, run_counts, n_runs, ref_keys, n_ref, max_expand, run_rlo, run_rcount, run_hits, key_mask, st);
+}
+
+void launch_join_count(const uint64_t* run_keys, const uint32_t* run_counts, uint64_t n_runs,
+                       const uint32_t* ref_keys, uint64_t n_ref, uint64_t max_expand, uint32_t* run_rlo,
+                       uint32_t* run_rcount, uint64_t* run_hits, uint64_t key_mask, cudaStream_t st) {
+  join_count(run_keys, run_counts, n_runs, ref_keys, n_ref, max_expand, run_rlo, run_rcount, run_hits, key_mask, st);
 }
 
 __global__ void k_join_expand(JoinExpandArgs a) {

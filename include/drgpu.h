@@ -202,7 +202,8 @@ void drg_db_destroy(drg_db* db);  /* before the db's context is destroyed */
  * sorts the reference seeds of every index chunk it covers, as the reference
  * does on every run (search.rs:104-126).  With a budget > 0 the sorted seeds of
  * each (shape set, reduction, complexity cut, index chunk) stay in device
- * memory (12 bytes per seed) for later searches from any context, the least
+ * memory (8 bytes per seed when the seed key fits 32 bits, else 12) for later
+ * searches from any context, the least
  * recently used leaving first when the held bytes pass the budget.  Results
  * are the same with or without it.  0 (the default) holds nothing and frees
  * what is held. */
