@@ -30,6 +30,22 @@ void launch_seed_enum(const uint8_t* letters, const uint64_t* offsets, const uin
 // request; "no seed" is 0xFFFFFFFF.
 void launch_seed_enum(const uint8_t* letters, const uint64_t* offsets, const uint32_t* owner, uint64_t letter_lo,
                       uint64_t letter_hi, int n_shapes, uint32_t* keys, uint32_t* vals, int slot, cudaStream_t st);
+// Bitmap of the query's seed keys for the filtered enumeration: bit
+// hash(run_keys[u] & key_mask) of 2^log2_bits is set (filter zeroed first).
+void launch_key_filter(const uint64_t* run_keys, uint64_t n, uint64_t key_mask, uint32_t* filter, int log2_bits,
+                       cudaStream_t st);
+// Reference seeds of letters [letter_lo, letter_hi) whose key's bit is set
+// in the filter, appended in no fixed order: counts[0] += kept, counts[1] +=
+// valid seeds (kept or not).  keys / vals need room for every seed of the
+// range; 32-bit keys for a seed key of at most 32 bits.
+void launch_seed_enum_filtered(const uint8_t* letters, const uint64_t* offsets, const uint32_t* owner,
+                               uint64_t letter_lo, uint64_t letter_hi, int n_shapes, const uint32_t* filter,
+                               int log2_bits, uint64_t* keys, uint32_t* vals, unsigned long long* counts, int slot,
+                               cudaStream_t st);
+void launch_seed_enum_filtered(const uint8_t* letters, const uint64_t* offsets, const uint32_t* owner,
+                               uint64_t letter_lo, uint64_t letter_hi, int n_shapes, const uint32_t* filter,
+                               int log2_bits, uint32_t* keys, uint32_t* vals, unsigned long long* counts, int slot,
+                               cudaStream_t st);
 constexpr uint64_t kNoSeed = ~0ull;
 constexpr uint32_t kMaxRequests = 65535;  // request ids of one batch
 

@@ -847,6 +847,10 @@ struct Search {
   void query_seeds(uint64_t* n_runs);
   // The join of index chunk [c0, c1): its hits are appended to acc.
   void join_chunk(uint64_t c0, uint64_t c1, uint64_t n_runs);
+  // bitmap of the query's seed keys (built on the first chunk that needs it)
+  uint32_t* key_filter = nullptr;
+  int key_filter_log2 = 0;
+  void build_key_filter(uint64_t n_runs);
   // X-drop, bands, score pass and gate over the accumulated hits.
   void process_hits(uint64_t pass_id);
   // Hits of the chunks joined since the last process_hits (device, from the
@@ -907,6 +911,19 @@ void Search::acc_reserve(uint64_t n) {
   acc_cap = cap;
 }
 
+// At least 32 bits per query run up to 2^29 bits (64 MB): then at most 3.1 %
+// of the keys that no query holds pass, and the bitmap stays resident in L2
+// while the reference seeds probe it.
+void Search::build_key_filter(uint64_t n_runs) {
+  int lg = 20;
+  while (lg < 29 && (1ull << lg) < 32 * n_runs) ++lg;
+  const uint64_t words = (1ull << lg) / 32;
+  key_filter = c->seed_filter.as<uint32_t>(words);
+  DRG_CUDA(cudaMemsetAsync(key_filter, 0, words * sizeof(uint32_t), c->stream));
+  launch_key_filter(c->run_keys.as<uint64_t>(0), n_runs, (1ull << seed_key_bits) - 1, key_filter, lg, c->stream);
+  key_filter_log2 = lg;
+}
+
 void Search::join_chunk(uint64_t c0, uint64_t c1, uint64_t n_runs) {
   Timer tm(c);
   const int S = (int)shapes.size();
@@ -923,13 +940,54 @@ void Search::join_chunk(uint64_t c0, uint64_t c1, uint64_t n_runs) {
   const uint64_t* keys_s = nullptr;
   const uint32_t* keys32_s = nullptr;
   const uint32_t* vals_s;
-  int64_t nr;
+  int64_t nr;             // reference seeds the join reads
+  uint64_t n_valid = 0;   // valid reference seeds of the chunk
   if (held) {
     keys_s = held->keys;
     keys32_s = held->keys32;
     vals_s = held->vals;
     nr = (int64_t)held->n;
+    n_valid = held->n;
     st.index_hits += 1;
+  } else if (!cache) {
+    // Nothing is kept for later searches, so only the seeds whose key the
+    // query holds are sorted: the join pairs equal keys only (seed.rs:110-140),
+    // so the rest cannot yield a hit or change a run's count.
+    if (!key_filter) build_key_filter(n_runs);
+    unsigned long long* cnt = c->seed_counts.as<unsigned long long>(2);
+    DRG_CUDA(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned long long), c->stream));
+    uint32_t* vals = c->r_vals.as<uint32_t>(N);
+    uint32_t* vs = c->r_vals_s.as<uint32_t>(N);
+    uint32_t *k32 = nullptr, *ks32 = nullptr;
+    uint64_t *k64 = nullptr, *ks64 = nullptr;
+    if (key32) {
+      k32 = c->r_keys.as<uint32_t>(N);
+      ks32 = c->r_keys_s.as<uint32_t>(N);
+      launch_seed_enum_filtered(db->letters, db->offsets, db->owner + lo, lo, hi, S, key_filter, key_filter_log2, k32,
+                                vals, cnt, c->slot, c->stream);
+    } else {
+      k64 = c->r_keys.as<uint64_t>(N);
+      ks64 = c->r_keys_s.as<uint64_t>(N);
+      launch_seed_enum_filtered(db->letters, db->offsets, db->owner + lo, lo, hi, S, key_filter, key_filter_log2, k64,
+                                vals, cnt, c->slot, c->stream);
+    }
+    std::vector<unsigned long long> h;
+    fetch_n(c, h, cnt, 2);
+    nr = (int64_t)h[0];
+    n_valid = h[1];
+    if (nr > 0) {
+      if (key32)
+        cub_call(c, [&](void* t, size_t& b) {
+          return cub::DeviceRadixSort::SortPairs(t, b, k32, ks32, vals, vs, nr, 0, seed_key_bits, c->stream);
+        });
+      else
+        cub_call(c, [&](void* t, size_t& b) {
+          return cub::DeviceRadixSort::SortPairs(t, b, k64, ks64, vals, vs, nr, 0, seed_key_bits, c->stream);
+        });
+    }
+    keys_s = ks64;
+    keys32_s = ks32;
+    vals_s = vs;
   } else {
     uint32_t* vals = c->r_vals.as<uint32_t>(N);
     uint32_t* vs = c->r_vals_s.as<uint32_t>(N);
@@ -953,9 +1011,10 @@ void Search::join_chunk(uint64_t c0, uint64_t c1, uint64_t n_runs) {
       keys_s = ks;
     }
     vals_s = vs;
-    if (cache) held = cache->insert(ikey, keys_s, keys32_s, vs, (uint64_t)nr, c->stream);
+    n_valid = (uint64_t)nr;
+    held = cache->insert(ikey, keys_s, keys32_s, vs, (uint64_t)nr, c->stream);
   }
-  st.ref_seeds += (uint64_t)nr;
+  st.ref_seeds += n_valid;
   uint32_t* rlo = c->run_rlo.as<uint32_t>(n_runs + 1);
   uint32_t* rcnt = c->run_rcount.as<uint32_t>(n_runs + 1);
   uint64_t* rhits = c->run_hits.as<uint64_t>(n_runs + 1);

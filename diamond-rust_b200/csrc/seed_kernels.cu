@@ -171,6 +171,123 @@ void launch_seed_enum(const uint8_t* letters, const uint64_t* offsets, const uin
   DRG_CUDA(cudaGetLastError());
 }
 
+// ---- reference seeds restricted to the query's seed keys --------------------
+// A reference seed joins only query seeds with the same key, so a chunk's
+// enumeration can keep just the seeds whose key has its bit set in a bitmap
+// of the query keys.  The bitmap is hashed: a false positive only keeps a
+// seed that then matches no query run, and no key of the query is missed.
+
+__device__ __forceinline__ uint32_t seed_key_hash(uint64_t k, int log2_bits) {
+  return (uint32_t)((k * 0x9E3779B97F4A7C15ull) >> (64 - log2_bits));  // Fibonacci hashing
+}
+
+__global__ void k_key_filter(const uint64_t* __restrict__ run_keys, uint64_t n, uint64_t key_mask,
+                             uint32_t* __restrict__ filter, int log2_bits) {
+  const uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (u >= n) return;
+  const uint32_t h = seed_key_hash(run_keys[u] & key_mask, log2_bits);
+  const uint32_t bit = 1u << (h & 31);
+  if (!(filter[h >> 5] & bit)) atomicOr(filter + (h >> 5), bit);
+}
+
+void launch_key_filter(const uint64_t* run_keys, uint64_t n, uint64_t key_mask, uint32_t* filter, int log2_bits,
+                       cudaStream_t st) {
+  if (n == 0) return;
+  count_launch();
+  k_key_filter<<<ceil_div(n, 256), 256, 0, st>>>(run_keys, n, key_mask, filter, log2_bits);
+  DRG_CUDA(cudaGetLastError());
+}
+
+// One thread per letter as in k_seed_enum.  Kept seeds collect in shared
+// memory, kFilterGroup shapes at a time, and each block reserves its output
+// range with one atomic per group; counts[0] = seeds kept, counts[1] = valid
+// seeds (kept or not).  The output order depends on the blocks' timing; the
+// caller sorts by key, and the hits made from them are sorted in full later.
+constexpr int kFilterBlock = 256, kFilterGroup = 8;
+
+template <typename K>
+__global__ void __launch_bounds__(kFilterBlock)
+    k_seed_enum_filtered(const uint8_t* __restrict__ letters, const uint64_t* __restrict__ offsets,
+                         const uint32_t* __restrict__ owner, uint64_t lo, uint64_t hi, int n_shapes,
+                         const uint32_t* __restrict__ filter, int log2_bits, K* __restrict__ keys,
+                         uint32_t* __restrict__ vals, unsigned long long* __restrict__ counts, int slot) {
+  __shared__ uint8_t bucket[32];
+  __shared__ double lnfact[33];
+  __shared__ K s_keys[kFilterBlock * kFilterGroup];
+  __shared__ uint32_t s_vals[kFilterBlock * kFilterGroup];
+  __shared__ uint32_t s_n;
+  __shared__ unsigned long long s_base, s_valid;
+  if (threadIdx.x < 32) bucket[threadIdx.x] = c_seed[slot].bucket[threadIdx.x];
+  if (threadIdx.x < 33) lnfact[threadIdx.x] = c_seed[slot].lnfact[threadIdx.x];
+  if (threadIdx.x == 0) {
+    s_n = 0;
+    s_valid = 0;
+  }
+  __syncthreads();
+  const uint64_t L = hi - lo;
+  const uint64_t i = blockIdx.x * (uint64_t)kFilterBlock + threadIdx.x;
+  const bool in = i < L;
+  const uint64_t g = lo + i;
+  const uint64_t end = in ? offsets[owner[i] + 1] : 0;
+  const SeedParams& sp = c_seed[slot];
+  unsigned long long valid = 0;
+  for (int s0 = 0; s0 < n_shapes; s0 += kFilterGroup) {
+    const int s1 = min(n_shapes, s0 + kFilterGroup);
+    for (int s = s0; s < s1; ++s) {
+      uint64_t key = 0;
+      if (in && g + c_shapes[slot].span[s] <= end && seed_at(letters + g, s, slot, bucket, lnfact, &key)) {
+        ++valid;
+        const uint64_t k = ((uint64_t)s << sp.shape_shift) | key;
+        const uint32_t h = seed_key_hash(k, log2_bits);
+        if (__ldg(filter + (h >> 5)) & (1u << (h & 31))) {
+          const uint32_t e = atomicAdd(&s_n, 1u);
+          s_keys[e] = (K)k;
+          s_vals[e] = (uint32_t)g;
+        }
+      }
+    }
+    __syncthreads();
+    const uint32_t n = s_n;
+    if (threadIdx.x == 0 && n > 0) s_base = atomicAdd(counts, (unsigned long long)n);
+    __syncthreads();  // every thread has read s_n and can see s_base
+    const unsigned long long base = s_base;
+    if (threadIdx.x == 0) s_n = 0;
+    for (uint32_t e = threadIdx.x; e < n; e += kFilterBlock) {
+      keys[base + e] = s_keys[e];
+      vals[base + e] = s_vals[e];
+    }
+    __syncthreads();  // the buffer is free for the next group
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) valid += __shfl_xor_sync(0xFFFFFFFFu, valid, o);
+  if ((threadIdx.x & 31) == 0 && valid) atomicAdd(&s_valid, valid);
+  __syncthreads();
+  if (threadIdx.x == 0 && s_valid) atomicAdd(counts + 1, s_valid);
+}
+
+template <typename K>
+void seed_enum_filtered(const uint8_t* letters, const uint64_t* offsets, const uint32_t* owner, uint64_t lo,
+                        uint64_t hi, int n_shapes, const uint32_t* filter, int log2_bits, K* keys, uint32_t* vals,
+                        unsigned long long* counts, int slot, cudaStream_t st) {
+  if (hi <= lo || n_shapes == 0) return;
+  count_launch();
+  k_seed_enum_filtered<K><<<ceil_div(hi - lo, kFilterBlock), kFilterBlock, 0, st>>>(
+      letters, offsets, owner, lo, hi, n_shapes, filter, log2_bits, keys, vals, counts, slot);
+  DRG_CUDA(cudaGetLastError());
+}
+
+void launch_seed_enum_filtered(const uint8_t* letters, const uint64_t* offsets, const uint32_t* owner, uint64_t lo,
+                               uint64_t hi, int n_shapes, const uint32_t* filter, int log2_bits, uint64_t* keys,
+                               uint32_t* vals, unsigned long long* counts, int slot, cudaStream_t st) {
+  seed_enum_filtered(letters, offsets, owner, lo, hi, n_shapes, filter, log2_bits, keys, vals, counts, slot, st);
+}
+
+void launch_seed_enum_filtered(const uint8_t* letters, const uint64_t* offsets, const uint32_t* owner, uint64_t lo,
+                               uint64_t hi, int n_shapes, const uint32_t* filter, int log2_bits, uint32_t* keys,
+                               uint32_t* vals, unsigned long long* counts, int slot, cudaStream_t st) {
+  seed_enum_filtered(letters, offsets, owner, lo, hi, n_shapes, filter, log2_bits, keys, vals, counts, slot, st);
+}
+
 template <typename K>
 __global__ void k_join_count(const uint64_t* __restrict__ run_keys, const uint32_t* __restrict__ run_counts,
                              uint64_t n_runs, const K* __restrict__ ref_keys, uint64_t n_ref,
