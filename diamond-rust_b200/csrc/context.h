@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <functional>
 #include <memory>
 #include <string>
 #include <vector>
@@ -80,11 +81,56 @@ struct DevSeqs {
   // what the DP kernels read: they index residue profiles by the code
   const uint8_t* dp_letters() const { return score_letters ? score_letters : letters; }
 };
+// Stage times of a search without draining the stream: spans between
+// recorded events, read once the work has been waited for (resolve()).
+class TimeLog {
+ public:
+  TimeLog() = default;
+  TimeLog(const TimeLog&) = delete;
+  TimeLog& operator=(const TimeLog&) = delete;
+  ~TimeLog() {
+    for (cudaEvent_t e : events_) cudaEventDestroy(e);
+  }
+  // A new event owned by the log (the caller records it).
+  cudaEvent_t event() {
+    cudaEvent_t e;
+    DRG_CUDA(cudaEventCreate(&e));
+    events_.push_back(e);
+    return e;
+  }
+  // *dst += milliseconds from a to b, at resolve().
+  void span(cudaEvent_t a, cudaEvent_t b, double* dst) { spans_.push_back({a, b, dst}); }
+  // f runs at resolve(), after the spans.
+  void later(std::function<void()> f) { jobs_.push_back(std::move(f)); }
+  // Every event recorded so far must have completed.
+  void resolve() {
+    for (const Span& s : spans_) {
+      float ms = 0;
+      DRG_CUDA(cudaEventElapsedTime(&ms, s.a, s.b));
+      *s.dst += ms;
+    }
+    for (auto& f : jobs_) f();
+    spans_.clear();
+    jobs_.clear();
+  }
+
+ private:
+  struct Span {
+    cudaEvent_t a, b;
+    double* dst;
+  };
+  std::vector<cudaEvent_t> events_;
+  std::vector<Span> spans_;
+  std::vector<std::function<void()>> jobs_;
+};
+
 struct ExactOut;
+// With a TimeLog the kernel times go into it; without one they are read
+// before returning (which waits for the launches).
 void run_bands(drg_ctx* c, const Band* bands, uint64_t n_bands, const DevSeqs& q, const DevSeqs& s,
                const Scoring& sc, bool trace, int32_t* scores, int32_t* best_row, ExactOut* out, uint32_t* ops,
                const uint64_t* d_ops_off, const std::vector<uint64_t>* h_ops_off, drg_run_stats& st,
-               int64_t* d_count, unsigned long long* cells_gpu);
+               int64_t* d_count, unsigned long long* cells_gpu, TimeLog* times = nullptr);
 // Whole-path search over resident inputs (pipeline.cu).
 void search(drg_ctx* ctx, const drg_db* db, const drg_batch* b, const drg_search_config* cfg, drg_result* out);
 // Whether n device letters hold a code above 24; syncs the context's stream.

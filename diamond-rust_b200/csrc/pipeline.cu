@@ -14,6 +14,7 @@
 #include <thrust/iterator/counting_iterator.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <thread>
 #include <cmath>
@@ -63,24 +64,21 @@ uint64_t select_indices(drg_ctx* c, const uint8_t* flags, uint64_t n, uint32_t* 
   return (uint64_t)fetch(c, d_count);
 }
 
+// Device time of a stage on the context's stream, added to a stats field
+// when the search's TimeLog resolves (no wait here).
 struct Timer {
   drg_ctx* c;
-  cudaEvent_t a, b;
-  explicit Timer(drg_ctx* ctx) : c(ctx) {
-    DRG_CUDA(cudaEventCreate(&a));
-    DRG_CUDA(cudaEventCreate(&b));
+  TimeLog* log;
+  cudaEvent_t a = nullptr;
+  Timer(drg_ctx* ctx, TimeLog* times) : c(ctx), log(times) {}
+  void start() {
+    a = log->event();
+    DRG_CUDA(cudaEventRecord(a, c->stream));
   }
-  ~Timer() {
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
-  }
-  void start() { DRG_CUDA(cudaEventRecord(a, c->stream)); }
-  double stop() {
+  void stop(double* dst) {
+    cudaEvent_t b = log->event();
     DRG_CUDA(cudaEventRecord(b, c->stream));
-    DRG_CUDA(cudaEventSynchronize(b));
-    float ms = 0;
-    DRG_CUDA(cudaEventElapsedTime(&ms, a, b));
-    return ms;
+    log->span(a, b, dst);
   }
 };
 
@@ -463,13 +461,15 @@ BandJobs make_band_jobs(drg_ctx* c, const uint32_t* order, const uint64_t* keys,
     });
     count_launch();
     k_set_band_trace_off<<<ceil_div(n, 256), 256, 0, c->stream>>>(r.jobs, off, n);
-    r.trace_words = fetch(c, off + n);
   }
-  unsigned long long h[5];
-  DRG_CUDA(cudaMemcpyAsync(h, dmaxw, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  // max width, jobs per route and (trace) the trace size, in one wait
+  unsigned long long* h = c->h_stage.as<unsigned long long>(6);
+  DRG_CUDA(cudaMemcpyAsync(h, dmaxw, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+  if (trace) DRG_CUDA(cudaMemcpyAsync(h + 5, off + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream));
   DRG_CUDA(cudaStreamSynchronize(c->stream));
   r.max_width = (int)h[0];
   for (int k = 0; k < 4; ++k) r.route_lo[k + 1] = r.route_lo[k] + h[1 + k];
+  if (trace) r.trace_words = h[5];
   return r;
 }
 
@@ -503,8 +503,10 @@ SwBandArgs band_args(const Band* bc, const BandJobs& bj, const DevSeqs& qs, cons
 void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, const DevSeqs& s,
                const Scoring& scr, bool trace, int32_t* scores, int32_t* best_row, ExactOut* out, uint32_t* ops,
                const uint64_t* d_ops_off, const std::vector<uint64_t>* h_ops_off, drg_run_stats& st,
-               int64_t* d_count, unsigned long long* cells_gpu) {
+               int64_t* d_count, unsigned long long* cells_gpu, TimeLog* times) {
   if (n_bands == 0) return;
+  TimeLog own;
+  TimeLog* log = times ? times : &own;
   uint8_t* flags = c->flags.as<uint8_t>(n_bands + 1);
   uint64_t* swk = c->sw_keys.as<uint64_t>(n_bands);
   uint64_t* swks = c->sw_keys_s.as<uint64_t>(n_bands);
@@ -548,9 +550,7 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
     SwBandArgs ba = band_args(bc, bj, qs, s, scr);
     ba.trace = c->trace.as<uint2>(bj.trace_words + 8);  // the walk reads 8-word windows
     ba.tband = tb;
-    cudaEvent_t e0, e1;
-    DRG_CUDA(cudaEventCreate(&e0));
-    DRG_CUDA(cudaEventCreate(&e1));
+    cudaEvent_t e0 = log->event(), e1 = log->event();
     DRG_CUDA(cudaEventRecord(e0, c->stream));
     // each band's walk (gapped.rs:205-279) runs in the band kernel right
     // after its DP
@@ -566,12 +566,7 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
     ba.walk.exact_below = scr.max_score + 1;
     launch_band_routes(ba, bj, true, c->stream);
     DRG_CUDA(cudaEventRecord(e1, c->stream));
-    DRG_CUDA(cudaEventSynchronize(e1));
-    float ms = 0;
-    DRG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    st.ms_trace_kernel += ms;
+    log->span(e0, e1, &st.ms_trace_kernel);
   } else if (n_fast > 0) {
     // score pass: warps of 32 narrow bands (packed inter-band kernel) and, on
     // the side stream, one warp per band for the wide ones
@@ -650,8 +645,8 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
     // The bulk class runs on the main stream; the wider classes and the wide
     // bands run on the side stream, queued first so that the long warps start
     // early and the pass ends on the bulk class's shortest tasks.
-    cudaEvent_t ev[2 * kSwClasses + 3];
-    for (auto& e : ev) DRG_CUDA(cudaEventCreate(&e));
+    std::array<cudaEvent_t, 2 * kSwClasses + 3> ev;
+    for (auto& e : ev) e = log->event();
     const int fork = 2 * kSwClasses, wide0 = fork + 1, wide1 = fork + 2;
     DRG_CUDA(cudaEventRecord(ev[fork], c->stream));
     DRG_CUDA(cudaStreamWaitEvent(c->side, ev[fork], 0));
@@ -679,21 +674,21 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
     launch_cls(0);
     const int side_end = 2 * 1 + 1;  // class 1 is the side stream's last launch
     DRG_CUDA(cudaStreamWaitEvent(c->stream, ev[side_end], 0));
-    DRG_CUDA(cudaEventSynchronize(ev[1]));
-    DRG_CUDA(cudaEventSynchronize(ev[side_end]));
-    float cls_ms[kSwClasses], side_span = 0, wide_ms = 0;
-    for (int k = 0; k < kSwClasses; ++k) DRG_CUDA(cudaEventElapsedTime(&cls_ms[k], ev[2 * k], ev[2 * k + 1]));
-    DRG_CUDA(cudaEventElapsedTime(&side_span, ev[fork], ev[side_end]));
-    DRG_CUDA(cudaEventElapsedTime(&wide_ms, ev[wide0], ev[wide1]));
-    for (auto& e : ev) cudaEventDestroy(e);
-    st.ms_sw_kernel += cls_ms[0] > side_span ? cls_ms[0] : side_span;  // wall of the concurrent launches
     for (int k = 0; k < kSwClasses; ++k) {
-      st.ms_sw_class[k] += cls_ms[k];
       st.sw_class_tasks[k] += hi[k] - lo[k];
       if (hmax[k] > st.sw_class_max_steps[k]) st.sw_class_max_steps[k] = hmax[k];
     }
-    st.ms_sw_wide += wide_ms;
     st.sw_wide_bands += wide.n;
+    drg_run_stats* stp = &st;
+    log->later([ev, fork, wide0, wide1, side_end, stp] {
+      float cls_ms[kSwClasses], side_span = 0, wide_ms = 0;
+      for (int k = 0; k < kSwClasses; ++k) DRG_CUDA(cudaEventElapsedTime(&cls_ms[k], ev[2 * k], ev[2 * k + 1]));
+      DRG_CUDA(cudaEventElapsedTime(&side_span, ev[fork], ev[side_end]));
+      DRG_CUDA(cudaEventElapsedTime(&wide_ms, ev[wide0], ev[wide1]));
+      stp->ms_sw_kernel += cls_ms[0] > side_span ? cls_ms[0] : side_span;  // wall of the concurrent launches
+      for (int k = 0; k < kSwClasses; ++k) stp->ms_sw_class[k] += cls_ms[k];
+      stp->ms_sw_wide += wide_ms;
+    });
   }
   // the exact kernel for the bands the packed kernel did not settle
   count_launch();
@@ -737,6 +732,10 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
     else k_scatter_scores<<<ceil_div(n_ex, 256), 256, 0, c->stream>>>(ex_idx, dout, n_ex, scores);
     DRG_CUDA(cudaGetLastError());
   }
+  if (!times) {  // a call of its own: its kernel times are read now
+    DRG_CUDA(cudaStreamSynchronize(c->stream));
+    own.resolve();
+  }
 }
 
 namespace {
@@ -769,6 +768,7 @@ struct Search {
   // [0] xdrops [1] cells_ref [2] computed [3] cells_gpu [4] lane cells [5] issued cells
   // [6] transposed bands
   unsigned long long* d_counters = nullptr;
+  TimeLog times;  // stage times, read after the search's last wait
 
   void configure(const drg_search_config* cfg) {
     std::string err;
@@ -925,7 +925,7 @@ void Search::build_key_filter(uint64_t n_runs) {
 }
 
 void Search::join_chunk(uint64_t c0, uint64_t c1, uint64_t n_runs) {
-  Timer tm(c);
+  Timer tm(c, &times);
   const int S = (int)shapes.size();
   const uint64_t lo = db->h_offsets[c0], hi = db->h_offsets[c1];
   const uint64_t N = (hi - lo) * (uint64_t)S;
@@ -1054,11 +1054,11 @@ void Search::join_chunk(uint64_t c0, uint64_t c1, uint64_t n_runs) {
     launch_join_expand(ja, c->stream);
   }
   acc_n += n_hits;
-  st.ms_join += tm.stop();
+  tm.stop(&st.ms_join);
 }
 
 void Search::process_hits(uint64_t pass_id) {
-  Timer tm(c);
+  Timer tm(c, &times);
   const uint64_t n_hits = acc_n;
   acc_n = 0;
   if (n_hits == 0) return;
@@ -1076,7 +1076,7 @@ void Search::process_hits(uint64_t pass_id) {
   });
   const uint64_t n_u = (uint64_t)fetch(c, d_count);
   st.unique_hits += n_u;
-  st.ms_sort += tm.stop();
+  tm.stop(&st.ms_sort);
   // ---- ungapped
   tm.start();
   uint8_t* flags = c->flags.as<uint8_t>(n_u + 1);
@@ -1112,7 +1112,7 @@ void Search::process_hits(uint64_t pass_id) {
     return cub::DeviceSelect::Flagged(t, b, segs, keep, sc_, d_count, (int64_t)n_u, c->stream);
   });
   st.segments += n_segs;
-  st.ms_ungapped += tm.stop();
+  tm.stop(&st.ms_ungapped);
   if (n_segs == 0) return;
   // ---- bands
   tm.start();
@@ -1145,7 +1145,7 @@ void Search::process_hits(uint64_t pass_id) {
   select_indices(c, flags, n_bands, pfirst, d_count);
   count_launch();
   k_set_u32<<<1, 1, 0, c->stream>>>(pfirst + n_pairs, (uint32_t)n_bands);
-  st.ms_bands += tm.stop();
+  tm.stop(&st.ms_bands);
   // ---- banded SW scores
   tm.start();
   int32_t* scores = c->scores.as<int32_t>(n_bands);
@@ -1153,8 +1153,8 @@ void Search::process_hits(uint64_t pass_id) {
   DevSeqs ss{db->letters, db->offsets, &db->h_offsets, db->score_letters};
   int32_t* best_row = c->best_row.as<int32_t>(n_bands);
   run_bands(c, bc, n_bands, qs, ss, sc, false, scores, best_row, nullptr, nullptr, nullptr, nullptr, st, d_count,
-            d_counters + 3);
-  st.ms_sw += tm.stop();
+            d_counters + 3, &times);
+  tm.stop(&st.ms_sw);
   flags = c->flags.as<uint8_t>(n_bands + 1);  // scratch buffers may have been regrown
   // ---- E-value gate and band walk
   tm.start();
@@ -1205,7 +1205,7 @@ void Search::process_hits(uint64_t pass_id) {
       cands.push_back(cd);
     }
   }
-  st.ms_select += tm.stop();
+  tm.stop(&st.ms_select);
 }
 
 int cmp_cand(const Candidate& a, const Candidate& b) {  // cmp_hsp, search.rs:273-282
@@ -1308,7 +1308,7 @@ void Search::finish(drg_result* out) {
   std::vector<ExactOut> eo;
   std::vector<uint32_t> ops_all;
   if (nj > 0) {
-    Timer tm(c);
+    Timer tm(c, &times);
     tm.start();
     Band* db_ = c->sel_bands.as<Band>(nj);
     uint64_t* doff = c->ops_off.as<uint64_t>(nj + 1);
@@ -1319,7 +1319,7 @@ void Search::finish(drg_result* out) {
     DevSeqs qs{q->letters, q->offsets, &q->h_offsets, q->score_letters};
     DevSeqs ss{db->letters, db->offsets, &db->h_offsets, db->score_letters};
     run_bands(c, db_, nj, qs, ss, sc, true, nullptr, nullptr, dout, dops, doff, &ops_off, st, d_count,
-              nullptr);
+              nullptr, &times);
     // only the ops the alignments use come back (each band has n + m slots)
     uint64_t* cnt = c->ops_cnt.as<uint64_t>(nj + 1);
     uint64_t* coff = c->ops_coff.as<uint64_t>(nj + 1);
@@ -1334,7 +1334,7 @@ void Search::finish(drg_result* out) {
     k_compact_ops<<<ceil_div(nj, 128), 128, 0, c->stream>>>(dops, doff, dout, coff, nj, cops);
     fetch_n(c, eo, dout, nj);
     fetch_n(c, ops_all, cops, n_used);
-    st.ms_trace += tm.stop();
+    tm.stop(&st.ms_trace);
   }
   auto t1 = std::chrono::steady_clock::now();
   // assemble per-target lists
@@ -1388,7 +1388,7 @@ void Search::finish(drg_result* out) {
 
 void Search::run(drg_result* out) {
   const uint64_t launches0 = kernel_launch_count();
-  Timer total(c);
+  Timer total(c, &times);
   total.start();
   std::memset(out, 0, sizeof(*out));
   d_count = c->counters.as<int64_t>(9);
@@ -1399,15 +1399,17 @@ void Search::run(drg_result* out) {
     out->target_offsets = (uint64_t*)std::calloc(q->n + 1, sizeof(uint64_t));
     out->hsps = (drg_hsp*)std::malloc(sizeof(drg_hsp));
     out->ops = (uint32_t*)std::malloc(sizeof(uint32_t));
-    st.ms_total = total.stop();
+    total.stop(&st.ms_total);
+    DRG_CUDA(cudaStreamSynchronize(c->stream));
+    times.resolve();
     out->stats = st;
     return;
   }
-  Timer tm(c);
+  Timer tm(c, &times);
   tm.start();
   uint64_t n_runs = 0;
   query_seeds(&n_runs);
-  st.ms_seed = tm.stop();
+  tm.stop(&st.ms_seed);
   if (n_runs > 0) {
     constexpr uint64_t kHitPassBudget = 1ull << 28;  // hits held before the stages after the join run
     uint64_t pass = 0;
@@ -1418,9 +1420,11 @@ void Search::run(drg_result* out) {
     process_hits(pass++);
   }
   finish(out);
+  total.stop(&st.ms_total);
   unsigned long long cnt[7];
   DRG_CUDA(cudaMemcpyAsync(cnt, d_counters, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
   DRG_CUDA(cudaStreamSynchronize(c->stream));
+  times.resolve();
   st.xdrops = cnt[0];
   st.dp_cells_ref = cnt[1];
   st.bands_computed = cnt[2];
@@ -1429,7 +1433,6 @@ void Search::run(drg_result* out) {
   st.dp_cells_issued = cnt[5];
   st.sw_transposed_bands = cnt[6];
   st.seed_shapes = shapes.size();
-  st.ms_total = total.stop();
   st.kernel_launches = kernel_launch_count() - launches0;
   out->stats = st;
 }
