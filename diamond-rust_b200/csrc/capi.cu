@@ -211,12 +211,13 @@ int drg_seed_build(drg_ctx* c, const uint8_t* letters, const uint64_t* offsets, 
   if (!parse_shape(shape_code, &sh))
     throw Error(DRG_ERR_INVALID, std::string("invalid seed shape \"") + shape_code + "\": expected only 0/1");
   if (sh.weight > kMaxWeight) throw Error(DRG_ERR_INVALID, "seed shape weight above 16");
+  if (sh.span > kMaxSpan) throw Error(DRG_ERR_INVALID, "seed shape longer than 256 positions");
   if (reduction < 0 || reduction > 2) throw Error(DRG_ERR_INVALID, "unknown reduction id");
   ReducedAlphabet red = reduction_by_id(reduction);
   ShapeTable t{};
   t.n = 1;
   t.weight[0] = (uint8_t)sh.weight;
-  t.span[0] = (uint8_t)sh.span;
+  t.span[0] = (uint16_t)sh.span;
   for (int k = 0; k < sh.weight; ++k) t.pos[0][k] = (uint8_t)sh.positions[k];
   SeedParams p{};
   for (int i = 0; i < 32; ++i) p.bucket[i] = 255;

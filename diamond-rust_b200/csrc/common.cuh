@@ -114,10 +114,11 @@ inline int bits_for(uint64_t v) {  // bits needed to store values 0..v
 // Seed shapes as the kernels see them (shape.rs:11-20).
 constexpr int kMaxShapes = 64;
 constexpr int kMaxWeight = 16;
+constexpr int kMaxSpan = 256;  // positions are bytes
 struct ShapeTable {
   int n;
   uint8_t weight[kMaxShapes];
-  uint8_t span[kMaxShapes];
+  uint16_t span[kMaxShapes];  // up to kMaxSpan (256)
   uint8_t pos[kMaxShapes][kMaxWeight];
 };
 

@@ -789,8 +789,9 @@ struct Search {
     t.n = (int)shapes.size();
     for (int s = 0; s < t.n; ++s) {
       if (shapes[s].weight > kMaxWeight) throw Error(DRG_ERR_INVALID, "seed shape weight above 16");
+      if (shapes[s].span > kMaxSpan) throw Error(DRG_ERR_INVALID, "seed shape longer than 256 positions");
       t.weight[s] = (uint8_t)shapes[s].weight;
-      t.span[s] = (uint8_t)shapes[s].span;
+      t.span[s] = (uint16_t)shapes[s].span;
       for (int k = 0; k < shapes[s].weight; ++k) t.pos[s][k] = (uint8_t)shapes[s].positions[k];
     }
     SeedParams p{};

@@ -86,37 +86,75 @@ void launch_letter_owner(const uint64_t* offsets, uint64_t n_seqs, uint64_t lo, 
   DRG_CUDA(cudaGetLastError());
 }
 
-// One seed: the reduced key and the log-multinomial complexity test.  The
-// counts live in three 64-bit words (8 buckets x 8 bits each); the entropy is
-// lnfact[w] minus lnfact[c_b] for b = 0, 1, ... in bucket order, the order the
-// reference subtracts in, so the double result is identical.  The bucket and
-// ln-factorial tables are indexed by per-lane data, so they are read from
-// shared copies (constant memory serialises distinct addresses in a warp).
-__device__ __forceinline__ bool seed_at(const uint8_t* __restrict__ p, int s, int slot, const uint8_t* bucket,
-                                        const double* lnfact, uint64_t* key_out) {
+// Seed enumeration runs one thread per letter in blocks of kEnumBlock; each
+// block first turns its letters (plus the longest span past the last one)
+// into reduced buckets in shared memory, 255 for a letter that cannot seed
+// (a code of 20 or more, a letter outside the reduction, or past the range).
+constexpr int kEnumBlock = 256;
+
+struct EnumTables {
+  uint8_t rb[kEnumBlock + kMaxSpan];
+  double lnfact[33];
+  double lnstep[33];  // lnfact[j] - lnfact[j - 1]
+};
+
+__device__ __forceinline__ void stage_enum_tables(const uint8_t* __restrict__ letters, uint64_t base, uint64_t hi,
+                                                  int slot, EnumTables& t) {
+  const SeedParams& sp = c_seed[slot];
+  for (int j = threadIdx.x; j < kEnumBlock + kMaxSpan; j += blockDim.x) {
+    const uint64_t g = base + j;
+    uint8_t b = 255;
+    if (g < hi) {
+      const uint32_t l = letters[g];
+      if (l < 20) b = sp.bucket[l];
+    }
+    t.rb[j] = b;
+  }
+  if (threadIdx.x < 33) {
+    t.lnfact[threadIdx.x] = sp.lnfact[threadIdx.x];
+    t.lnstep[threadIdx.x] = threadIdx.x ? sp.lnfact[threadIdx.x] - sp.lnfact[threadIdx.x - 1] : 0.0;
+  }
+  __syncthreads();
+}
+
+// One seed from the staged buckets at rb: the reduced key and the
+// log-multinomial complexity test (seed.rs).  The counts live in three
+// 64-bit words (8 buckets x 8 bits each).  The reference's entropy is
+// lnfact[w] minus lnfact[c_b] for b = 0, 1, ... in bucket order; the same
+// quantity is first summed per letter as ln(count after the letter), which
+// differs from the bucket-ordered double result by under 1e-12.  Only when
+// that sum lies within 1e-9 of the cut is the bucket-ordered value computed,
+// so the decision is the reference's.
+__device__ __forceinline__ bool seed_at(const uint8_t* rb, int s, int slot, const EnumTables& t,
+                                        uint64_t* key_out) {
   const ShapeTable& shp = c_shapes[slot];
   const SeedParams& sp = c_seed[slot];
   const int w = shp.weight[s];
   const uint64_t size = sp.size;
   uint64_t key = 0, c0 = 0, c1 = 0, c2 = 0;
+  double acc = 0.0;
   for (int k = 0; k < w; ++k) {
-    uint32_t l = p[shp.pos[s][k]];
-    if (l >= 20) return false;
-    uint32_t b = bucket[l];
+    const uint32_t b = rb[shp.pos[s][k]];
     if (b >= 24) return false;
     key = key * size + b;
-    uint64_t inc = 1ull << (8 * (b & 7));
-    if (b < 8) c0 += inc;
-    else if (b < 16) c1 += inc;
-    else c2 += inc;
+    const int sh = 8 * (b & 7);
+    const uint64_t inc = 1ull << sh;
+    uint64_t word;
+    if (b < 8) word = (c0 += inc);
+    else if (b < 16) word = (c1 += inc);
+    else word = (c2 += inc);
+    acc += t.lnstep[(word >> sh) & 0xffu];
   }
   const double cut = sp.cut;
   if (cut > 0.0) {
-    double e = lnfact[w];
-    for (int b = 0; b < (int)size; ++b) {
-      uint64_t word = b < 8 ? c0 : (b < 16 ? c1 : c2);
-      uint32_t c = (uint32_t)(word >> (8 * (b & 7))) & 0xffu;
-      if (c > 0) e = __dsub_rn(e, lnfact[c]);
+    double e = t.lnfact[w] - acc;
+    if (fabs(e - cut) <= 1e-9) {
+      e = t.lnfact[w];
+      for (int b = 0; b < (int)size; ++b) {
+        uint64_t word = b < 8 ? c0 : (b < 16 ? c1 : c2);
+        uint32_t c = (uint32_t)(word >> (8 * (b & 7))) & 0xffu;
+        if (c > 0) e = __dsub_rn(e, t.lnfact[c]);
+      }
     }
     if (!(e >= cut)) return false;
   }
@@ -131,13 +169,10 @@ __global__ void k_seed_enum(const uint8_t* __restrict__ letters, const uint64_t*
                             const uint32_t* __restrict__ owner, uint64_t lo, uint64_t hi, int n_shapes,
                             K* __restrict__ keys, uint32_t* __restrict__ vals,
                             const uint32_t* __restrict__ request, int slot) {
-  __shared__ uint8_t bucket[32];
-  __shared__ double lnfact[33];
-  if (threadIdx.x < 32) bucket[threadIdx.x] = c_seed[slot].bucket[threadIdx.x];
-  if (threadIdx.x < 33) lnfact[threadIdx.x] = c_seed[slot].lnfact[threadIdx.x];
-  __syncthreads();
+  __shared__ EnumTables tab;
   const uint64_t L = hi - lo;
-  const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t i = blockIdx.x * (uint64_t)kEnumBlock + threadIdx.x;
+  stage_enum_tables(letters, lo + blockIdx.x * (uint64_t)kEnumBlock, hi, slot, tab);
   if (i >= L) return;
   const uint64_t g = lo + i;
   const uint32_t seq = owner[i];
@@ -146,7 +181,7 @@ __global__ void k_seed_enum(const uint8_t* __restrict__ letters, const uint64_t*
   const uint64_t req = request ? (uint64_t)request[seq] << sp.request_shift : 0;
   for (int s = 0; s < n_shapes; ++s) {
     uint64_t key = 0;
-    const bool ok = g + c_shapes[slot].span[s] <= end && seed_at(letters + g, s, slot, bucket, lnfact, &key);
+    const bool ok = g + c_shapes[slot].span[s] <= end && seed_at(tab.rb + threadIdx.x, s, slot, tab, &key);
     keys[s * L + i] = ok ? (K)(req | ((uint64_t)s << sp.shape_shift) | key) : (K)kNoSeed;
     vals[s * L + i] = (uint32_t)g;
   }
@@ -157,8 +192,8 @@ void launch_seed_enum(const uint8_t* letters, const uint64_t* offsets, const uin
                       const uint32_t* request) {
   if (hi <= lo || n_shapes == 0) return;
   count_launch();
-  k_seed_enum<uint64_t><<<ceil_div(hi - lo, 256), 256, 0, st>>>(letters, offsets, owner, lo, hi, n_shapes, keys,
-                                                               vals, request, slot);
+  k_seed_enum<uint64_t><<<ceil_div(hi - lo, kEnumBlock), kEnumBlock, 0, st>>>(letters, offsets, owner, lo, hi,
+                                                                             n_shapes, keys, vals, request, slot);
   DRG_CUDA(cudaGetLastError());
 }
 
@@ -166,8 +201,8 @@ void launch_seed_enum(const uint8_t* letters, const uint64_t* offsets, const uin
                       uint64_t hi, int n_shapes, uint32_t* keys, uint32_t* vals, int slot, cudaStream_t st) {
   if (hi <= lo || n_shapes == 0) return;
   count_launch();
-  k_seed_enum<uint32_t><<<ceil_div(hi - lo, 256), 256, 0, st>>>(letters, offsets, owner, lo, hi, n_shapes, keys,
-                                                               vals, nullptr, slot);
+  k_seed_enum<uint32_t><<<ceil_div(hi - lo, kEnumBlock), kEnumBlock, 0, st>>>(letters, offsets, owner, lo, hi,
+                                                                             n_shapes, keys, vals, nullptr, slot);
   DRG_CUDA(cudaGetLastError());
 }
 
@@ -203,7 +238,7 @@ void launch_key_filter(const uint64_t* run_keys, uint64_t n, uint64_t key_mask, 
 // range with one atomic per group; counts[0] = seeds kept, counts[1] = valid
 // seeds (kept or not).  The output order depends on the blocks' timing; the
 // caller sorts by key, and the hits made from them are sorted in full later.
-constexpr int kFilterBlock = 256, kFilterGroup = 8;
+constexpr int kFilterBlock = kEnumBlock, kFilterGroup = 8;
 
 template <typename K>
 __global__ void __launch_bounds__(kFilterBlock)
@@ -211,19 +246,16 @@ __global__ void __launch_bounds__(kFilterBlock)
                          const uint32_t* __restrict__ owner, uint64_t lo, uint64_t hi, int n_shapes,
                          const uint32_t* __restrict__ filter, int log2_bits, K* __restrict__ keys,
                          uint32_t* __restrict__ vals, unsigned long long* __restrict__ counts, int slot) {
-  __shared__ uint8_t bucket[32];
-  __shared__ double lnfact[33];
+  __shared__ EnumTables tab;
   __shared__ K s_keys[kFilterBlock * kFilterGroup];
   __shared__ uint32_t s_vals[kFilterBlock * kFilterGroup];
   __shared__ uint32_t s_n;
   __shared__ unsigned long long s_base, s_valid;
-  if (threadIdx.x < 32) bucket[threadIdx.x] = c_seed[slot].bucket[threadIdx.x];
-  if (threadIdx.x < 33) lnfact[threadIdx.x] = c_seed[slot].lnfact[threadIdx.x];
   if (threadIdx.x == 0) {
     s_n = 0;
     s_valid = 0;
   }
-  __syncthreads();
+  stage_enum_tables(letters, lo + blockIdx.x * (uint64_t)kFilterBlock, hi, slot, tab);  // ends with a barrier
   const uint64_t L = hi - lo;
   const uint64_t i = blockIdx.x * (uint64_t)kFilterBlock + threadIdx.x;
   const bool in = i < L;
@@ -235,7 +267,7 @@ __global__ void __launch_bounds__(kFilterBlock)
     const int s1 = min(n_shapes, s0 + kFilterGroup);
     for (int s = s0; s < s1; ++s) {
       uint64_t key = 0;
-      if (in && g + c_shapes[slot].span[s] <= end && seed_at(letters + g, s, slot, bucket, lnfact, &key)) {
+      if (in && g + c_shapes[slot].span[s] <= end && seed_at(tab.rb + threadIdx.x, s, slot, tab, &key)) {
         ++valid;
         const uint64_t k = ((uint64_t)s << sp.shape_shift) | key;
         const uint32_t h = seed_key_hash(k, log2_bits);

@@ -26,7 +26,8 @@ def rand_seq(r, n, ambiguous=0.0):
 
 
 # ---------------------------------------------------------------- seed::build
-SHAPES = ["1111", "101", "111101110111", "1011110111", "11110111", "1101110101101111", "1100010100000010011"]
+SHAPES = ["1111", "101", "111101110111", "1011110111", "11110111", "1101110101101111", "1100010100000010011",
+          "1" + "0" * 40 + "111"]
 
 
 @pytest.mark.parametrize("shape", SHAPES)
@@ -64,6 +65,35 @@ def test_seed_build_rejects_bad_shape(ctx):
     with pytest.raises(drgpu.DrgError) as ei:
         ctx.seed_build([np.zeros(10, np.uint8)], "1021")
     assert ei.value.code == 1
+    with pytest.raises(drgpu.DrgError) as ei:  # positions are bytes: 256 at most
+        ctx.seed_build([np.zeros(300, np.uint8)], "1" + "0" * 255 + "1")
+    assert ei.value.code == 1
+
+
+def test_seed_build_longest_span(ctx, orc):
+    r = rng(19)
+    seqs = [rand_seq(r, int(n)) for n in (0, 255, 256, 257, 300, 600)]
+    shape = "11" + "0" * 252 + "11"  # span 256
+    got = np.sort(ctx.seed_build(seqs, shape, 0, base=3, cut=0.0), order=["key", "seq", "pos"])
+    exp = np.sort(orc.seed_build(seqs, shape, 0, base=3, cut=0.0), order=["key", "seq", "pos"])
+    assert len(exp) == 1 + 2 + 45 + 345 and (got == exp).all()
+
+
+def test_seed_complexity_cut_at_the_boundary(ctx, orc):
+    # The device sums the entropy per letter and recomputes it in the
+    # reference's bucket order only near the cut: cuts a few ulps around the
+    # entropy of each count pattern of a 4-letter seed must decide as the
+    # oracle does.
+    words = ["AACC", "ACAC", "AAAC", "AACD", "ACDE", "AAAA", "CACA", "DCBA"]
+    seqs = [orc.encode(w * 6) for w in words]
+    for e in (np.log(6.0), np.log(4.0), np.log(12.0), np.log(24.0), 0.0):
+        for k in range(-4, 5):
+            cut = float(e)
+            for _ in range(abs(k)):
+                cut = float(np.nextafter(cut, np.inf if k > 0 else -np.inf))
+            got = np.sort(ctx.seed_build(seqs, "1111", 2, base=0, cut=cut), order=["key", "seq", "pos"])
+            exp = np.sort(orc.seed_build(seqs, "1111", 2, base=0, cut=cut), order=["key", "seq", "pos"])
+            assert len(got) == len(exp) and (got == exp).all(), (e, k)
 
 
 # ------------------------------------------------------------- seed::join_into
