@@ -140,14 +140,39 @@ __host__ __device__ __forceinline__ void band_rows(const Band& b, int64_t m, boo
 }
 
 // Number of sorted keys below `bound`.
-__global__ void k_count_below(const uint64_t* keys, uint64_t n, uint64_t bound, int64_t* out) {
+// After a run-length encoding of n sorted seed keys into io[0] runs (keys
+// rk): io[0] = runs of valid keys (the last run is dropped when it is the
+// "no seed" run), io[1] = valid keys.
+__global__ void k_valid_runs(const uint64_t* keys, uint64_t n, const uint64_t* rk, int64_t* io) {
   uint64_t lo = 0, hi = n;
   while (lo < hi) {
     const uint64_t m = (lo + hi) >> 1;
-    if (keys[m] < bound) lo = m + 1;
+    if (keys[m] < kNoSeed) lo = m + 1;
     else hi = m;
   }
-  *out = (int64_t)lo;
+  const int64_t runs = io[0];
+  io[0] = runs > 0 && rk[runs - 1] == kNoSeed ? runs - 1 : runs;
+  io[1] = (int64_t)lo;
+}
+
+// Sorted band keys: out[0] = keys below kNoSeed (bands the packed kernels
+// take), out[1] = keys below kWideKey (narrow bands, which sort first).
+__global__ void k_count_fast_narrow(const uint64_t* keys, uint64_t n, int64_t* out) {
+  uint64_t lo = 0, hi = n;
+  while (lo < hi) {
+    const uint64_t m = (lo + hi) >> 1;
+    if (keys[m] < kNoSeed) lo = m + 1;
+    else hi = m;
+  }
+  out[0] = (int64_t)lo;
+  hi = lo;
+  lo = 0;
+  while (lo < hi) {
+    const uint64_t m = (lo + hi) >> 1;
+    if (keys[m] < kWideKey) lo = m + 1;
+    else hi = m;
+  }
+  out[1] = (int64_t)lo;
 }
 
 // Which kernel a band goes to: the packed kernel (fast), its wide-band
@@ -538,7 +563,16 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
   cub_call(c, [&](void* t, size_t& b) {
     return cub::DeviceRadixSort::SortPairs(t, b, swk_r, swks, swo_r, swos, (int64_t)n_bands, kKeyLo, 64, c->stream);
   });
-  const uint64_t n_fast = (uint64_t)count_valid(c, swks, n_bands, d_count);
+  uint64_t n_fast = 0, n_narrow = 0;
+  {
+    count_launch();
+    k_count_fast_narrow<<<1, 1, 0, c->stream>>>(swks, n_bands, d_count);
+    int64_t* h = c->h_stage.as<int64_t>(2);
+    DRG_CUDA(cudaMemcpyAsync(h, d_count, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
+    DRG_CUDA(cudaStreamSynchronize(c->stream));
+    n_fast = (uint64_t)h[0];
+    n_narrow = (uint64_t)h[1];
+  }
   TraceBand* tb = nullptr;
   if (trace) {
     tb = c->tband.as<TraceBand>(n_bands);
@@ -570,11 +604,6 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
   } else if (n_fast > 0) {
     // score pass: warps of 32 narrow bands (packed inter-band kernel) and, on
     // the side stream, one warp per band for the wide ones
-    const uint64_t n_narrow = [&] {
-      count_launch();
-      k_count_below<<<1, 1, 0, c->stream>>>(swks, n_fast, kWideKey, d_count);
-      return (uint64_t)fetch(c, d_count);
-    }();
     const BandJobs wide = make_band_jobs(c, swos + n_narrow, swks + n_narrow, n_fast - n_narrow, bc, s.offsets,
                                          false);
     uint64_t n_tasks = 0;
@@ -877,16 +906,22 @@ void Search::query_seeds(uint64_t* n_runs_out) {
   cub_call(c, [&](void* t, size_t& b) {
     return cub::DeviceRadixSort::SortPairs(t, b, keys, keys_s, vals, vals_s, (int64_t)N, 0, key_bits, c->stream);
   });
-  int64_t nv = count_valid(c, keys_s, N, d_count);
-  st.query_seeds = (uint64_t)nv;
-  uint64_t* rk = c->run_keys.as<uint64_t>(nv + 1);
-  uint32_t* rc = c->run_counts.as<uint32_t>(nv + 1);
+  // runs of every key (the "no seed" keys, last, form one run of their own),
+  // then the valid keys and their runs counted in one kernel: one wait
+  uint64_t* rk = c->run_keys.as<uint64_t>(N + 1);
+  uint32_t* rc = c->run_counts.as<uint32_t>(N + 1);
   uint64_t n_runs = 0;
-  if (nv > 0) {
+  if (N > 0) {
     cub_call(c, [&](void* t, size_t& b) {
-      return cub::DeviceRunLengthEncode::Encode(t, b, keys_s, rk, rc, d_count, (int64_t)nv, c->stream);
+      return cub::DeviceRunLengthEncode::Encode(t, b, keys_s, rk, rc, d_count, (int64_t)N, c->stream);
     });
-    n_runs = (uint64_t)fetch(c, d_count);
+    count_launch();
+    k_valid_runs<<<1, 1, 0, c->stream>>>(keys_s, N, rk, d_count);
+    int64_t* h = c->h_stage.as<int64_t>(2);
+    DRG_CUDA(cudaMemcpyAsync(h, d_count, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
+    DRG_CUDA(cudaStreamSynchronize(c->stream));
+    n_runs = (uint64_t)h[0];
+    st.query_seeds = (uint64_t)h[1];
   }
   uint32_t* qs = c->run_qstart.as<uint32_t>(n_runs + 1);
   if (n_runs > 0)
