@@ -52,12 +52,20 @@ constexpr uint32_t kMaxRequests = 65535;  // request ids of one batch
 // For each query run u (unique key, count, start): the reference run [lo, hi)
 // with the same key (query key & key_mask) and the number of hits it yields
 // under the expansion cap.
+// With `first` (launch_bucket_first over the same reference keys), each
+// search covers one bucket of keys sharing their bits above `shift`.
 void launch_join_count(const uint64_t* run_keys, const uint32_t* run_counts, uint64_t n_runs,
                        const uint64_t* ref_keys, uint64_t n_ref, uint64_t max_expand, uint32_t* run_rlo,
-                       uint32_t* run_rcount, uint64_t* run_hits, uint64_t key_mask, cudaStream_t st);
+                       uint32_t* run_rcount, uint64_t* run_hits, uint64_t key_mask, cudaStream_t st,
+                       const uint32_t* first = nullptr, int shift = 0);
 void launch_join_count(const uint64_t* run_keys, const uint32_t* run_counts, uint64_t n_runs,
                        const uint32_t* ref_keys, uint64_t n_ref, uint64_t max_expand, uint32_t* run_rlo,
-                       uint32_t* run_rcount, uint64_t* run_hits, uint64_t key_mask, cudaStream_t st);
+                       uint32_t* run_rcount, uint64_t* run_hits, uint64_t key_mask, cudaStream_t st,
+                       const uint32_t* first = nullptr, int shift = 0);
+// first[b] (b in [0, nb]) = index of the first of n sorted keys whose
+// key >> shift is at least b; first[nb] = n.  Keys must be below nb << shift.
+void launch_bucket_first(const uint64_t* keys, uint64_t n, int shift, uint32_t nb, uint32_t* first, cudaStream_t st);
+void launch_bucket_first(const uint32_t* keys, uint64_t n, int shift, uint32_t nb, uint32_t* first, cudaStream_t st);
 
 // Layout of the packed 64-bit hit key (target, subject, diag + doff, spos).
 struct HitKeyLayout {

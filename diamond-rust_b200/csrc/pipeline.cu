@@ -122,6 +122,10 @@ __host__ __device__ __forceinline__ int sw_class_of(uint32_t w) {
 // (Medium bands share warps with the narrow bands of their group: giving
 // them warps of their own left most of those warps' lanes idle.)
 constexpr uint64_t kWideKey = 1ull << 63, kTransposedKey = 1ull << 61;
+// Task and band-job sort keys: class or route (< 8) above a cost field whose
+// inverse orders longest first; the order only schedules, so costs saturate.
+constexpr int kCostBits = 24;
+constexpr uint64_t kCostMax = (1ull << kCostBits) - 1;
 constexpr int kGroupShift = 24, kWidthShift = 13, kKeyLo = 13;
 
 // DP rows [rs, re] of a band with at least one in-matrix cell: rows are the
@@ -291,7 +295,8 @@ __global__ void k_sw_fill_tasks(const uint32_t* starts, uint64_t n_tasks, const 
   tasks[t] = k;
   const uint64_t steps = (uint64_t)k.n_strips * (wmax + 16ull);
   const int cls = sw_class_of(wmax);
-  sort_key[t] = ((uint64_t)cls << 60) | ((~steps) & ((1ull << 60) - 1));  // class, then longest first
+  // class, then longest first (a scheduling order: 24 bits of steps, saturated, suffice)
+  sort_key[t] = ((uint64_t)cls << kCostBits) | (kCostMax - (steps < kCostMax ? steps : kCostMax));
   sort_val[t] = (uint32_t)t;
   if (trace_size) trace_size[t] = steps * 32ull;
   if (cells_gpu) {
@@ -366,7 +371,7 @@ __global__ void k_band_jobs(const uint32_t* order, const uint64_t* keys, uint64_
   // by kernel route (sw_band_route), then longest first
   const int route = sw_band_route((int)W, trace);
   const uint64_t cost = (uint64_t)(j.n_strips - 1) * 19ull + W + 16ull;
-  sort_key[k] = ((uint64_t)route << 60) | ((~cost) & ((1ull << 60) - 1));
+  sort_key[k] = ((uint64_t)route << kCostBits) | (kCostMax - (cost < kCostMax ? cost : kCostMax));
   sort_val[k] = (uint32_t)k;
   atomicMax(max_width, (unsigned long long)W);
   atomicAdd(max_width + 1 + route, 1ull);
@@ -474,7 +479,7 @@ BandJobs make_band_jobs(drg_ctx* c, const uint32_t* order, const uint64_t* keys,
   k_band_jobs<<<ceil_div(n, 256), 256, 0, c->stream>>>(order, keys, n, bc, s_offsets, trace, jobs_u, key, val,
                                                        dmaxw);
   cub_call(c, [&](void* t, size_t& b) {
-    return cub::DeviceRadixSort::SortPairs(t, b, key, key_s, val, val_s, (int64_t)n, 0, 64, c->stream);
+    return cub::DeviceRadixSort::SortPairs(t, b, key, key_s, val, val_s, (int64_t)n, 0, kCostBits + 3, c->stream);
   });
   uint64_t* size = c->bj_size.as<uint64_t>(n + 1);
   uint64_t* off = c->bj_off.as<uint64_t>(n + 1);
@@ -632,7 +637,7 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
                                                                       cells_gpu);
       // by width class, longest warps first within a class
       cub_call(c, [&](void* t, size_t& b) {
-        return cub::DeviceRadixSort::SortPairs(t, b, tkey, tkey_s, tval, tval_s, (int64_t)n_tasks, 0, 64,
+        return cub::DeviceRadixSort::SortPairs(t, b, tkey, tkey_s, tval, tval_s, (int64_t)n_tasks, 0, kCostBits + 2,
                                                c->stream);
       });
       count_launch();
@@ -1055,12 +1060,21 @@ void Search::join_chunk(uint64_t c0, uint64_t c1, uint64_t n_runs) {
   uint32_t* rcnt = c->run_rcount.as<uint32_t>(n_runs + 1);
   uint64_t* rhits = c->run_hits.as<uint64_t>(n_runs + 1);
   uint64_t* roff = c->run_hit_off.as<uint64_t>(n_runs + 1);
-  if (keys32_s)
+  // bucket starts over the top 16 bits of the sorted reference keys: each
+  // query run then searches ~nr / 65536 keys instead of nr
+  const int bucket_bits = std::min(16, seed_key_bits);
+  const int shift = seed_key_bits - bucket_bits;
+  const uint32_t nb = 1u << bucket_bits;
+  uint32_t* first = c->ref_first.as<uint32_t>(nb + 1);
+  if (keys32_s) {
+    launch_bucket_first(keys32_s, (uint64_t)nr, shift, nb, first, c->stream);
     launch_join_count(c->run_keys.as<uint64_t>(0), c->run_counts.as<uint32_t>(0), n_runs, keys32_s, (uint64_t)nr,
-                      4096, rlo, rcnt, rhits, (1ull << seed_key_bits) - 1, c->stream);
-  else
+                      4096, rlo, rcnt, rhits, (1ull << seed_key_bits) - 1, c->stream, first, shift);
+  } else {
+    launch_bucket_first(keys_s, (uint64_t)nr, shift, nb, first, c->stream);
     launch_join_count(c->run_keys.as<uint64_t>(0), c->run_counts.as<uint32_t>(0), n_runs, keys_s, (uint64_t)nr, 4096,
-                      rlo, rcnt, rhits, (1ull << seed_key_bits) - 1, c->stream);
+                      rlo, rcnt, rhits, (1ull << seed_key_bits) - 1, c->stream, first, shift);
+  }
   count_launch();
   k_set_u64<<<1, 1, 0, c->stream>>>(rhits + n_runs, 0);
   cub_call(c, [&](void* t, size_t& b) {

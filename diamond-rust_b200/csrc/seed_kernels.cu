@@ -320,22 +320,60 @@ void launch_seed_enum_filtered(const uint8_t* letters, const uint64_t* offsets, 
   seed_enum_filtered(letters, offsets, owner, lo, hi, n_shapes, filter, log2_bits, keys, vals, counts, slot, st);
 }
 
+// first[b] = the first of n sorted keys with key >> shift >= b, for b in
+// [0, nb]; the join then searches one bucket's range instead of all keys.
+template <typename K>
+__global__ void k_bucket_first(const K* __restrict__ keys, uint64_t n, int shift, uint32_t nb,
+                               uint32_t* __restrict__ first) {
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b > nb) return;
+  const uint64_t key = (uint64_t)b << shift;
+  uint64_t lo = 0, hi = n;
+  while (lo < hi) {
+    const uint64_t m = (lo + hi) >> 1;
+    if ((uint64_t)keys[m] < key) lo = m + 1;
+    else hi = m;
+  }
+  first[b] = b == nb ? (uint32_t)n : (uint32_t)lo;
+}
+
+template <typename K>
+void bucket_first(const K* keys, uint64_t n, int shift, uint32_t nb, uint32_t* first, cudaStream_t st) {
+  count_launch();
+  k_bucket_first<K><<<ceil_div((long long)nb + 1, 256), 256, 0, st>>>(keys, n, shift, nb, first);
+  DRG_CUDA(cudaGetLastError());
+}
+
+void launch_bucket_first(const uint64_t* keys, uint64_t n, int shift, uint32_t nb, uint32_t* first, cudaStream_t st) {
+  bucket_first(keys, n, shift, nb, first, st);
+}
+
+void launch_bucket_first(const uint32_t* keys, uint64_t n, int shift, uint32_t nb, uint32_t* first, cudaStream_t st) {
+  bucket_first(keys, n, shift, nb, first, st);
+}
+
 template <typename K>
 __global__ void k_join_count(const uint64_t* __restrict__ run_keys, const uint32_t* __restrict__ run_counts,
                              uint64_t n_runs, const K* __restrict__ ref_keys, uint64_t n_ref,
                              uint64_t max_expand, uint32_t* __restrict__ run_rlo, uint32_t* __restrict__ run_rcount,
-                             uint64_t* __restrict__ run_hits, uint64_t key_mask) {
+                             uint64_t* __restrict__ run_hits, uint64_t key_mask, const uint32_t* __restrict__ first,
+                             int shift) {
   uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (u >= n_runs) return;
   const uint64_t key = run_keys[u] & key_mask;  // the query run's request does not take part
-  uint64_t a = 0, b = n_ref;
+  uint64_t a = 0, end = n_ref;
+  if (first) {
+    a = first[key >> shift];
+    end = first[(key >> shift) + 1];
+  }
+  uint64_t b = end;
   while (a < b) {  // lower bound
     uint64_t m = (a + b) >> 1;
     if ((uint64_t)ref_keys[m] < key) a = m + 1;
     else b = m;
   }
   uint64_t lo = a;
-  b = n_ref;
+  b = end;
   while (a < b) {  // upper bound
     uint64_t m = (a + b) >> 1;
     if ((uint64_t)ref_keys[m] <= key) a = m + 1;
@@ -351,24 +389,28 @@ __global__ void k_join_count(const uint64_t* __restrict__ run_keys, const uint32
 template <typename K>
 void join_count(const uint64_t* run_keys, const uint32_t* run_counts, uint64_t n_runs, const K* ref_keys,
                 uint64_t n_ref, uint64_t max_expand, uint32_t* run_rlo, uint32_t* run_rcount, uint64_t* run_hits,
-                uint64_t key_mask, cudaStream_t st) {
+                uint64_t key_mask, cudaStream_t st, const uint32_t* first, int shift) {
   if (n_runs == 0) return;
   count_launch();
   k_join_count<K><<<ceil_div(n_runs, 256), 256, 0, st>>>(run_keys, run_counts, n_runs, ref_keys, n_ref, max_expand,
-                                                         run_rlo, run_rcount, run_hits, key_mask);
+                                                         run_rlo, run_rcount, run_hits, key_mask, first, shift);
   DRG_CUDA(cudaGetLastError());
 }
 
 void launch_join_count(const uint64_t* run_keys, const uint32_t* run_counts, uint64_t n_runs,
                        const uint64_t* ref_keys, uint64_t n_ref, uint64_t max_expand, uint32_t* run_rlo,
-                       uint32_t* run_rcount, uint64_t* run_hits, uint64_t key_mask, cudaStream_t st) {
-  join_count(run_keys, run_counts, n_runs, ref_keys, n_ref, max_expand, run_rlo, run_rcount, run_hits, key_mask, st);
+                       uint32_t* run_rcount, uint64_t* run_hits, uint64_t key_mask, cudaStream_t st,
+                       const uint32_t* first, int shift) {
+  join_count(run_keys, run_counts, n_runs, ref_keys, n_ref, max_expand, run_rlo, run_rcount, run_hits, key_mask, st,
+             first, shift);
 }
 
 void launch_join_count(const uint64_t* run_keys, const uint32_t* run_counts, uint64_t n_runs,
                        const uint32_t* ref_keys, uint64_t n_ref, uint64_t max_expand, uint32_t* run_rlo,
-                       uint32_t* run_rcount, uint64_t* run_hits, uint64_t key_mask, cudaStream_t st) {
-  join_count(run_keys, run_counts, n_runs, ref_keys, n_ref, max_expand, run_rlo, run_rcount, run_hits, key_mask, st);
+                       uint32_t* run_rcount, uint64_t* run_hits, uint64_t key_mask, cudaStream_t st,
+                       const uint32_t* first, int shift) {
+  join_count(run_keys, run_counts, n_runs, ref_keys, n_ref, max_expand, run_rlo, run_rcount, run_hits, key_mask, st,
+             first, shift);
 }
 
 __global__ void k_join_expand(JoinExpandArgs a) {
