@@ -79,6 +79,8 @@ struct HitKeyLayout {
 // straight from the entries' (seq, pos).
 struct JoinExpandArgs {
   const uint64_t* run_hit_off;  // exclusive scan of run_hits, n_runs + 1 entries
+  const uint32_t* coarse;       // launch_hit_coarse over run_hit_off (optional)
+  int coarse_shift;
   const uint32_t* run_qstart;
   const uint32_t* run_rlo;
   const uint32_t* run_rcount;
@@ -101,6 +103,10 @@ struct JoinExpandArgs {
   uint32_t* hits4;  // 4 x u32 per hit
 };
 void launch_join_expand(const JoinExpandArgs& a, cudaStream_t st);
+// coarse[j] (j in [0, ceil(n_hits >> shift)]) = the run holding hit j << shift
+// (the last run for j past the hits): narrows each hit's run search.
+void launch_hit_coarse(const uint64_t* run_hit_off, uint64_t n_runs, int shift, uint64_t n_hits, uint32_t* coarse,
+                       cudaStream_t st);
 
 // ---- blastx front end (translate.cu) ----------------------------------------
 // Per (read, frame) entry i = 6 * read + frame; arrays of 6 * n_reads + 1

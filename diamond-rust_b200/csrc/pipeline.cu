@@ -1088,6 +1088,10 @@ void Search::join_chunk(uint64_t c0, uint64_t c1, uint64_t n_runs) {
   if (n_hits > 0) {
     JoinExpandArgs ja{};
     ja.run_hit_off = roff;
+    ja.coarse_shift = 7;  // one entry per 128 hits
+    uint32_t* coarse = c->hit_coarse.as<uint32_t>(((n_hits - 1) >> ja.coarse_shift) + 2);
+    launch_hit_coarse(roff, n_runs, ja.coarse_shift, n_hits, coarse, c->stream);
+    ja.coarse = coarse;
     ja.run_qstart = c->run_qstart.as<uint32_t>(0);
     ja.run_rlo = rlo;
     ja.run_rcount = rcnt;

@@ -413,11 +413,42 @@ void launch_join_count(const uint64_t* run_keys, const uint32_t* run_counts, uin
              first, shift);
 }
 
+// coarse[j] = the largest run u < n_runs with run_hit_off[u] <= j << shift,
+// for j in [0, nc]: the run of hit h lies in [coarse[h >> shift],
+// coarse[(h >> shift) + 1]].
+__global__ void k_hit_coarse(const uint64_t* __restrict__ run_hit_off, uint64_t n_runs, int shift, uint64_t nc,
+                             uint32_t* __restrict__ coarse) {
+  const uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (j > nc) return;
+  const uint64_t h = j << shift;
+  uint64_t lo = 0, hi = n_runs;  // run_hit_off[0] = 0 <= h
+  while (hi - lo > 1) {
+    const uint64_t m = (lo + hi) >> 1;
+    if (run_hit_off[m] <= h) lo = m;
+    else hi = m;
+  }
+  coarse[j] = (uint32_t)lo;
+}
+
+void launch_hit_coarse(const uint64_t* run_hit_off, uint64_t n_runs, int shift, uint64_t n_hits, uint32_t* coarse,
+                       cudaStream_t st) {
+  if (n_runs == 0 || n_hits == 0) return;
+  const uint64_t nc = ((n_hits - 1) >> shift) + 1;
+  count_launch();
+  k_hit_coarse<<<ceil_div((long long)nc + 1, 256), 256, 0, st>>>(run_hit_off, n_runs, shift, nc, coarse);
+  DRG_CUDA(cudaGetLastError());
+}
+
 __global__ void k_join_expand(JoinExpandArgs a) {
   uint64_t h = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (h >= a.n_hits) return;
   // run u: largest with run_hit_off[u] <= h
   uint64_t lo = 0, hi = a.n_runs;
+  if (a.coarse) {
+    const uint64_t j = h >> a.coarse_shift;
+    lo = a.coarse[j];
+    hi = min((uint64_t)a.coarse[j + 1] + 1, a.n_runs);
+  }
   while (hi - lo > 1) {
     uint64_t m = (lo + hi) >> 1;
     if (a.run_hit_off[m] <= h) lo = m;
