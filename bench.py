@@ -426,9 +426,11 @@ def main():
     gcups = cells_ref / (sw_ms / 1000.0) / 1e9 if sw_ms > 0 else 0.0
     launches = sum(s["kernel_launches"] for s in steps)
 
-    # ---- seed enumeration + sort + join (HBM-bound): algorithmic bytes per
-    # search = the letters read once per shape, each seed entry written and
-    # read once as 8 bytes, each hit written once as 16 bytes
+    # ---- seed enumeration + sort + join: bytes per search of an enumeration
+    # of every seed = the letters read once per shape, each seed entry written
+    # and read once as 8 bytes, each hit written once as 16 bytes (without an
+    # index the library keeps only the reference seeds its queries can join,
+    # so fewer bytes move than this counts)
     sl = steps[-1]
     S = int(sl["seed_shapes"])
     seed_bytes = (S * (int(do[-1]) + int(to[-1])) + 16 * (int(sl["ref_seeds"]) + int(sl["query_seeds"]))
@@ -442,7 +444,9 @@ def main():
                   "peak_source": "hbm_gbs of fallback" if measured_peaks().get("fallback")
                   else "MEASURED_PEAKS.json hbm_gbs (of measured)",
                   "what": "seed enumeration, radix sorts and the join of one search (stages seed + join + sort, "
-                          "device time incl. the host round trips that size each launch)"}
+                          "device time incl. the host round trips that size each launch); algorithmic_bytes "
+                          "counts every seed position's entry, of which only the reference seeds the queries "
+                          "can join are written"}
 
     # ---- very-sensitive (config 2's second preset), resident
     vs = None
