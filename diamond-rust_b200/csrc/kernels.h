@@ -311,8 +311,33 @@ struct ExactOut {
   uint32_t n_ops;
   uint64_t cells;
 };
-// scratch bytes a job needs (trace bytes + four int32 rows of max width)
-uint64_t exact_scratch_bytes(uint32_t n, uint32_t m, int32_t d0, int32_t d1, bool trace);
+// Sum over x = 0..X of min(x, m) (0 for X < 0).
+__host__ __device__ inline uint64_t exact_clamped_sum(int64_t X, uint64_t m) {
+  if (X < 0) return 0;
+  const uint64_t x = (uint64_t)X;
+  if (x <= m) return x * (x + 1) / 2;
+  return m * (m + 1) / 2 + (x - m) * m;
+}
+// Scratch bytes of one exact DP job: the trace bytes of the reference's row
+// ranges (gapped.rs:82-97, rows 0..n, columns clamp(i - d1 .. i - d0, 0, m)),
+// four int32 rows of the widest row, and in trace mode the reversed op bytes;
+// rounded up to 256.  The host sizes the scratch with it and the no-allocation
+// entry point lays jobs out on the device with it, so both must agree.
+// Lengths below 2^31 and diagonals within +-2^30 keep every term in 64 bits.
+__host__ __device__ inline uint64_t exact_scratch_bytes(uint32_t n, uint32_t m, int32_t d0, int32_t d1, bool trace) {
+  const int64_t lo_d = d0 < d1 ? d0 : d1, hi_d = d0 < d1 ? d1 : d0;
+  int64_t wmax = hi_d - lo_d + 1;
+  if (wmax > (int64_t)m + 1) wmax = (int64_t)m + 1;
+  uint64_t tb = 0;
+  if (trace) {
+    // sum over rows i of clamp(i - lo_d, 0, m) - clamp(i - hi_d, 0, m) + 1
+    const auto F = [&](int64_t a) { return exact_clamped_sum((int64_t)n - a, m) - exact_clamped_sum(-a - 1, m); };
+    tb = (uint64_t)n + 1 + F(lo_d) - F(hi_d);
+  }
+  uint64_t bytes = ((tb + 15) & ~15ull) + 4ull * 4ull * (uint64_t)wmax;
+  if (trace) bytes += (uint64_t)n + (uint64_t)m + 1;  // reversed op bytes
+  return (bytes + 255) & ~255ull;
+}
 // The substitution scores travel with each launch (no shared host state).
 void launch_sw_exact_with_matrix(const ExactJob* jobs, uint64_t n_jobs, int gap_open, int gap_extend, bool trace,
                                  uint8_t* scratch, uint32_t* ops, ExactOut* out, const int8_t* scores625,

@@ -1,26 +1,27 @@
 // gapped::extend_span with traceback for callers that must not allocate.
 //
-// Some callers cannot call cudaMalloc: code that runs while a CUDA graph is
-// being captured on its stream, services that own every byte of device memory
-// through their own pool and forbid allocations by libraries on the request
-// path, and real-time loops that may not take the allocator's locks or
-// latency.  drg_extend_span_noalloc gives them the exact banded
-// Smith-Waterman (the kernel behind drg_extend_span_batch) with every buffer
-// supplied by the caller, and its scratch in a fixed static device array:
+// Some callers cannot call cudaMalloc: services that own every byte of device
+// memory through their own pool and forbid allocations by libraries on the
+// request path, and real-time loops that may not take the allocator's locks
+// or wait for its latency.  drg_extend_span_noalloc gives them the exact
+// banded Smith-Waterman (the kernel behind drg_extend_span_batch) with every
+// buffer supplied by the caller, and its scratch in a fixed static device
+// array:
 //
 //  - the scratch is g_noalloc_scratch below, 32 MiB, present on every GPU that
 //    loads this library until the process exits;
 //  - a call whose bands need more than that is rejected (DRG_ERR_INVALID and
 //    a message saying how many bytes it needed) before any work is queued;
 //  - the first call on a device, with that device current, looks up the
-//    array's device address (cudaGetSymbolAddress); make that first call
-//    before any stream capture;
+//    array's device address (cudaGetSymbolAddress);
 //  - all calls share the one array, so calls whose work overlaps on the GPU
 //    (other streams, other host threads) race: order them on one stream or
 //    serialise them.  Nothing in the array has to start at zero: a call
 //    writes every byte it reads before reading it.
 // No cudaMalloc, cudaFree, host heap or library allocation is made here.
 #include <mutex>
+
+#include <cub/block/block_scan.cuh>
 
 #include "kernels.h"
 #include "host/scoring.h"
@@ -60,12 +61,23 @@ struct Layout {
   uint64_t jobs, q_off, s_off, exact_jobs, exact_out, dp, total;
 };
 
-// One block: per-job scratch needs, their prefix sums and the kernel's job
-// descriptors, built from the copies of the caller's host arrays.
-__global__ void k_noalloc_prepare(const drg_span_job* __restrict__ jobs, uint32_t n_jobs,
-                                  const uint64_t* __restrict__ q_off, const uint64_t* __restrict__ s_off,
-                                  const uint8_t* q_letters, const uint8_t* s_letters, ExactJob* __restrict__ out) {
-  for (uint32_t i = threadIdx.x; i < n_jobs; i += blockDim.x) {
+constexpr int kPrepThreads = 1024;
+
+// One block: the kernel's job descriptors and their scratch and op offsets,
+// built from the copies of the caller's host arrays.  Thread t takes a
+// contiguous run of jobs, so a block-wide exclusive scan of the threads'
+// totals gives each run its first offsets.
+__global__ void __launch_bounds__(kPrepThreads) k_noalloc_prepare(const drg_span_job* __restrict__ jobs,
+                                                                  uint32_t n_jobs, const uint64_t* __restrict__ q_off,
+                                                                  const uint64_t* __restrict__ s_off,
+                                                                  const uint8_t* q_letters, const uint8_t* s_letters,
+                                                                  ExactJob* __restrict__ out) {
+  using Scan = cub::BlockScan<uint64_t, kPrepThreads>;
+  __shared__ typename Scan::TempStorage tmp;
+  const uint32_t per = (n_jobs + kPrepThreads - 1) / kPrepThreads;
+  const uint32_t lo = min(n_jobs, threadIdx.x * per), hi = min(n_jobs, lo + per);
+  uint64_t scratch = 0, slots = 0;
+  for (uint32_t i = lo; i < hi; ++i) {
     const drg_span_job j = jobs[i];
     ExactJob e;
     e.q = q_letters + q_off[j.query];
@@ -74,33 +86,19 @@ __global__ void k_noalloc_prepare(const drg_span_job* __restrict__ jobs, uint32_
     e.m = (uint32_t)(s_off[j.subject + 1] - s_off[j.subject]);
     e.d0 = (int32_t)j.d0;
     e.d1 = (int32_t)j.d1;
-    // scratch bytes of the job: the trace bytes of every row, four int32 rows
-    // of the widest row and the reversed op bytes (same rule as the host's)
-    int64_t lo_d = e.d0 < e.d1 ? e.d0 : e.d1, hi_d = e.d0 < e.d1 ? e.d1 : e.d0;
-    int64_t wmax = hi_d - lo_d + 1;
-    if (wmax > (int64_t)e.m + 1) wmax = (int64_t)e.m + 1;
-    uint64_t tb = 0;
-    for (int64_t r = 0; r <= (int64_t)e.n; ++r) {
-      int64_t lo = r - hi_d, hi = r - lo_d;
-      lo = lo < 0 ? 0 : (lo > (int64_t)e.m ? (int64_t)e.m : lo);
-      hi = hi < 0 ? 0 : (hi > (int64_t)e.m ? (int64_t)e.m : hi);
-      tb += (uint64_t)(hi - lo + 1);
-    }
-    uint64_t bytes = ((tb + 15) & ~15ull) + 16ull * (uint64_t)wmax + (uint64_t)e.n + e.m + 1;
-    e.scratch_off = (bytes + 255) & ~255ull;  // size for now, offset after the scan
-    e.ops_off = (uint64_t)e.n + e.m;          // slots for now, offset after the scan
+    e.scratch_off = scratch;  // within the thread's run for now
+    e.ops_off = slots;
+    scratch += exact_scratch_bytes(e.n, e.m, e.d0, e.d1, true);
+    slots += (uint64_t)e.n + e.m;
     out[i] = e;
   }
+  uint64_t scratch0, slots0;
+  Scan(tmp).ExclusiveSum(scratch, scratch0);
   __syncthreads();
-  if (threadIdx.x == 0) {
-    uint64_t s = 0, o = 0;
-    for (uint32_t i = 0; i < n_jobs; ++i) {
-      uint64_t sz = out[i].scratch_off, ns = out[i].ops_off;
-      out[i].scratch_off = s;
-      out[i].ops_off = o;
-      s += sz;
-      o += ns;
-    }
+  Scan(tmp).ExclusiveSum(slots, slots0);
+  for (uint32_t i = lo; i < hi; ++i) {
+    out[i].scratch_off += scratch0;
+    out[i].ops_off += slots0;
   }
 }
 
@@ -160,7 +158,11 @@ extern "C" int drg_extend_span_noalloc(const uint8_t* d_q_letters, const uint64_
     if (j.query >= n_q || j.subject >= n_s) return fail(err, err_cap, DRG_ERR_INVALID, "job %llu: index out of range", i);
     if (j.d0 < INT32_MIN / 2 || j.d0 > INT32_MAX / 2 || j.d1 < INT32_MIN / 2 || j.d1 > INT32_MAX / 2)
       return fail(err, err_cap, DRG_ERR_INVALID, "job %llu: diagonal out of range", i);
+    if (q_offsets[j.query + 1] < q_offsets[j.query] || s_offsets[j.subject + 1] < s_offsets[j.subject])
+      return fail(err, err_cap, DRG_ERR_INVALID, "job %llu: offsets decrease", i);
     uint64_t n = q_offsets[j.query + 1] - q_offsets[j.query], m = s_offsets[j.subject + 1] - s_offsets[j.subject];
+    if (n >= (1ull << 31) || m >= (1ull << 31))
+      return fail(err, err_cap, DRG_ERR_INVALID, "job %llu: sequence longer than 2^31 letters", i);
     dp += exact_scratch_bytes((uint32_t)n, (uint32_t)m, (int32_t)j.d0, (int32_t)j.d1, true);
     ops += n + m;
   }
@@ -179,10 +181,20 @@ extern "C" int drg_extend_span_noalloc(const uint8_t* d_q_letters, const uint64_
     return fail(err, err_cap, DRG_ERR_INVALID, "call needs %llu bytes of scratch, the static scratch holds %llu",
                 (unsigned long long)L.total, (unsigned long long)kNoAllocScratchBytes);
   if (n_jobs == 0) return DRG_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  {
+    // the scratch address is the current device's, so the stream must be too
+    int cur = 0, sdev = 0;
+    cudaError_t ce = cudaGetDevice(&cur);
+    if (ce == cudaSuccess) ce = cudaStreamGetDevice(st, &sdev);
+    if (ce != cudaSuccess) return fail(err, err_cap, DRG_ERR_CUDA, "cannot query the stream's device (%llu)", ce);
+    if (sdev != cur)
+      return fail(err, err_cap, DRG_ERR_INVALID, "stream belongs to device %llu, the current device is %llu",
+                  (unsigned long long)sdev, (unsigned long long)cur);
+  }
   uint8_t* base = nullptr;
   cudaError_t ce = scratch_address(&base);
   if (ce != cudaSuccess) return fail(err, err_cap, DRG_ERR_CUDA, "cudaGetSymbolAddress failed (%llu)", (unsigned long long)ce);
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
   try {
     DRG_CUDA(cudaMemcpyAsync(base + L.jobs, jobs, n_jobs * sizeof(drg_span_job), cudaMemcpyHostToDevice, st));
     DRG_CUDA(cudaMemcpyAsync(base + L.q_off, q_offsets, (n_q + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
@@ -190,7 +202,7 @@ extern "C" int drg_extend_span_noalloc(const uint8_t* d_q_letters, const uint64_
     ExactJob* ej = reinterpret_cast<ExactJob*>(base + L.exact_jobs);
     ExactOut* eo = reinterpret_cast<ExactOut*>(base + L.exact_out);
     count_launch();
-    k_noalloc_prepare<<<1, 256, 0, st>>>(reinterpret_cast<const drg_span_job*>(base + L.jobs), (uint32_t)n_jobs,
+    k_noalloc_prepare<<<1, kPrepThreads, 0, st>>>(reinterpret_cast<const drg_span_job*>(base + L.jobs), (uint32_t)n_jobs,
                                          reinterpret_cast<const uint64_t*>(base + L.q_off),
                                          reinterpret_cast<const uint64_t*>(base + L.s_off), d_q_letters, d_s_letters,
                                          ej);

@@ -219,24 +219,6 @@ __global__ void k_sw_exact(const ExactJob* __restrict__ jobs, uint64_t n_jobs, i
 }
 }  // namespace
 
-uint64_t exact_scratch_bytes(uint32_t n, uint32_t m, int32_t d0, int32_t d1, bool trace) {
-  int64_t lo_d = d0 < d1 ? d0 : d1, hi_d = d0 < d1 ? d1 : d0;
-  int64_t wmax = hi_d - lo_d + 1;
-  if (wmax > (int64_t)m + 1) wmax = (int64_t)m + 1;
-  uint64_t tb = 0;
-  if (trace) {
-    for (int64_t i = 0; i <= (int64_t)n; ++i) {
-      int64_t lo = i - hi_d, hi = i - lo_d;
-      lo = lo < 0 ? 0 : (lo > (int64_t)m ? (int64_t)m : lo);
-      hi = hi < 0 ? 0 : (hi > (int64_t)m ? (int64_t)m : hi);
-      tb += (uint64_t)(hi - lo + 1);
-    }
-  }
-  uint64_t bytes = ((tb + 15) & ~15ull) + 4ull * 4ull * (uint64_t)wmax;
-  if (trace) bytes += (uint64_t)n + (uint64_t)m + 1;  // reversed op bytes
-  return (bytes + 255) & ~255ull;
-}
-
 void launch_sw_exact_with_matrix(const ExactJob* jobs, uint64_t n_jobs, int go, int ge, bool trace,
                                  uint8_t* scratch, uint32_t* ops, ExactOut* out, const int8_t* scores625,
                                  cudaStream_t st) {

@@ -174,18 +174,21 @@ int drg_extend_span_scores(drg_ctx* ctx, const uint8_t* q_letters, const uint64_
 
 /* gapped::extend_span with traceback, allocating nothing.  This entry point
  * has no counterpart in the reference; it exists for callers that cannot
- * allocate device memory (work recorded while a CUDA graph is being captured,
- * services whose own pool owns all device memory, real-time loops that may not
- * take allocator locks).  Results equal drg_extend_span_batch's.
+ * allocate device memory: services whose own pool owns all device memory and
+ * forbids library allocations on the request path, and real-time loops that
+ * may not take allocator locks.  Results equal drg_extend_span_batch's.
  *  - d_q_letters, d_s_letters: device letters; q_offsets, s_offsets, jobs:
- *    host arrays; d_out (n_jobs entries) and d_ops: device outputs.  Job i's
- *    ops start at d_out[i].ops_offset; d_ops needs sum(n + m) entries.
+ *    host arrays, copied to the device with cudaMemcpyAsync on `stream`
+ *    (pageable arrays may be reused once the call returns; page-locked ones
+ *    must stay unchanged until the stream has run the call's work); d_out
+ *    (n_jobs entries) and d_ops: device outputs.  Job i's ops start at
+ *    d_out[i].ops_offset; d_ops needs sum(n + m) entries.
  *  - Scratch is a static 32 MiB device array per GPU, kept until exit; calls
  *    needing more are rejected with DRG_ERR_INVALID and a message in err.
- *  - Work is queued on `stream` (a cudaStream_t); all calls share the scratch
- *    array, so calls that overlap on the GPU race.
+ *  - Work is queued on `stream` (a cudaStream_t of the current device); all
+ *    calls share the scratch array, so calls that overlap on the GPU race.
  *  - The first call on a device sets up the scratch address (with that device
- *    current); make it before any stream capture. */
+ *    current). */
 int drg_extend_span_noalloc(const uint8_t* d_q_letters, const uint64_t* q_offsets, uint64_t n_q,
                             const uint8_t* d_s_letters, const uint64_t* s_offsets, uint64_t n_s,
                             const drg_span_job* jobs, uint64_t n_jobs, const char* matrix, int32_t gap_open,

@@ -1,10 +1,10 @@
 """The allocation-free extend_span entry point (drg_extend_span_noalloc).
 
-Callers that cannot allocate device memory -- work recorded while a CUDA
-graph is captured, services whose own pool owns every device byte, real-time
-loops that may not take allocator locks -- use this entry point with buffers
-they already own.  This test is that caller: it owns the device buffers
-(through torch) and checks that two calls in a row give exactly what the
+Callers that cannot allocate device memory -- services whose own pool owns
+every device byte and forbids library allocations on the request path,
+real-time loops that may not take allocator locks -- use this entry point with
+buffers they already own.  This test is that caller: it owns the device
+buffers (through torch) and checks that calls in a row give exactly what the
 allocating entry point drg_extend_span_batch gives (exact integer results,
 tolerance 0).  It lives in its own file, collected last.
 """
@@ -29,16 +29,16 @@ def _bind():
     return fn
 
 
-def _cases(seed, n_cases):
+def _cases(seed, n_cases, max_len=300, halves=(5, 12, 30, 64)):
     r = np.random.Generator(np.random.PCG64(seed))
     queries, subjects, jobs = [], [], []
     for i in range(n_cases):
-        q = synth.random_protein(r, int(r.integers(1, 300)))
-        s = synth.mutate(r, q, float(r.uniform(0.3, 0.9))) if i % 2 else synth.random_protein(r, int(r.integers(1, 300)))
+        q = synth.random_protein(r, int(r.integers(1, max_len)))
+        s = synth.mutate(r, q, float(r.uniform(0.3, 0.9))) if i % 2 else synth.random_protein(r, int(r.integers(1, max_len)))
         if len(s) == 0:
             s = synth.random_protein(r, 5)
         d = int(r.integers(-len(s) + 1, len(q)))
-        half = int(r.choice([5, 12, 30, 64]))
+        half = int(r.choice(halves))
         queries.append(q)
         subjects.append(s)
         jobs.append((i, i, d - half, d + half))
@@ -82,8 +82,11 @@ def test_noalloc_matches_extend_span_batch_twice():
     fn = _bind()
     ctx = drgpu.Context(0)
     try:
-        for seed in (101, 102):  # two calls in a row share the static scratch
-            queries, subjects, jobs = _cases(seed, 120)
+        # calls in a row share the static scratch; the last has several jobs
+        # per thread of the one-block offset scan (1,024 threads)
+        for seed, n, mx, halves in ((101, 120, 300, (5, 12, 30, 64)), (102, 120, 300, (5, 12, 30, 64)),
+                                    (103, 2600, 60, (3, 8, 12))):
+            queries, subjects, jobs = _cases(seed, n, mx, halves)
             got = _noalloc(fn, queries, subjects, jobs)
             exp = ctx.extend_span(queries, subjects, jobs)
             assert got == exp
@@ -110,3 +113,20 @@ def test_noalloc_rejects_oversized_calls():
             ops.data_ptr(), len(jobs) * 10000, torch.cuda.current_stream().cuda_stream, err, 256)
     assert rc == 1
     assert b"static scratch" in err.value
+
+
+def test_noalloc_rejects_decreasing_offsets():
+    torch = pytest.importorskip("torch")
+    fn = _bind()
+    ql = np.full(64, 3, np.uint8)
+    qo = np.array([0, 40, 20, 64], np.uint64)  # sequence 1 would have a negative length
+    dq = torch.from_numpy(ql).cuda()
+    out = torch.zeros(C.sizeof(drgpu.Aligned), dtype=torch.uint8, device="cuda")
+    ops = torch.zeros(256, dtype=torch.int32, device="cuda")
+    ja = (drgpu.SpanJob * 1)(drgpu.SpanJob(1, 0, -3, 3))
+    err = C.create_string_buffer(256)
+    rc = fn(dq.data_ptr(), qo.ctypes.data_as(C.POINTER(C.c_uint64)), 3, dq.data_ptr(),
+            qo.ctypes.data_as(C.POINTER(C.c_uint64)), 3, ja, 1, b"BLOSUM62", -1, -1, out.data_ptr(),
+            ops.data_ptr(), 256, torch.cuda.current_stream().cuda_stream, err, 256)
+    assert rc == 1
+    assert b"offsets decrease" in err.value
