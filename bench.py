@@ -75,7 +75,7 @@ def workload(n_queries=None):
     return w
 
 
-def config_desc(w):
+def config_desc(w, world=1):
     return {
         "workload": f"{len(w.queries)} queries (lognormal mean 350, 50-1500 aa, 5 planted homologs each) x 7,860-sequence "
                     "synthetic DB, blastp --sensitive, BLOSUM62 11/1, evalue 1e-3, k 25, max-hsps 1, "
@@ -86,6 +86,7 @@ def config_desc(w):
         "db_letters": w.db_letters,
         "sensitivity": SENS,
         "l2": "flushed between timed steps (256 MiB write)",
+        "parallelism": f"replicas x{world}",
     }
 
 
@@ -342,6 +343,30 @@ def blastx_leg(ctx, steps, warmup, n_reads, cpu_sample, with_cpu):
     return out
 
 
+def full_batch_parity(ctx, db, batch, n_targets, presets):
+    """Every HSP of the timed batch (all queries, one search, the resident
+    entry point the bench times) against the oracle's answer for that same
+    batch (tests/golden/config2_<preset>.jsonl.gz).  The join cap counts query
+    seeds over the whole batch (seed.rs:120-127), so only the whole batch is
+    the timed search."""
+    import gzip
+    import drgpu
+    out = {}
+    for preset in presets:
+        path = os.path.join(ROOT, "tests", "golden", f"config2_{preset}.jsonl.gz")
+        exp = [[] for _ in range(n_targets)]
+        with gzip.open(path, "rb") as f:
+            for line in f.read().decode().splitlines():
+                row = json.loads(line)
+                exp[row[0]].append(tuple(row[1:17]) + (tuple(row[17]),))
+        cfg = drgpu.make_config(sensitivity=preset, index_chunks=1)
+        got = drgpu.search_resident(ctx, db, batch, cfg)[0]
+        got = [[h.key() for h in lst] for lst in got]
+        out[preset] = {"identical": got == exp, "hsps": sum(len(x) for x in exp),
+                       "targets_differing": sum(1 for a, b in zip(got, exp) if a != b)}
+    return out
+
+
 def cpu_sample_run(w, n_sample, threads):
     import pyoracle
     qs = w.queries[:n_sample]
@@ -369,7 +394,7 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
-            "data": "synthetic", "config": config_desc(w),
+            "data": "synthetic", "config": config_desc(w, world),
             "cpu_baseline": {"value": value, "unit": "queries/s", "cores": threads, "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -535,6 +560,14 @@ def main():
         got, _ = ctx.search(dl, do, stl, sto, cfg)
         parity = [[h.key() for h in x] for x in got] == exp
 
+    # ---- parity of the whole timed batch (both presets of the workload)
+    parity_full = None
+    if args.queries is None:
+        parity_full = full_batch_parity(ctx, db, batch, len(w.queries),
+                                        ["sensitive"] + ([] if args.no_very_sensitive else ["very-sensitive"]))
+        parity_full["batch"] = (f"the timed batch: all {len(w.queries)} queries x {len(w.db)} sequences as one "
+                                "search (drg_search_batch), every HSP field against the oracle's answer")
+
     batch.close()
     db.close()
     ctx.close()
@@ -544,7 +577,7 @@ def main():
             "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": job_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int16x2/int32", "data": "synthetic",
-            "config": dict(config_desc(w), parallelism=f"replicas x{world}"),
+            "config": config_desc(w, world),
             "gcups": gcups,
             "roofline": {"bound": "int", "kernel": "k_sw (banded SW score pass, packed s16x2 DPX)",
                          "achieved": gcups, "peak": peak_gcups, "unit": "GCUPS", "frac": gcups / peak_gcups,
@@ -578,9 +611,12 @@ def main():
             "gpu_launches": int(launches),
             "cpu_baseline": cpu,
             "parity_sample": parity,
+            "parity_full": parity_full,
             "clocks": clocks.summary(),
         }
         print(json.dumps(line), flush=True)
+    if parity_full and not all(v["identical"] for k, v in parity_full.items() if k != "batch"):
+        raise SystemExit("the timed batch's HSPs differ from the oracle's")
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

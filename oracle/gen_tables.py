@@ -10,13 +10,15 @@ Chebyshev coefficients for erfc.  They are read from the reference sources
   oracle/score_tables.inc                       (the CPU oracle's copy)
   diamond-rust_b200/csrc/host/score_tables.inc  (the product's copy)
 
-Usage: python oracle/gen_tables.py [REFERENCE_ROOT]
+Usage: python oracle/gen_tables.py REFERENCE_ROOT   (the diamond-rust source tree)
 """
 import os
 import re
 import sys
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit(__doc__)
+ref = sys.argv[1]
 here = os.path.dirname(os.path.abspath(__file__))
 repo = os.path.dirname(here)
 

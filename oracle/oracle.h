@@ -197,6 +197,7 @@ struct Target { size_t query; uint8_t frame; std::vector<uint8_t> letters; };
 struct RunStats {
   uint64_t query_seeds = 0, ref_seeds = 0, hits = 0, xdrops = 0, segments = 0, bands = 0, dp_cells = 0, hsps = 0;
   double t_seed_join = 0, t_align = 0;
+  uint64_t clipped_windows = 0;  // gapped_hsp windows clipped to max_rows (search.rs:303-312)
 };
 
 // search.rs:95-146.  Hit maps are built serially, targets aligned on `threads` threads.

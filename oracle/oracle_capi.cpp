@@ -47,6 +47,7 @@ struct orc_search_config {
 struct orc_run_stats {
   uint64_t query_seeds, ref_seeds, hits, xdrops, segments, bands, dp_cells, hsps;
   double t_seed_join, t_align;
+  uint64_t clipped_windows;
 };
 
 static thread_local std::string g_err;
@@ -389,6 +390,7 @@ int orc_search(const uint8_t* db_letters, const uint64_t* db_offsets, size_t n_d
     stats_out->hsps = rs.hsps;
     stats_out->t_seed_join = rs.t_seed_join;
     stats_out->t_align = rs.t_align;
+    stats_out->clipped_windows = rs.clipped_windows;
   }
   return 0;
 }

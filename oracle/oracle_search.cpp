@@ -53,12 +53,13 @@ struct DbAccess {
 std::optional<Hsp> gapped_hsp(const uint8_t* query, size_t qlen, const uint8_t* subject, size_t slen,
                               std::pair<size_t, size_t> anchor, std::pair<long, long> span, size_t band,
                               const SearchConfig& cfg, uint64_t db_letters, const Target& target, uint32_t sid,
-                              uint64_t* cells) {
+                              uint64_t* cells, uint64_t* clipped) {
   size_t row_cells = (size_t)std::max<long>(span.second - span.first, 0) + 1;
   size_t budget = 16000000;
   size_t max_rows = std::max(budget / row_cells, 2 * band + 16);
   size_t q0 = 0, q1 = qlen;
   if (q1 - q0 > max_rows) {
+    ++*clipped;  // test counter: windows clipped to max_rows query rows
     q0 = anchor.first >= max_rows / 2 ? anchor.first - max_rows / 2 : 0;
     q1 = std::min(q0 + max_rows, qlen);
     q0 = q1 >= max_rows ? q1 - max_rows : 0;
@@ -87,7 +88,7 @@ std::optional<Hsp> gapped_hsp(const uint8_t* query, size_t qlen, const uint8_t* 
 }
 
 struct TargetCounters {
-  uint64_t xdrops = 0, segments = 0, bands = 0, cells = 0, hsps = 0;
+  uint64_t xdrops = 0, segments = 0, bands = 0, cells = 0, hsps = 0, clipped = 0;
 };
 
 // search.rs:148-271
@@ -162,7 +163,7 @@ std::vector<Hsp> align_target(const DbAccess& db, const Target& target, const Hi
       ++tc->bands;
       const Segment& seg = segments[bd.best];
       auto hsp = gapped_hsp(query, qlen, subject, slen, {seg.q_start, seg.s_start}, {bd.d0, bd.d1}, band, cfg,
-                            db_letters, target, sid, &tc->cells);
+                            db_letters, target, sid, &tc->cells, &tc->clipped);
       if (!hsp) continue;
       if (hsp->evalue <= cfg.evalue) hsps.push_back(std::move(*hsp));
     }
@@ -238,6 +239,7 @@ std::vector<std::vector<Hsp>> run_impl(const DbAccess& db, const std::vector<Tar
     local.bands += c.bands;
     local.dp_cells += c.cells;
     local.hsps += c.hsps;
+    local.clipped_windows += c.clipped;
   }
   local.t_seed_join = std::chrono::duration<double>(t1 - t0).count();
   local.t_align = std::chrono::duration<double>(t2 - t1).count();

@@ -62,7 +62,8 @@ class _Cfg(C.Structure):
 class _Stats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in ("query_seeds", "ref_seeds", "hits", "xdrops", "segments", "bands",
                                           "dp_cells", "hsps")] + [("t_seed_join", C.c_double),
-                                                                  ("t_align", C.c_double)]
+                                                                  ("t_align", C.c_double),
+                                                                  ("clipped_windows", C.c_uint64)]
 
 
 _lib = None

@@ -110,3 +110,35 @@ def test_search_with_letter_codes_above_24(ctx, orc):
     got, exp, _, _ = run_both(ctx, orc, w, sensitivity="sensitive")
     assert got == exp
     assert sum(len(x) for x in exp) > 0
+
+
+def clip_workload():
+    """One 5,000-aa query whose single subject holds 30 copies of 20-aa query
+    pieces on diagonals 110 apart (-1650 .. +1540).  Each copy is an X-drop
+    segment; their +-64 windows (band_for(5000) = 64, gapped.rs:27-32) overlap,
+    so they merge into one band about 3,320 diagonals wide (search.rs:206-230).
+    Then max_rows = max(16e6 / width, 2 * 64 + 16) ~ 4,800 < 5,000 and
+    gapped_hsp clips the query rows around the anchor (search.rs:298-312)."""
+    r = np.random.Generator(np.random.PCG64(7117))
+    q = synth.random_protein(r, 5000)
+    s = synth.random_protein(r, 5000)
+    for k in range(30):
+        qk = 100 + 150 * k
+        d = -1650 + 110 * k
+        sk = qk - d
+        s[sk:sk + 20] = q[qk:qk + 20]
+    db = [synth.random_protein(r, int(x)) for x in r.integers(100, 600, 40)]
+    db.insert(17, s)
+    return q, db
+
+
+def test_search_window_clip(ctx, orc):
+    q, db = clip_workload()
+    dl, do = drgpu.concat(db)
+    tl, to = drgpu.concat([q])
+    for sens in ("default", "sensitive"):
+        got, _ = ctx.search(dl, do, tl, to, drgpu.make_config(sensitivity=sens))
+        exp, ostats = orc.search(db, [q], sensitivity=sens, threads=8)
+        assert ostats["clipped_windows"] > 0
+        assert as_tuples(got) == exp
+        assert any(h[1] == 17 for h in exp[0])

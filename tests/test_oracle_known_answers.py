@@ -5,7 +5,12 @@ The reference's README reports, for its bench/e2e data (7,860 proteins,
 --fast / --sensitive / --more-sensitive / --very-sensitive; under
 --sensitive WP_048121137.1 aligns over 612 columns at 91.7 bits; under
 --default WP_048121132.1 is reported at 26.2 % identity and 83.2 bits.
-These tests run where that data set is mounted and skip elsewhere.
+
+tests/golden/e2e_outfmt6.txt holds the oracle's tabular output on that data
+(made by tests/golden/make_e2e_golden.py); the published answers are checked
+on it everywhere.  Where the data set is mounted (DRG_REFERENCE_E2E = the
+reference's bench/e2e directory) the oracle is also re-run on it and must
+print exactly those lines.
 """
 import os
 import subprocess
@@ -14,10 +19,48 @@ import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE = os.path.join(ROOT, "oracle", "_build", "oracle")
-E2E = os.environ.get("DRG_REFERENCE_E2E", "/root/reference/bench/e2e")
+GOLDEN = os.path.join(ROOT, "tests", "golden", "e2e_outfmt6.txt")
+E2E = os.environ.get("DRG_REFERENCE_E2E")
+PRESETS = [("default", 4), ("fast", 1), ("sensitive", 7), ("more-sensitive", 7), ("very-sensitive", 7)]
 
-pytestmark = pytest.mark.skipif(not os.path.exists(os.path.join(E2E, "db_prot.fa")),
-                                reason="the reference's bench/e2e data is not mounted here")
+needs_data = pytest.mark.skipif(not E2E or not os.path.exists(os.path.join(E2E, "db_prot.fa")),
+                                reason="DRG_REFERENCE_E2E does not point at the reference's bench/e2e data")
+
+
+def golden():
+    blocks, cur = {}, None
+    with open(GOLDEN) as f:
+        for line in f.read().splitlines():
+            if line.startswith("# "):
+                cur = line[2:]
+                blocks[cur] = []
+            elif line:
+                blocks[cur].append(line.split("\t"))
+    return blocks
+
+
+@pytest.mark.parametrize("preset,hits", PRESETS)
+def test_hit_counts(preset, hits):
+    assert len(golden()[preset]) == hits
+
+
+def test_sensitive_612_columns():
+    r = {r[1]: r for r in golden()["sensitive"]}["WP_048121137.1"]
+    assert r[3] == "612"
+    assert r[11] == "91.7"
+
+
+def test_default_extra_hit():
+    r = {r[1]: r for r in golden()["default"]}["WP_048121132.1"]
+    assert r[2] == "26.2"
+    assert r[11] == "83.2"
+
+
+def test_diamond_evalues():
+    # the E-values DIAMOND 2.2.8 prints for the top --default hits (alp.rs:387-418)
+    ev = [r[10] for r in golden()["default"]]
+    assert ev[:2] == ["3.21e-105", "3.89e-25"]
+    assert "7.60e-17" in ev
 
 
 @pytest.fixture(scope="module")
@@ -30,30 +73,12 @@ def e2e_db(tmp_path_factory):
     return db
 
 
-def blastp(db, preset):
-    args = [ORACLE, "blastp", "-d", db, "-q", os.path.join(E2E, "query.fa"), "--quiet"]
+@needs_data
+@pytest.mark.parametrize("preset", [p for p, _ in PRESETS])
+def test_oracle_reproduces_golden(e2e_db, preset):
+    args = [ORACLE, "blastp", "-d", e2e_db, "-q", os.path.join(E2E, "query.fa"), "--quiet"]
     if preset != "default":
         args.append(f"--{preset}")
     r = subprocess.run(args, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr
-    return [line.split("\t") for line in r.stdout.splitlines()]
-
-
-@pytest.mark.parametrize("preset,hits", [("default", 4), ("fast", 1), ("sensitive", 7), ("more-sensitive", 7),
-                                         ("very-sensitive", 7)])
-def test_hit_counts(e2e_db, preset, hits):
-    assert len(blastp(e2e_db, preset)) == hits
-
-
-def test_sensitive_612_columns(e2e_db):
-    rows = {r[1]: r for r in blastp(e2e_db, "sensitive")}
-    r = rows["WP_048121137.1"]
-    assert r[3] == "612"
-    assert r[11] == "91.7"
-
-
-def test_default_extra_hit(e2e_db):
-    rows = {r[1]: r for r in blastp(e2e_db, "default")}
-    r = rows["WP_048121132.1"]
-    assert r[2] == "26.2"
-    assert r[11] == "83.2"
+    assert [line.split("\t") for line in r.stdout.splitlines()] == golden()[preset]
