@@ -102,7 +102,18 @@ void cub_run(drg_ctx* c, F f) {
   DRG_CUDA(f(t, bytes));
 }
 
-void sync(drg_ctx* c) { DRG_CUDA(cudaStreamSynchronize(c->stream)); }
+// Waits for the context's stream; a radix sort whose bounded wait gave up
+// since the last check makes the call fail.
+void sync(drg_ctx* c) {
+  uint32_t* d_err = c->sort_err.as<uint32_t>(1);
+  uint32_t* h = c->h_stage.as<uint32_t>(1);
+  DRG_CUDA(cudaMemcpyAsync(h, d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+  DRG_CUDA(cudaStreamSynchronize(c->stream));
+  if (*h) {
+    DRG_CUDA(cudaMemsetAsync(d_err, 0, sizeof(uint32_t), c->stream));
+    throw Error(DRG_ERR_TIMEOUT, "radix sort: a tile's bounded wait for an earlier tile gave up");
+  }
+}
 
 int cmp_hsp(const drg_hsp& a, const drg_hsp& b) {  // search.rs:273-282
   if (a.score != b.score) return b.score < a.score ? -1 : 1;
@@ -202,6 +213,45 @@ int drg_seed_chunks(uint64_t n, uint64_t parts, uint64_t* out_pairs, uint64_t* n
   return DRG_OK;
 }
 
+int drg_radix_sort(drg_ctx* c, void* keys, int32_t key_bytes, uint32_t* vals, uint64_t n, int32_t begin_bit,
+                   int32_t end_bit, int32_t count_on_device) {
+  if (!c || (n && !keys) || (key_bytes != 4 && key_bytes != 8) || begin_bit < 0 || end_bit < begin_bit ||
+      end_bit > 8 * key_bytes)
+    return DRG_ERR_INVALID;
+  API_BEGIN(c)
+  if (n >= (1ull << 30)) throw Error(DRG_ERR_INVALID, "radix sort: at most 2^30 - 1 keys");
+  // with the count on the device, the buffers hold a larger capacity (tiles
+  // past the count are never taken), as when a sort follows the kernel that
+  // counted its input
+  const uint64_t cap = count_on_device ? 2 * n + 5000 : n;
+  DevArr<uint8_t> k(cap * key_bytes), ka(cap * key_bytes);
+  DevArr<uint32_t> v(vals ? cap : 0), va(vals ? cap : 0);
+  DevArr<uint64_t> dn(1);
+  if (n) DRG_CUDA(cudaMemcpyAsync(k.p, keys, n * key_bytes, cudaMemcpyHostToDevice, c->stream));
+  if (n && vals) DRG_CUDA(cudaMemcpyAsync(v.p, vals, n * 4, cudaMemcpyHostToDevice, c->stream));
+  DRG_CUDA(cudaMemcpyAsync(dn.p, &n, sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
+  const uint64_t* d_n = count_on_device ? dn.p : nullptr;
+  void* rk;
+  uint32_t* rv;
+  if (key_bytes == 4) {
+    auto r = radix_sort<uint32_t>(reinterpret_cast<uint32_t*>(k.p), reinterpret_cast<uint32_t*>(ka.p),
+                                  vals ? v.p : nullptr, vals ? va.p : nullptr, cap, d_n, begin_bit, end_bit,
+                                  c->sort_tmp, c->sort_err.as<uint32_t>(1), c->stream);
+    rk = r.keys;
+    rv = r.vals;
+  } else {
+    auto r = radix_sort<uint64_t>(reinterpret_cast<uint64_t*>(k.p), reinterpret_cast<uint64_t*>(ka.p),
+                                  vals ? v.p : nullptr, vals ? va.p : nullptr, cap, d_n, begin_bit, end_bit,
+                                  c->sort_tmp, c->sort_err.as<uint32_t>(1), c->stream);
+    rk = r.keys;
+    rv = r.vals;
+  }
+  if (n) DRG_CUDA(cudaMemcpyAsync(keys, rk, n * key_bytes, cudaMemcpyDeviceToHost, c->stream));
+  if (n && vals) DRG_CUDA(cudaMemcpyAsync(vals, rv, n * 4, cudaMemcpyDeviceToHost, c->stream));
+  sync(c);
+  API_END(c)
+}
+
 int drg_seed_build(drg_ctx* c, const uint8_t* letters, const uint64_t* offsets, uint64_t n_seqs,
                    const char* shape_code, int32_t reduction, uint32_t base, double complexity_cut,
                    drg_seed_entry** out, uint64_t* n_out) {
@@ -234,14 +284,13 @@ int drg_seed_build(drg_ctx* c, const uint8_t* letters, const uint64_t* offsets, 
   DevArr<uint64_t> k(N), ks(N);
   DevArr<uint32_t> v(N), vs(N);
   launch_seed_enum(s.letters, s.offsets, s.owner, 0, s.total, 1, k.p, v.p, c->slot, c->stream);
-  cub_run(c, [&](void* tmp, size_t& b) {
-    return cub::DeviceRadixSort::SortPairs(tmp, b, k.p, ks.p, v.p, vs.p, (int64_t)N, 0, 64, c->stream);
-  });
+  const SortResult<uint64_t> sr = radix_sort<uint64_t>(k.p, ks.p, v.p, vs.p, N, nullptr, 0, 64, c->sort_tmp,
+                                                       c->sort_err.as<uint32_t>(1), c->stream);
   std::vector<uint64_t> hk(N);
   std::vector<uint32_t> hv(N);
   if (N) {
-    DRG_CUDA(cudaMemcpyAsync(hk.data(), ks.p, N * 8, cudaMemcpyDeviceToHost, c->stream));
-    DRG_CUDA(cudaMemcpyAsync(hv.data(), vs.p, N * 4, cudaMemcpyDeviceToHost, c->stream));
+    DRG_CUDA(cudaMemcpyAsync(hk.data(), sr.keys, N * 8, cudaMemcpyDeviceToHost, c->stream));
+    DRG_CUDA(cudaMemcpyAsync(hv.data(), sr.vals, N * 4, cudaMemcpyDeviceToHost, c->stream));
   }
   sync(c);
   uint64_t nv = 0;

@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "drgpu.h"
@@ -73,6 +74,10 @@ struct DevBuf {
   template <typename T>
   T* as(size_t n) {
     return static_cast<T*>(ensure(n * sizeof(T)));
+  }
+  void swap(DevBuf& o) {
+    std::swap(p, o.p);
+    std::swap(cap, o.cap);
   }
 };
 

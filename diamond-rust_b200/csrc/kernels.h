@@ -295,6 +295,27 @@ constexpr int kSwClasses = 4;
 int sw_width_class(int width);  // 0..3, or -1 for the exact kernel
 void launch_sw_class(const SwScoreArgs& a, int cls, cudaStream_t st);  // score mode
 
+// ---- device radix sort (radix_sort.cu) --------------------------------------
+// Where the sorted keys (and values) ended up: the LSD passes alternate between
+// the two buffers of each array.
+template <typename K>
+struct SortResult {
+  K* keys;
+  uint32_t* vals;
+};
+// Stable LSD sort of keys[0, n) by bits [begin_bit, end_bit), with optional u32
+// values (vals == nullptr: keys only).  n is *d_n when d_n is set (a count
+// written by an earlier launch; n_max bounds it and sizes the grids), else
+// n_max; n < 2^30.  keys_alt / vals_alt are buffers of the same capacity;
+// both buffers of each array are overwritten.  temp is the sort's scratch;
+// *d_err becomes non-zero if a tile's bounded wait for an earlier tile gave up
+// (the outputs are then not valid).  small_tiles: half the keys per tile.
+// No host wait.
+template <typename K>
+SortResult<K> radix_sort(K* keys, K* keys_alt, uint32_t* vals, uint32_t* vals_alt, uint64_t n_max,
+                         const uint64_t* d_n, int begin_bit, int end_bit, DevBuf& temp, uint32_t* d_err,
+                         cudaStream_t st, bool small_tiles = false);
+
 // ---- exact DP with traceback (sw_exact.cu) ----------------------------------
 struct ExactJob {
   const uint8_t* q;  // query window

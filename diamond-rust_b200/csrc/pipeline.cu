@@ -38,6 +38,14 @@ void cub_call(drg_ctx* c, F f) {
   DRG_CUDA(f(t, bytes));
 }
 
+// The library's radix sort on the context's stream (no host wait).
+template <typename K>
+SortResult<K> dsort(drg_ctx* c, K* k, K* k_alt, uint32_t* v, uint32_t* v_alt, uint64_t n, int begin_bit,
+                    int end_bit, const uint64_t* d_n = nullptr) {
+  return radix_sort<K>(k, k_alt, v, v_alt, n, d_n, begin_bit, end_bit, c->sort_tmp, c->sort_err.as<uint32_t>(1),
+                       c->stream);
+}
+
 template <typename T>
 T fetch(drg_ctx* c, const T* d) {
   T* h = c->h_stage.as<T>(1);
@@ -478,13 +486,11 @@ BandJobs make_band_jobs(drg_ctx* c, const uint32_t* order, const uint64_t* keys,
   count_launch();
   k_band_jobs<<<ceil_div(n, 256), 256, 0, c->stream>>>(order, keys, n, bc, s_offsets, trace, jobs_u, key, val,
                                                        dmaxw);
-  cub_call(c, [&](void* t, size_t& b) {
-    return cub::DeviceRadixSort::SortPairs(t, b, key, key_s, val, val_s, (int64_t)n, 0, kCostBits + 3, c->stream);
-  });
+  const uint32_t* val_sorted = dsort(c, key, key_s, val, val_s, n, 0, kCostBits + 3).vals;
   uint64_t* size = c->bj_size.as<uint64_t>(n + 1);
   uint64_t* off = c->bj_off.as<uint64_t>(n + 1);
   count_launch();
-  k_gather_band_jobs<<<ceil_div(n + 1, 256), 256, 0, c->stream>>>(jobs_u, val_s, n, r.jobs, size);
+  k_gather_band_jobs<<<ceil_div(n + 1, 256), 256, 0, c->stream>>>(jobs_u, val_sorted, n, r.jobs, size);
   if (trace) {
     cub_call(c, [&](void* t, size_t& b) {
       return cub::DeviceScan::ExclusiveSum(t, b, size, off, (int64_t)n + 1, c->stream);
@@ -541,7 +547,7 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
   uint64_t* swk = c->sw_keys.as<uint64_t>(n_bands);
   uint64_t* swks = c->sw_keys_s.as<uint64_t>(n_bands);
   uint32_t* swo = c->sw_order.as<uint32_t>(n_bands);
-  uint32_t* swos = c->sw_order_s.as<uint32_t>(n_bands);
+  uint32_t* swos = c->sw_order_s.as<uint32_t>(n_bands);  // sorted keys and order: where the sorts leave them
   uint32_t* rows = c->sw_rows.as<uint32_t>(n_bands);
   uint32_t* rows_s = c->sw_rows_s.as<uint32_t>(n_bands);
   uint64_t* swk_r = c->sw_keys_r.as<uint64_t>(n_bands);
@@ -560,14 +566,14 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
   k_sw_keys<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(bc, n_bands, s.offsets, scr.max_score, tr_count, swk,
                                                            rows, swo);
   // rows first, then a stable sort by (target, window, width)
-  cub_call(c, [&](void* t, size_t& b) {
-    return cub::DeviceRadixSort::SortPairs(t, b, rows, rows_s, swo, swo_r, (int64_t)n_bands, 0, 32, c->stream);
-  });
+  uint32_t* by_rows = dsort(c, rows, rows_s, swo, swo_r, n_bands, 0, 32).vals;
   count_launch();
-  k_gather_keys<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(swk, swo_r, n_bands, swk_r);
-  cub_call(c, [&](void* t, size_t& b) {
-    return cub::DeviceRadixSort::SortPairs(t, b, swk_r, swks, swo_r, swos, (int64_t)n_bands, kKeyLo, 64, c->stream);
-  });
+  k_gather_keys<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(swk, by_rows, n_bands, swk_r);
+  {
+    const SortResult<uint64_t> r = dsort(c, swk_r, swks, by_rows, swos, n_bands, kKeyLo, 64);
+    swks = r.keys;
+    swos = r.vals;
+  }
   uint64_t n_fast = 0, n_narrow = 0;
   {
     count_launch();
@@ -636,12 +642,9 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
                                                                       s.offsets, false, tasks_u, tkey, tval, nullptr,
                                                                       cells_gpu);
       // by width class, longest warps first within a class
-      cub_call(c, [&](void* t, size_t& b) {
-        return cub::DeviceRadixSort::SortPairs(t, b, tkey, tkey_s, tval, tval_s, (int64_t)n_tasks, 0, kCostBits + 2,
-                                               c->stream);
-      });
+      const uint32_t* task_order = dsort(c, tkey, tkey_s, tval, tval_s, n_tasks, 0, kCostBits + 2).vals;
       count_launch();
-      k_gather_tasks<<<ceil_div(n_tasks, 256), 256, 0, c->stream>>>(tasks_u, tval_s, n_tasks, tasks);
+      k_gather_tasks<<<ceil_div(n_tasks, 256), 256, 0, c->stream>>>(tasks_u, task_order, n_tasks, tasks);
       // task_max holds the per-class step maxima, then the class bounds
       int64_t* dbounds = reinterpret_cast<int64_t*>(c->task_max.as<unsigned long long>(2 * kSwClasses)) + kSwClasses;
       count_launch();
@@ -908,9 +911,15 @@ void Search::query_seeds(uint64_t* n_runs_out) {
   uint32_t* vals_s = c->q_vals_s.as<uint32_t>(N);
   launch_seed_enum(q->letters, q->offsets, q->owner, 0, q->total, S, keys, vals, c->slot, c->stream, q->request);
   const int key_bits = q->request ? 64 : seed_key_bits;  // request ids sit above the seed key
-  cub_call(c, [&](void* t, size_t& b) {
-    return cub::DeviceRadixSort::SortPairs(t, b, keys, keys_s, vals, vals_s, (int64_t)N, 0, key_bits, c->stream);
-  });
+  {
+    // the sorted seeds stay in q_keys_s / q_vals_s (the join reads them there)
+    const SortResult<uint64_t> r = dsort(c, keys, keys_s, vals, vals_s, N, 0, key_bits);
+    if (r.keys != keys_s) {
+      c->q_keys.swap(c->q_keys_s);
+      c->q_vals.swap(c->q_vals_s);
+      keys_s = r.keys;
+    }
+  }
   // runs of every key (the "no seed" keys, last, form one run of their own),
   // then the valid keys and their runs counted in one kernel: one wait
   uint64_t* rk = c->run_keys.as<uint64_t>(N + 1);
@@ -1017,14 +1026,15 @@ void Search::join_chunk(uint64_t c0, uint64_t c1, uint64_t n_runs) {
     nr = (int64_t)h[0];
     n_valid = h[1];
     if (nr > 0) {
-      if (key32)
-        cub_call(c, [&](void* t, size_t& b) {
-          return cub::DeviceRadixSort::SortPairs(t, b, k32, ks32, vals, vs, nr, 0, seed_key_bits, c->stream);
-        });
-      else
-        cub_call(c, [&](void* t, size_t& b) {
-          return cub::DeviceRadixSort::SortPairs(t, b, k64, ks64, vals, vs, nr, 0, seed_key_bits, c->stream);
-        });
+      if (key32) {
+        const SortResult<uint32_t> r = dsort(c, k32, ks32, vals, vs, (uint64_t)nr, 0, seed_key_bits);
+        ks32 = r.keys;
+        vs = r.vals;
+      } else {
+        const SortResult<uint64_t> r = dsort(c, k64, ks64, vals, vs, (uint64_t)nr, 0, seed_key_bits);
+        ks64 = r.keys;
+        vs = r.vals;
+      }
     }
     keys_s = ks64;
     keys32_s = ks32;
@@ -1036,18 +1046,18 @@ void Search::join_chunk(uint64_t c0, uint64_t c1, uint64_t n_runs) {
       uint32_t* keys = c->r_keys.as<uint32_t>(N);
       uint32_t* ks = c->r_keys_s.as<uint32_t>(N);
       launch_seed_enum(db->letters, db->offsets, db->owner + lo, lo, hi, S, keys, vals, c->slot, c->stream);
-      cub_call(c, [&](void* t, size_t& b) {
-        return cub::DeviceRadixSort::SortPairs(t, b, keys, ks, vals, vs, (int64_t)N, 0, seed_key_bits, c->stream);
-      });
+      const SortResult<uint32_t> r = dsort(c, keys, ks, vals, vs, N, 0, seed_key_bits);
+      ks = r.keys;
+      vs = r.vals;
       nr = count_valid(c, ks, N, d_count);
       keys32_s = ks;
     } else {
       uint64_t* keys = c->r_keys.as<uint64_t>(N);
       uint64_t* ks = c->r_keys_s.as<uint64_t>(N);
       launch_seed_enum(db->letters, db->offsets, db->owner + lo, lo, hi, S, keys, vals, c->slot, c->stream);
-      cub_call(c, [&](void* t, size_t& b) {
-        return cub::DeviceRadixSort::SortPairs(t, b, keys, ks, vals, vs, (int64_t)N, 0, seed_key_bits, c->stream);
-      });
+      const SortResult<uint64_t> r = dsort(c, keys, ks, vals, vs, N, 0, seed_key_bits);
+      ks = r.keys;
+      vs = r.vals;
       nr = count_valid(c, ks, N, d_count);
       keys_s = ks;
     }
@@ -1122,9 +1132,7 @@ void Search::process_hits(uint64_t pass_id) {
   tm.start();
   uint64_t* hs = c->hits_s.as<uint64_t>(n_hits);
   uint64_t* hu = c->hits_u.as<uint64_t>(n_hits);
-  cub_call(c, [&](void* t, size_t& b) {
-    return cub::DeviceRadixSort::SortKeys(t, b, hk, hs, (int64_t)n_hits, 0, L.total(), c->stream);
-  });
+  hs = dsort<uint64_t>(c, const_cast<uint64_t*>(hk), hs, nullptr, nullptr, n_hits, 0, L.total()).keys;
   cub_call(c, [&](void* t, size_t& b) {
     return cub::DeviceSelect::Unique(t, b, hs, hu, d_count, (int64_t)n_hits, c->stream);
   });
@@ -1448,6 +1456,7 @@ void Search::run(drg_result* out) {
   d_count = c->counters.as<int64_t>(9);
   d_counters = reinterpret_cast<unsigned long long*>(d_count + 2);
   DRG_CUDA(cudaMemsetAsync(d_count, 0, 9 * sizeof(int64_t), c->stream));
+  DRG_CUDA(cudaMemsetAsync(c->sort_err.as<uint32_t>(1), 0, sizeof(uint32_t), c->stream));
   if (q->n == 0 || db->n == 0) {
     out->n_targets = q->n;
     out->target_offsets = (uint64_t*)std::calloc(q->n + 1, sizeof(uint64_t));
@@ -1476,8 +1485,11 @@ void Search::run(drg_result* out) {
   finish(out);
   total.stop(&st.ms_total);
   unsigned long long cnt[7];
+  uint32_t sort_err = 0;
   DRG_CUDA(cudaMemcpyAsync(cnt, d_counters, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
+  DRG_CUDA(cudaMemcpyAsync(&sort_err, c->sort_err.as<uint32_t>(1), sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
   DRG_CUDA(cudaStreamSynchronize(c->stream));
+  if (sort_err) throw Error(DRG_ERR_TIMEOUT, "radix sort: a tile's bounded wait for an earlier tile gave up");
   times.resolve();
   st.xdrops = cnt[0];
   st.dp_cells_ref = cnt[1];

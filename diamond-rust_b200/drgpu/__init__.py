@@ -123,6 +123,8 @@ _SIGNATURES = {
     "drg_seed_join": (C.c_int, [C.c_void_p, _P(SeedEntry), C.c_uint64, _P(SeedEntry), C.c_uint64, C.c_uint64,
                                 C.c_uint64, _P(_P(SeedHit)), _u64p]),
     "drg_seed_chunks": (C.c_int, [C.c_uint64, C.c_uint64, _u64p, _u64p]),
+    "drg_radix_sort": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, _u32p, C.c_uint64, C.c_int32, C.c_int32,
+                                 C.c_int32]),
     "drg_xdrop_batch": (C.c_int, [C.c_void_p, _u8p, _u64p, C.c_uint64, _u8p, _u64p, C.c_uint64, _P(XdropJob),
                                   C.c_uint64, C.c_char_p, C.c_int32, _P(Segment)]),
     "drg_extend_span_batch": (C.c_int, [C.c_void_p, _u8p, _u64p, C.c_uint64, _u8p, _u64p, C.c_uint64,
@@ -309,6 +311,20 @@ class Context:
                        dtype=[("key", "u8"), ("seq", "u4"), ("pos", "u4")])
         self.lib.drg_free(out)
         return arr
+
+    def radix_sort(self, keys, vals=None, begin_bit=0, end_bit=None, count_on_device=False):
+        """The device radix sort (stable) of u32 or u64 keys, with optional
+        u32 values; returns sorted copies."""
+        k = np.ascontiguousarray(keys).copy()
+        if k.dtype not in (np.uint32, np.uint64):
+            raise TypeError("keys must be uint32 or uint64")
+        v = None if vals is None else np.ascontiguousarray(vals, dtype=np.uint32).copy()
+        kb = k.dtype.itemsize
+        eb = 8 * kb if end_bit is None else end_bit
+        self._check(self.lib.drg_radix_sort(self.h, k.ctypes.data_as(C.c_void_p), kb,
+                                            None if v is None else v.ctypes.data_as(_u32p), len(k), begin_bit, eb,
+                                            int(count_on_device)))
+        return k, v
 
     def seed_join(self, q_entries, r_entries, n_targets: int, max_expand: int = 4096):
         def to_c(e):

@@ -149,6 +149,16 @@ int drg_seed_build(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offsets
 int drg_seed_join(drg_ctx* ctx, const drg_seed_entry* query, uint64_t n_query, const drg_seed_entry* ref,
                   uint64_t n_ref, uint64_t n_targets, uint64_t max_expand, drg_seed_hit** out, uint64_t* n_out);
 
+/* The device radix sort behind seed::build's key sort (seed.rs:102,
+ * sort_unstable_by_key) and align_target's hit sort (search.rs:178), from host
+ * buffers: keys (key_bytes 4 or 8) and, when vals is not NULL, u32 values are
+ * sorted in place by bits [begin_bit, end_bit) of the key, stably (equal keys
+ * keep their order).  n < 2^30.  count_on_device = 1 hands the sort its count
+ * in device memory, as the search does when a sort follows the kernel that
+ * counted its input. */
+int drg_radix_sort(drg_ctx* ctx, void* keys, int32_t key_bytes, uint32_t* vals, uint64_t n, int32_t begin_bit,
+                   int32_t end_bit, int32_t count_on_device);
+
 /* seed::chunks (seed.rs:146-164): up to `parts` (start, end) pairs. */
 int drg_seed_chunks(uint64_t n, uint64_t parts, uint64_t* out_pairs, uint64_t* n_out);
 
