@@ -49,23 +49,49 @@ void launch_seed_enum_filtered(const uint8_t* letters, const uint64_t* offsets, 
 constexpr uint64_t kNoSeed = ~0ull;
 constexpr uint32_t kMaxRequests = 65535;  // request ids of one batch
 
+// A block of the query batch: the targets whose letters lie in [lo, hi).  A
+// query key run's entries are in ascending letter order (the key sort is
+// stable over the enumeration order), so a block's entries of a run are one
+// contiguous sub-range; the join finds it by binary search, tests the
+// expansion cap on the count of the whole run (the reference counts a key's
+// query occurrences over every target of the run, seed.rs:120-127) and
+// expands only the block's entries.
+struct JoinBlock {
+  const uint32_t* q_vals;      // sorted query entry payloads (letter indices)
+  const uint32_t* run_qstart;  // first entry of each run
+  uint64_t lo, hi;             // letters of the block
+  uint32_t* run_qlo;           // out: first entry of the block in each run
+  uint32_t* run_qcount;        // out: entries of the block in each run
+};
 // For each query run u (unique key, count, start): the reference run [lo, hi)
 // with the same key (query key & key_mask) and the number of hits it yields
 // under the expansion cap.
 // With `first` (launch_bucket_first over the same reference keys), each
 // search covers one bucket of keys sharing their bits above `shift`.
+// With `blk`, hits count only the block's entries of each run.  With
+// d_n_ref, n_ref is *d_n_ref (a count an earlier launch wrote).
 void launch_join_count(const uint64_t* run_keys, const uint32_t* run_counts, uint64_t n_runs,
                        const uint64_t* ref_keys, uint64_t n_ref, uint64_t max_expand, uint32_t* run_rlo,
                        uint32_t* run_rcount, uint64_t* run_hits, uint64_t key_mask, cudaStream_t st,
-                       const uint32_t* first = nullptr, int shift = 0);
+                       const uint32_t* first = nullptr, int shift = 0, const JoinBlock* blk = nullptr,
+                       const uint64_t* d_n_ref = nullptr);
 void launch_join_count(const uint64_t* run_keys, const uint32_t* run_counts, uint64_t n_runs,
                        const uint32_t* ref_keys, uint64_t n_ref, uint64_t max_expand, uint32_t* run_rlo,
                        uint32_t* run_rcount, uint64_t* run_hits, uint64_t key_mask, cudaStream_t st,
-                       const uint32_t* first = nullptr, int shift = 0);
+                       const uint32_t* first = nullptr, int shift = 0, const JoinBlock* blk = nullptr,
+                       const uint64_t* d_n_ref = nullptr);
+// target_hits[t] += hits the join gives target t (runs that pass the cap,
+// after launch_join_count without a block): sizes the query blocks.
+void launch_target_hits(const uint32_t* run_counts, const uint32_t* run_qstart, const uint32_t* run_rcount,
+                        const uint64_t* run_hits, uint64_t n_runs, const uint32_t* q_vals, const uint32_t* q_owner,
+                        unsigned long long* target_hits, cudaStream_t st);
 // first[b] (b in [0, nb]) = index of the first of n sorted keys whose
 // key >> shift is at least b; first[nb] = n.  Keys must be below nb << shift.
-void launch_bucket_first(const uint64_t* keys, uint64_t n, int shift, uint32_t nb, uint32_t* first, cudaStream_t st);
-void launch_bucket_first(const uint32_t* keys, uint64_t n, int shift, uint32_t nb, uint32_t* first, cudaStream_t st);
+// With d_n, n is *d_n (a count an earlier launch wrote).
+void launch_bucket_first(const uint64_t* keys, uint64_t n, int shift, uint32_t nb, uint32_t* first, cudaStream_t st,
+                         const uint64_t* d_n = nullptr);
+void launch_bucket_first(const uint32_t* keys, uint64_t n, int shift, uint32_t nb, uint32_t* first, cudaStream_t st,
+                         const uint64_t* d_n = nullptr);
 
 // Layout of the packed 64-bit hit key (target, subject, diag + doff, spos).
 struct HitKeyLayout {

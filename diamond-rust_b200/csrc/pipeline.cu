@@ -112,6 +112,7 @@ int64_t count_valid(drg_ctx* c, const K* keys, uint64_t n, int64_t* d_tmp) {
 }
 
 __global__ void k_set_u64(uint64_t* p, uint64_t v) { *p = v; }
+__global__ void k_add_u64(unsigned long long* p, const unsigned long long* v) { *p += *v; }
 __global__ void k_set_u32(uint32_t* p, uint32_t v) { *p = v; }
 
 __global__ void k_rank0_flags(const Band* b, uint64_t n, uint8_t* f) {
@@ -798,12 +799,15 @@ struct Search {
   double evalue = 1e-3;
   uint64_t max_hsps = 1, max_targets = 25;
   uint64_t host_threads = 0;  // 0: all of the context's host threads
+  uint64_t hit_budget = 1ull << 28;  // hits held before the stages after the join run
+  uint64_t pass = 0;                 // passes of those stages so far
+  uint64_t query_blocks = 0;         // blocks the batch was joined in (over all chunks)
   drg_run_stats st{};
   std::vector<Candidate> cands;
   // device scratch for counters
   int64_t* d_count = nullptr;
   // [0] xdrops [1] cells_ref [2] computed [3] cells_gpu [4] lane cells [5] issued cells
-  // [6] transposed bands
+  // [6] transposed bands [7] valid reference seeds of chunks enumerated without an index
   unsigned long long* d_counters = nullptr;
   TimeLog times;  // stage times, read after the search's last wait
 
@@ -821,6 +825,7 @@ struct Search {
     max_hsps = std::max<uint32_t>(cfg->max_hsps, 1);
     max_targets = std::max<uint32_t>(cfg->max_target_seqs, 1);
     host_threads = cfg->threads;
+    hit_budget = cfg->max_hits_per_pass ? cfg->max_hits_per_pass : (1ull << 28);
     if ((int)shapes.size() > kMaxShapes) throw Error(DRG_ERR_INVALID, "too many seed shapes");
     ShapeTable t{};
     t.n = (int)shapes.size();
@@ -990,8 +995,9 @@ void Search::join_chunk(uint64_t c0, uint64_t c1, uint64_t n_runs) {
   const uint64_t* keys_s = nullptr;
   const uint32_t* keys32_s = nullptr;
   const uint32_t* vals_s;
-  int64_t nr;             // reference seeds the join reads
-  uint64_t n_valid = 0;   // valid reference seeds of the chunk
+  int64_t nr;             // reference seeds the join reads (a bound when d_nr is set)
+  const uint64_t* d_nr = nullptr;  // their count on the device, when the host does not know it
+  uint64_t n_valid = 0;   // valid reference seeds of the chunk (counted on the device when d_nr is set)
   if (held) {
     keys_s = held->keys;
     keys32_s = held->keys32;
@@ -1021,20 +1027,20 @@ void Search::join_chunk(uint64_t c0, uint64_t c1, uint64_t n_runs) {
       launch_seed_enum_filtered(db->letters, db->offsets, db->owner + lo, lo, hi, S, key_filter, key_filter_log2, k64,
                                 vals, cnt, c->slot, c->stream);
     }
-    std::vector<unsigned long long> h;
-    fetch_n(c, h, cnt, 2);
-    nr = (int64_t)h[0];
-    n_valid = h[1];
-    if (nr > 0) {
-      if (key32) {
-        const SortResult<uint32_t> r = dsort(c, k32, ks32, vals, vs, (uint64_t)nr, 0, seed_key_bits);
-        ks32 = r.keys;
-        vs = r.vals;
-      } else {
-        const SortResult<uint64_t> r = dsort(c, k64, ks64, vals, vs, (uint64_t)nr, 0, seed_key_bits);
-        ks64 = r.keys;
-        vs = r.vals;
-      }
+    // the kept count stays on the device: the sort, the bucket starts and the
+    // join read it there (no host wait); the valid count joins the counters
+    d_nr = reinterpret_cast<const uint64_t*>(cnt);
+    nr = (int64_t)N;  // capacity
+    count_launch();
+    k_add_u64<<<1, 1, 0, c->stream>>>(d_counters + 7, cnt + 1);
+    if (key32) {
+      const SortResult<uint32_t> r = dsort(c, k32, ks32, vals, vs, N, 0, seed_key_bits, d_nr);
+      ks32 = r.keys;
+      vs = r.vals;
+    } else {
+      const SortResult<uint64_t> r = dsort(c, k64, ks64, vals, vs, N, 0, seed_key_bits, d_nr);
+      ks64 = r.keys;
+      vs = r.vals;
     }
     keys_s = ks64;
     keys32_s = ks32;
@@ -1077,47 +1083,102 @@ void Search::join_chunk(uint64_t c0, uint64_t c1, uint64_t n_runs) {
   const uint32_t nb = 1u << bucket_bits;
   uint32_t* first = c->ref_first.as<uint32_t>(nb + 1);
   if (keys32_s) {
-    launch_bucket_first(keys32_s, (uint64_t)nr, shift, nb, first, c->stream);
+    launch_bucket_first(keys32_s, (uint64_t)nr, shift, nb, first, c->stream, d_nr);
     launch_join_count(c->run_keys.as<uint64_t>(0), c->run_counts.as<uint32_t>(0), n_runs, keys32_s, (uint64_t)nr,
-                      4096, rlo, rcnt, rhits, (1ull << seed_key_bits) - 1, c->stream, first, shift);
+                      4096, rlo, rcnt, rhits, (1ull << seed_key_bits) - 1, c->stream, first, shift, nullptr, d_nr);
   } else {
-    launch_bucket_first(keys_s, (uint64_t)nr, shift, nb, first, c->stream);
+    launch_bucket_first(keys_s, (uint64_t)nr, shift, nb, first, c->stream, d_nr);
     launch_join_count(c->run_keys.as<uint64_t>(0), c->run_counts.as<uint32_t>(0), n_runs, keys_s, (uint64_t)nr, 4096,
-                      rlo, rcnt, rhits, (1ull << seed_key_bits) - 1, c->stream, first, shift);
+                      rlo, rcnt, rhits, (1ull << seed_key_bits) - 1, c->stream, first, shift, nullptr, d_nr);
   }
-  count_launch();
-  k_set_u64<<<1, 1, 0, c->stream>>>(rhits + n_runs, 0);
-  cub_call(c, [&](void* t, size_t& b) {
-    return cub::DeviceScan::ExclusiveSum(t, b, rhits, roff, (int64_t)n_runs + 1, c->stream);
-  });
-  const uint64_t n_hits = fetch(c, roff + n_runs);
-  st.hits += n_hits;
-  const HitKeyLayout L = layout();
-  acc_reserve(acc_n + n_hits);
-  uint64_t* hk = acc + acc_n;
-  if (n_hits > 0) {
-    JoinExpandArgs ja{};
-    ja.run_hit_off = roff;
-    ja.coarse_shift = 7;  // one entry per 128 hits
-    uint32_t* coarse = c->hit_coarse.as<uint32_t>(((n_hits - 1) >> ja.coarse_shift) + 2);
-    launch_hit_coarse(roff, n_runs, ja.coarse_shift, n_hits, coarse, c->stream);
-    ja.coarse = coarse;
-    ja.run_qstart = c->run_qstart.as<uint32_t>(0);
-    ja.run_rlo = rlo;
-    ja.run_rcount = rcnt;
-    ja.n_runs = n_runs;
-    ja.q_vals = c->q_vals_s.as<uint32_t>(0);
-    ja.r_vals = vals_s;
-    ja.n_hits = n_hits;
-    ja.q_owner = q->owner;
-    ja.q_offsets = q->offsets;
-    ja.r_owner = db->owner;
-    ja.r_offsets = db->offsets;
-    ja.layout = L;
-    ja.hit_keys = hk;
-    launch_join_expand(ja, c->stream);
+  // hits of the runs' entries in [qstart, +count) (all, or one block's)
+  auto scan_hits = [&]() {
+    count_launch();
+    k_set_u64<<<1, 1, 0, c->stream>>>(rhits + n_runs, 0);
+    cub_call(c, [&](void* t, size_t& b) {
+      return cub::DeviceScan::ExclusiveSum(t, b, rhits, roff, (int64_t)n_runs + 1, c->stream);
+    });
+    return fetch(c, roff + n_runs);
+  };
+  auto expand = [&](uint64_t n_hits, const uint32_t* qstart) {
+    st.hits += n_hits;
+    acc_reserve(acc_n + n_hits);
+    if (n_hits > 0) {
+      JoinExpandArgs ja{};
+      ja.run_hit_off = roff;
+      ja.coarse_shift = 7;  // one entry per 128 hits
+      uint32_t* coarse = c->hit_coarse.as<uint32_t>(((n_hits - 1) >> ja.coarse_shift) + 2);
+      launch_hit_coarse(roff, n_runs, ja.coarse_shift, n_hits, coarse, c->stream);
+      ja.coarse = coarse;
+      ja.run_qstart = qstart;
+      ja.run_rlo = rlo;
+      ja.run_rcount = rcnt;
+      ja.n_runs = n_runs;
+      ja.q_vals = c->q_vals_s.as<uint32_t>(0);
+      ja.r_vals = vals_s;
+      ja.n_hits = n_hits;
+      ja.q_owner = q->owner;
+      ja.q_offsets = q->offsets;
+      ja.r_owner = db->owner;
+      ja.r_offsets = db->offsets;
+      ja.layout = layout();
+      ja.hit_keys = acc + acc_n;
+      launch_join_expand(ja, c->stream);
+    }
+    acc_n += n_hits;
+  };
+  const uint64_t n_hits = scan_hits();
+  if (n_hits <= hit_budget || q->n == 1) {
+    // the stages after the join run on hits of several chunks at once, up to
+    // the budget (a subject lives in one chunk: pairs never span passes)
+    if (acc_n > 0 && acc_n + n_hits > hit_budget) {
+      tm.stop(&st.ms_join);
+      process_hits(pass++);
+      tm.start();
+    }
+    expand(n_hits, c->run_qstart.as<uint32_t>(0));
+    ++query_blocks;
+    tm.stop(&st.ms_join);
+    return;
   }
-  acc_n += n_hits;
+  // ---- query blocks: consecutive targets whose hits stay under the budget
+  // (a target is never split: its pairs are then all in one pass)
+  unsigned long long* thits = c->target_hits.as<unsigned long long>(q->n);
+  DRG_CUDA(cudaMemsetAsync(thits, 0, q->n * sizeof(unsigned long long), c->stream));
+  launch_target_hits(c->run_counts.as<uint32_t>(0), c->run_qstart.as<uint32_t>(0), rcnt, rhits, n_runs,
+                     c->q_vals_s.as<uint32_t>(0), q->owner, thits, c->stream);
+  std::vector<unsigned long long> th;
+  fetch_n(c, th, thits, q->n);
+  std::vector<std::pair<uint64_t, uint64_t>> blocks;
+  for (uint64_t t0 = 0; t0 < q->n;) {
+    uint64_t t1 = t0, sum = 0;
+    while (t1 < q->n && (t1 == t0 || sum + th[t1] <= hit_budget)) sum += th[t1++];
+    blocks.push_back({t0, t1});
+    t0 = t1;
+  }
+  if (acc_n > 0) {
+    tm.stop(&st.ms_join);
+    process_hits(pass++);
+    tm.start();
+  }
+  uint32_t* qlo = c->run_qlo.as<uint32_t>(n_runs + 1);
+  uint32_t* qcnt = c->run_qcount.as<uint32_t>(n_runs + 1);
+  for (auto [t0, t1] : blocks) {
+    JoinBlock jb{c->q_vals_s.as<uint32_t>(0), c->run_qstart.as<uint32_t>(0), q->h_offsets[t0], q->h_offsets[t1], qlo,
+                 qcnt};
+    const uint64_t key_mask = (1ull << seed_key_bits) - 1;
+    if (keys32_s)
+      launch_join_count(c->run_keys.as<uint64_t>(0), c->run_counts.as<uint32_t>(0), n_runs, keys32_s, (uint64_t)nr,
+                        4096, rlo, rcnt, rhits, key_mask, c->stream, first, shift, &jb, d_nr);
+    else
+      launch_join_count(c->run_keys.as<uint64_t>(0), c->run_counts.as<uint32_t>(0), n_runs, keys_s, (uint64_t)nr,
+                        4096, rlo, rcnt, rhits, key_mask, c->stream, first, shift, &jb, d_nr);
+    expand(scan_hits(), qlo);
+    ++query_blocks;
+    tm.stop(&st.ms_join);
+    process_hits(pass++);
+    tm.start();
+  }
   tm.stop(&st.ms_join);
 }
 
@@ -1453,9 +1514,9 @@ void Search::run(drg_result* out) {
   Timer total(c, &times);
   total.start();
   std::memset(out, 0, sizeof(*out));
-  d_count = c->counters.as<int64_t>(9);
+  d_count = c->counters.as<int64_t>(12);
   d_counters = reinterpret_cast<unsigned long long*>(d_count + 2);
-  DRG_CUDA(cudaMemsetAsync(d_count, 0, 9 * sizeof(int64_t), c->stream));
+  DRG_CUDA(cudaMemsetAsync(d_count, 0, 12 * sizeof(int64_t), c->stream));
   DRG_CUDA(cudaMemsetAsync(c->sort_err.as<uint32_t>(1), 0, sizeof(uint32_t), c->stream));
   if (q->n == 0 || db->n == 0) {
     out->n_targets = q->n;
@@ -1474,17 +1535,12 @@ void Search::run(drg_result* out) {
   query_seeds(&n_runs);
   tm.stop(&st.ms_seed);
   if (n_runs > 0) {
-    constexpr uint64_t kHitPassBudget = 1ull << 28;  // hits held before the stages after the join run
-    uint64_t pass = 0;
-    for (auto [c0, c1] : split_chunks(db->n, index_chunks)) {
-      join_chunk(c0, c1, n_runs);
-      if (acc_n >= kHitPassBudget) process_hits(pass++);
-    }
+    for (auto [c0, c1] : split_chunks(db->n, index_chunks)) join_chunk(c0, c1, n_runs);
     process_hits(pass++);
   }
   finish(out);
   total.stop(&st.ms_total);
-  unsigned long long cnt[7];
+  unsigned long long cnt[8];
   uint32_t sort_err = 0;
   DRG_CUDA(cudaMemcpyAsync(cnt, d_counters, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
   DRG_CUDA(cudaMemcpyAsync(&sort_err, c->sort_err.as<uint32_t>(1), sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
@@ -1498,7 +1554,10 @@ void Search::run(drg_result* out) {
   st.dp_cells_lane = cnt[4];
   st.dp_cells_issued = cnt[5];
   st.sw_transposed_bands = cnt[6];
+  st.ref_seeds += cnt[7];  // valid reference seeds counted on the device
   st.seed_shapes = shapes.size();
+  st.query_blocks = query_blocks;
+  st.hit_passes = pass;
   st.kernel_launches = kernel_launch_count() - launches0;
   out->stats = st;
 }

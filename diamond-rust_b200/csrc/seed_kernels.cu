@@ -324,9 +324,10 @@ void launch_seed_enum_filtered(const uint8_t* letters, const uint64_t* offsets, 
 // [0, nb]; the join then searches one bucket's range instead of all keys.
 template <typename K>
 __global__ void k_bucket_first(const K* __restrict__ keys, uint64_t n, int shift, uint32_t nb,
-                               uint32_t* __restrict__ first) {
+                               uint32_t* __restrict__ first, const uint64_t* d_n) {
   const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b > nb) return;
+  if (d_n) n = *d_n;
   const uint64_t key = (uint64_t)b << shift;
   uint64_t lo = 0, hi = n;
   while (lo < hi) {
@@ -338,18 +339,21 @@ __global__ void k_bucket_first(const K* __restrict__ keys, uint64_t n, int shift
 }
 
 template <typename K>
-void bucket_first(const K* keys, uint64_t n, int shift, uint32_t nb, uint32_t* first, cudaStream_t st) {
+void bucket_first(const K* keys, uint64_t n, int shift, uint32_t nb, uint32_t* first, cudaStream_t st,
+                  const uint64_t* d_n) {
   count_launch();
-  k_bucket_first<K><<<ceil_div((long long)nb + 1, 256), 256, 0, st>>>(keys, n, shift, nb, first);
+  k_bucket_first<K><<<ceil_div((long long)nb + 1, 256), 256, 0, st>>>(keys, n, shift, nb, first, d_n);
   DRG_CUDA(cudaGetLastError());
 }
 
-void launch_bucket_first(const uint64_t* keys, uint64_t n, int shift, uint32_t nb, uint32_t* first, cudaStream_t st) {
-  bucket_first(keys, n, shift, nb, first, st);
+void launch_bucket_first(const uint64_t* keys, uint64_t n, int shift, uint32_t nb, uint32_t* first, cudaStream_t st,
+                         const uint64_t* d_n) {
+  bucket_first(keys, n, shift, nb, first, st, d_n);
 }
 
-void launch_bucket_first(const uint32_t* keys, uint64_t n, int shift, uint32_t nb, uint32_t* first, cudaStream_t st) {
-  bucket_first(keys, n, shift, nb, first, st);
+void launch_bucket_first(const uint32_t* keys, uint64_t n, int shift, uint32_t nb, uint32_t* first, cudaStream_t st,
+                         const uint64_t* d_n) {
+  bucket_first(keys, n, shift, nb, first, st, d_n);
 }
 
 template <typename K>
@@ -357,9 +361,10 @@ __global__ void k_join_count(const uint64_t* __restrict__ run_keys, const uint32
                              uint64_t n_runs, const K* __restrict__ ref_keys, uint64_t n_ref,
                              uint64_t max_expand, uint32_t* __restrict__ run_rlo, uint32_t* __restrict__ run_rcount,
                              uint64_t* __restrict__ run_hits, uint64_t key_mask, const uint32_t* __restrict__ first,
-                             int shift) {
+                             int shift, JoinBlock blk, bool blocked, const uint64_t* d_n_ref) {
   uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (u >= n_runs) return;
+  if (d_n_ref) n_ref = *d_n_ref;
   const uint64_t key = run_keys[u] & key_mask;  // the query run's request does not take part
   uint64_t a = 0, end = n_ref;
   if (first) {
@@ -383,34 +388,79 @@ __global__ void k_join_count(const uint64_t* __restrict__ run_keys, const uint32
   uint64_t qc = run_counts[u];
   run_rlo[u] = (uint32_t)lo;
   run_rcount[u] = (uint32_t)rc;
-  run_hits[u] = (rc > 0 && qc * rc <= max_expand) ? qc * rc : 0;
+  uint64_t qb = qc;  // entries that expand: the block's share of the run
+  if (blocked) {
+    const uint32_t q0 = blk.run_qstart[u];
+    uint32_t x = q0, y = q0 + (uint32_t)qc;
+    while (x < y) {  // first entry at or after the block's first letter
+      const uint32_t m = (x + y) >> 1;
+      if (blk.q_vals[m] < blk.lo) x = m + 1;
+      else y = m;
+    }
+    const uint32_t b0 = x;
+    y = q0 + (uint32_t)qc;
+    while (x < y) {  // first entry at or after the block's end
+      const uint32_t m = (x + y) >> 1;
+      if (blk.q_vals[m] < blk.hi) x = m + 1;
+      else y = m;
+    }
+    blk.run_qlo[u] = b0;
+    blk.run_qcount[u] = x - b0;
+    qb = x - b0;
+  }
+  // the cap sees the whole run's count (seed.rs:120-127)
+  run_hits[u] = (rc > 0 && qc * rc <= max_expand) ? qb * rc : 0;
+}
+
+// One thread per query run: each entry of a run that passes the cap adds
+// rcount hits to its target.
+__global__ void k_target_hits(const uint32_t* __restrict__ run_counts, const uint32_t* __restrict__ run_qstart,
+                              const uint32_t* __restrict__ run_rcount, const uint64_t* __restrict__ run_hits,
+                              uint64_t n_runs, const uint32_t* __restrict__ q_vals,
+                              const uint32_t* __restrict__ q_owner, unsigned long long* __restrict__ target_hits) {
+  const uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (u >= n_runs || run_hits[u] == 0) return;
+  const uint32_t q0 = run_qstart[u], qc = run_counts[u], rc = run_rcount[u];
+  for (uint32_t e = q0; e < q0 + qc; ++e) atomicAdd(&target_hits[q_owner[q_vals[e]]], (unsigned long long)rc);
+}
+
+void launch_target_hits(const uint32_t* run_counts, const uint32_t* run_qstart, const uint32_t* run_rcount,
+                        const uint64_t* run_hits, uint64_t n_runs, const uint32_t* q_vals, const uint32_t* q_owner,
+                        unsigned long long* target_hits, cudaStream_t st) {
+  if (n_runs == 0) return;
+  count_launch();
+  k_target_hits<<<ceil_div(n_runs, 256), 256, 0, st>>>(run_counts, run_qstart, run_rcount, run_hits, n_runs, q_vals,
+                                                        q_owner, target_hits);
+  DRG_CUDA(cudaGetLastError());
 }
 
 template <typename K>
 void join_count(const uint64_t* run_keys, const uint32_t* run_counts, uint64_t n_runs, const K* ref_keys,
                 uint64_t n_ref, uint64_t max_expand, uint32_t* run_rlo, uint32_t* run_rcount, uint64_t* run_hits,
-                uint64_t key_mask, cudaStream_t st, const uint32_t* first, int shift) {
+                uint64_t key_mask, cudaStream_t st, const uint32_t* first, int shift, const JoinBlock* blk,
+                const uint64_t* d_n_ref) {
   if (n_runs == 0) return;
   count_launch();
   k_join_count<K><<<ceil_div(n_runs, 256), 256, 0, st>>>(run_keys, run_counts, n_runs, ref_keys, n_ref, max_expand,
-                                                         run_rlo, run_rcount, run_hits, key_mask, first, shift);
+                                                         run_rlo, run_rcount, run_hits, key_mask, first, shift,
+                                                         blk ? *blk : JoinBlock{}, blk != nullptr, d_n_ref);
   DRG_CUDA(cudaGetLastError());
 }
 
 void launch_join_count(const uint64_t* run_keys, const uint32_t* run_counts, uint64_t n_runs,
                        const uint64_t* ref_keys, uint64_t n_ref, uint64_t max_expand, uint32_t* run_rlo,
                        uint32_t* run_rcount, uint64_t* run_hits, uint64_t key_mask, cudaStream_t st,
-                       const uint32_t* first, int shift) {
+                       const uint32_t* first, int shift, const JoinBlock* blk, const uint64_t* d_n_ref) {
   join_count(run_keys, run_counts, n_runs, ref_keys, n_ref, max_expand, run_rlo, run_rcount, run_hits, key_mask, st,
-             first, shift);
+             first, shift, blk, d_n_ref);
 }
 
 void launch_join_count(const uint64_t* run_keys, const uint32_t* run_counts, uint64_t n_runs,
                        const uint32_t* ref_keys, uint64_t n_ref, uint64_t max_expand, uint32_t* run_rlo,
                        uint32_t* run_rcount, uint64_t* run_hits, uint64_t key_mask, cudaStream_t st,
-                       const uint32_t* first, int shift) {
+                       const uint32_t* first, int shift, const JoinBlock* blk, const uint64_t* d_n_ref) {
   join_count(run_keys, run_counts, n_runs, ref_keys, n_ref, max_expand, run_rlo, run_rcount, run_hits, key_mask, st,
-             first, shift);
+             first, shift, blk, d_n_ref);
 }
 
 // coarse[j] = the largest run u < n_runs with run_hit_off[u] <= j << shift,

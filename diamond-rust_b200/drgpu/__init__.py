@@ -74,7 +74,7 @@ class SearchConfig(C.Structure):
     _fields_ = [("matrix", C.c_char_p), ("gap_open", C.c_int32), ("gap_extend", C.c_int32), ("evalue", C.c_double),
                 ("max_target_seqs", C.c_uint32), ("max_hsps", C.c_uint32), ("sensitivity", C.c_char_p),
                 ("index_chunks", C.c_int32), ("has_seed_cut", C.c_int32), ("seed_cut", C.c_double),
-                ("threads", C.c_uint32), ("flags", C.c_uint32)]
+                ("threads", C.c_uint32), ("flags", C.c_uint32), ("max_hits_per_pass", C.c_uint64)]
 
 
 class RunStats(C.Structure):
@@ -89,7 +89,7 @@ class RunStats(C.Structure):
                 ("ms_sw_class", C.c_double * 4), ("ms_trace_kernel", C.c_double), ("dp_cells_lane", C.c_uint64),
                 ("sw_wide_bands", C.c_uint64), ("ms_sw_wide", C.c_double), ("dp_cells_issued", C.c_uint64),
                 ("index_hits", C.c_uint64), ("sw_transposed_bands", C.c_uint64),
-                ("seed_shapes", C.c_uint64)]
+                ("seed_shapes", C.c_uint64), ("query_blocks", C.c_uint64), ("hit_passes", C.c_uint64)]
 
     def as_dict(self):
         d = {}
@@ -255,7 +255,8 @@ def _result_lists(res: Result):
 
 
 def make_config(sensitivity="default", matrix="BLOSUM62", gap_open=-1, gap_extend=-1, evalue=1e-3,
-                max_target_seqs=25, max_hsps=1, index_chunks=None, seed_cut=None, threads=0) -> SearchConfig:
+                max_target_seqs=25, max_hsps=1, index_chunks=None, seed_cut=None, threads=0,
+                max_hits_per_pass=0) -> SearchConfig:
     c = SearchConfig()
     c.matrix = matrix.encode()
     c.gap_open = gap_open
@@ -269,6 +270,7 @@ def make_config(sensitivity="default", matrix="BLOSUM62", gap_open=-1, gap_exten
     c.seed_cut = 0.0 if seed_cut is None else float(seed_cut)
     c.threads = threads
     c.flags = 0
+    c.max_hits_per_pass = max_hits_per_pass
     return c
 
 

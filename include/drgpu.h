@@ -85,6 +85,11 @@ typedef struct {
   double seed_cut;
   uint32_t threads;         /* host threads for the CPU-side steps (0 = all) */
   uint32_t flags;           /* reserved, 0 */
+  /* Seed hits held at once before the stages after the join run over them
+   * (0 = 2^28).  When one index chunk yields more, the batch's targets are
+   * joined in blocks that each stay under it; the expansion cap still counts
+   * every target of the batch, so results do not depend on it. */
+  uint64_t max_hits_per_pass;
 } drg_search_config;
 
 /* Counters and device times of the last search (milliseconds, CUDA events). */
@@ -111,6 +116,8 @@ typedef struct {
   uint64_t index_hits;             /* index chunks whose sorted reference seeds came from the db's cache */
   uint64_t sw_transposed_bands;    /* score kernel: bands run with the subject as rows */
   uint64_t seed_shapes;            /* shapes of the preset (seeds per letter enumerated) */
+  uint64_t query_blocks;           /* (index chunk, target block) joins: more than the chunks when blocked */
+  uint64_t hit_passes;             /* passes of the stages after the join */
 } drg_run_stats;
 
 /* search::run result: per-target HSP lists, target_offsets[n_targets+1]. */

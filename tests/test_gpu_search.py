@@ -142,3 +142,61 @@ def test_search_window_clip(ctx, orc):
         assert ostats["clipped_windows"] > 0
         assert as_tuples(got) == exp
         assert any(h[1] == 17 for h in exp[0])
+
+
+def cap_workload():
+    """60 queries and 80 database sequences that all hold one 24-aa motif, plus
+    10 planted homologs.  With one index chunk every motif seed key has 60
+    query and 80 reference occurrences: 4,800 > 4,096, so the reference's join
+    drops those pairs (seed.rs:120-127, cap from search.rs:131).  Any 51
+    queries alone stay under the cap, so a join that counted query
+    occurrences per block instead of over the batch would report them."""
+    r = np.random.Generator(np.random.PCG64(4242))
+    motif = synth.random_protein(r, 24)
+    queries = []
+    for i in range(60):
+        q = synth.random_protein(r, int(r.integers(200, 400)))
+        p = int(r.integers(0, len(q) - 24))
+        q[p:p + 24] = motif
+        queries.append(q)
+    db = []
+    for j in range(80):
+        s = synth.random_protein(r, int(r.integers(150, 500)))
+        p = int(r.integers(0, len(s) - 24))
+        s[p:p + 24] = motif
+        db.append(s)
+    for j in range(10):
+        db.append(synth.planted_homolog(r, queries[j * 6], 120, 200, 0.5, 0.7, 400))
+    return queries, db
+
+
+@pytest.mark.parametrize("sens", ["default", "sensitive"])
+def test_query_blocks_keep_the_batch_wide_cap(ctx, orc, sens):
+    queries, db = cap_workload()
+    dl, do = drgpu.concat(db)
+    tl, to = drgpu.concat(queries)
+    whole, wst = ctx.search(dl, do, tl, to, drgpu.make_config(sensitivity=sens, index_chunks=1))
+    # a hit budget far below the batch's hits: the join runs in target blocks
+    budget = max(200, wst["hits"] // 6)
+    blocked, bst = ctx.search(dl, do, tl, to, drgpu.make_config(sensitivity=sens, index_chunks=1,
+                                                                 max_hits_per_pass=budget))
+    assert wst["query_blocks"] == 1
+    assert bst["query_blocks"] >= 4 and bst["hit_passes"] >= 4
+    assert bst["hits"] == wst["hits"]
+    exp, _ = orc.search(db, queries, sensitivity=sens, index_chunks=1, threads=8)
+    assert as_tuples(whole) == exp
+    assert as_tuples(blocked) == exp
+    # the construction crosses the cap: the first queries alone differ
+    alone, _ = orc.search(db, queries[:20], sensitivity=sens, index_chunks=1, threads=8)
+    assert alone != exp[:20]
+
+
+def test_query_blocks_with_index_chunks(ctx, orc):
+    w = small(2, 40, 600, seed=9)
+    dl, do = drgpu.concat(w.db)
+    tl, to = drgpu.concat(w.queries)
+    exp, _ = orc.search(w.db, w.queries, sensitivity="sensitive", index_chunks=3, threads=8)
+    got, st = ctx.search(dl, do, tl, to, drgpu.make_config(sensitivity="sensitive", index_chunks=3,
+                                                            max_hits_per_pass=3000))
+    assert st["query_blocks"] > 3
+    assert as_tuples(got) == exp
