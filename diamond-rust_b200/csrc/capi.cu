@@ -22,6 +22,11 @@ std::atomic<uint64_t> g_launches{0};
 }  // namespace
 
 namespace drg {
+// The message drg_last_error returns, from host code that sees the context
+// only through the C ABI (the per-stage search).
+void set_context_error(drg_ctx* ctx, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+}
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 uint64_t kernel_launch_count() { return g_launches.load(std::memory_order_relaxed); }
 }  // namespace drg

@@ -151,6 +151,8 @@ _SIGNATURES = {
     "drg_search_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, _P(SearchConfig), _P(Result)]),
     "drg_search_run": (C.c_int, [C.c_void_p, _u8p, _u64p, C.c_uint64, _u8p, _u64p, _u32p, _u8p, C.c_uint64,
                                  _P(SearchConfig), _P(Result)]),
+    "drg_search_run_per_stage": (C.c_int, [C.c_void_p, _u8p, _u64p, C.c_uint64, _u8p, _u64p, _u32p, _u8p,
+                                           C.c_uint64, _P(SearchConfig), _P(Result)]),
     "drg_merge_frames": (C.c_int, [_P(Result), C.c_uint64, _u32p, C.c_uint64, C.c_uint64]),
     "drg_result_free": (None, [_P(Result)]),
     "drg_matrix_evalue": (C.c_int, [C.c_char_p, C.c_int32, C.c_int32, C.c_int32, C.c_uint64, C.c_uint64,
@@ -411,6 +413,25 @@ class Context:
                                             C.byref(config), C.byref(res)))
         try:
             return _result_lists(res), res.stats.as_dict()
+        finally:
+            self.lib.drg_result_free(C.byref(res))
+
+    def search_per_stage(self, db_letters, db_offsets, t_letters, t_offsets, config: SearchConfig, t_query=None,
+                         t_frame=None, want_lists=True):
+        """search::run orchestrated on the host over the per-stage entry
+        points (drg_search_run_per_stage): the plain per-stage drop-in."""
+        dl, dlp = _u8(db_letters if len(db_letters) else np.zeros(1, np.uint8))
+        do, dop = _u64(db_offsets)
+        tl, tlp = _u8(t_letters if len(t_letters) else np.zeros(1, np.uint8))
+        to, top = _u64(t_offsets)
+        n_t = len(t_offsets) - 1
+        tq, tqp = _u32(np.arange(n_t) if t_query is None else t_query)
+        tf, tfp = _u8(np.zeros(n_t) if t_frame is None else t_frame)
+        res = Result()
+        self._check(self.lib.drg_search_run_per_stage(self.h, dlp, dop, len(db_offsets) - 1, tlp, top, tqp, tfp,
+                                                      n_t, C.byref(config), C.byref(res)))
+        try:
+            return (_result_lists(res) if want_lists else None), res.stats.as_dict(), int(res.n_hsps)
         finally:
             self.lib.drg_result_free(C.byref(res))
 

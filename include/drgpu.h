@@ -280,6 +280,18 @@ int drg_search_run(drg_ctx* ctx, const uint8_t* db_letters, const uint64_t* db_o
                    const uint8_t* t_letters, const uint64_t* t_offsets, const uint32_t* t_query,
                    const uint8_t* t_frame, uint64_t n_targets, const drg_search_config* cfg, drg_result* out);
 
+/* search::run from host buffers as the reference orchestrates it
+ * (search.rs:95-271), every hot function replaced by its per-stage entry
+ * point above: drg_seed_build per shape and chunk, drg_seed_join,
+ * drg_xdrop_batch, drg_extend_span_scores, drg_extend_span_batch, with the
+ * adjacency rule, band merge, window, E-value walk and culling on the host
+ * threads.  Results equal drg_search_run's; it is the plain per-stage drop-in
+ * that the fused device pipeline is measured against. */
+int drg_search_run_per_stage(drg_ctx* ctx, const uint8_t* db_letters, const uint64_t* db_offsets, uint64_t n_db,
+                             const uint8_t* t_letters, const uint64_t* t_offsets, const uint32_t* t_query,
+                             const uint8_t* t_frame, uint64_t n_targets, const drg_search_config* cfg,
+                             drg_result* out);
+
 /* search::merge_frames (search.rs:357-396) applied to a result, in place:
  * target_offsets becomes per-query offsets (n_queries + 1 entries). */
 int drg_merge_frames(drg_result* res, uint64_t n_queries, const uint32_t* t_query, uint64_t max_hsps,

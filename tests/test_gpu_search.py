@@ -200,3 +200,35 @@ def test_query_blocks_with_index_chunks(ctx, orc):
                                                             max_hits_per_pass=3000))
     assert st["query_blocks"] > 3
     assert as_tuples(got) == exp
+
+
+@pytest.mark.parametrize("sens", ["fast", "default", "sensitive", "very-sensitive"])
+def test_per_stage_drop_in_matches_oracle(ctx, orc, sens):
+    """search::run orchestrated on the host over the stage entry points
+    (drg_search_run_per_stage) equals the oracle and the fused search."""
+    w = small(2, 24, 400, seed=1)
+    dl, do = drgpu.concat(w.db)
+    tl, to = drgpu.concat(w.queries)
+    cfg = drgpu.make_config(sensitivity=sens, index_chunks=2)
+    got, st, _ = ctx.search_per_stage(dl, do, tl, to, cfg)
+    fused, _ = ctx.search(dl, do, tl, to, cfg)
+    exp, ost = orc.search(w.db, w.queries, sensitivity=sens, index_chunks=2, threads=8)
+    assert as_tuples(got) == exp
+    assert as_tuples(fused) == exp
+    assert st["hits"] == ost["hits"]
+    assert sum(len(x) for x in exp) > 0
+
+
+def test_per_stage_window_clip_and_cap(ctx, orc):
+    q, db = clip_workload()
+    dl, do = drgpu.concat(db)
+    tl, to = drgpu.concat([q])
+    got, _, _ = ctx.search_per_stage(dl, do, tl, to, drgpu.make_config(sensitivity="sensitive"))
+    exp, _ = orc.search(db, [q], sensitivity="sensitive", threads=8)
+    assert as_tuples(got) == exp
+    queries, db = cap_workload()
+    dl, do = drgpu.concat(db)
+    tl, to = drgpu.concat(queries)
+    got, _, _ = ctx.search_per_stage(dl, do, tl, to, drgpu.make_config(sensitivity="default", index_chunks=1))
+    exp, _ = orc.search(db, queries, sensitivity="default", index_chunks=1, threads=8)
+    assert as_tuples(got) == exp
