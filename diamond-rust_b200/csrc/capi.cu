@@ -205,6 +205,24 @@ void drg_ctx_destroy(drg_ctx* c) {
 
 const char* drg_last_error(const drg_ctx* c) { return c ? c->err.c_str() : "no context"; }
 
+int drg_ctx_get_tuning(const drg_ctx* c, drg_tuning* out) {
+  if (!c || !out) return DRG_ERR_INVALID;
+  *out = c->tuning;
+  return DRG_OK;
+}
+
+int drg_ctx_set_tuning(drg_ctx* c, const drg_tuning* t) {
+  if (!c || !t) return DRG_ERR_INVALID;
+  const int w = t->sw_wide_min_width, p = t->sw_min_packed_width;
+  if ((w != 137 && w != 273 && w != 545 && w != 1701) || (p != 17 && p != 33) ||
+      (t->sw_transpose != 0 && t->sw_transpose != 1) || (t->sort_small_tiles != 0 && t->sort_small_tiles != 1)) {
+    c->err = "tuning value outside its list (include/drgpu.h)";
+    return DRG_ERR_INVALID;
+  }
+  c->tuning = *t;
+  return DRG_OK;
+}
+
 int drg_seed_chunks(uint64_t n, uint64_t parts, uint64_t* out_pairs, uint64_t* n_out) {
   if (!n_out) return DRG_ERR_INVALID;
   auto v = split_chunks(n, parts);

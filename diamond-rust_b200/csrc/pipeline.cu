@@ -43,7 +43,7 @@ template <typename K>
 SortResult<K> dsort(drg_ctx* c, K* k, K* k_alt, uint32_t* v, uint32_t* v_alt, uint64_t n, int begin_bit,
                     int end_bit, const uint64_t* d_n = nullptr) {
   return radix_sort<K>(k, k_alt, v, v_alt, n, d_n, begin_bit, end_bit, c->sort_tmp, c->sort_err.as<uint32_t>(1),
-                       c->stream);
+                       c->stream, c->tuning.sort_small_tiles != 0);
 }
 
 template <typename T>
@@ -188,36 +188,47 @@ __global__ void k_count_fast_narrow(const uint64_t* keys, uint64_t n, int64_t* o
   out[1] = (int64_t)lo;
 }
 
+// The tuned routing (drg_tuning): where the packed 16-bit kernel starts, where
+// the score pass hands bands to the band kernel, and whether it transposes.
+struct SwTune {
+  int wide_min, min_packed, transpose;
+};
+SwTune sw_tune(const drg_ctx* c) {
+  return SwTune{c->tuning.sw_wide_min_width, c->tuning.sw_min_packed_width, c->tuning.sw_transpose};
+}
+
 // Which kernel a band goes to: the packed kernel (fast), its wide-band
 // variant (wide), and whether the band has fewer strips transposed.
 struct SwRoute {
   bool fast, wide, tr;
   int64_t rs, re, ts, te;
 };
-__device__ __forceinline__ SwRoute sw_route(const Band& b, const uint64_t* s_offsets, int max_score) {
+__device__ __forceinline__ SwRoute sw_route(const Band& b, const uint64_t* s_offsets, int max_score,
+                                            const SwTune& tn) {
   SwRoute r;
   const int64_t W = (int64_t)b.d1 - b.d0 + 1;
   const int64_t m = (int64_t)(s_offsets[b.subject + 1] - s_offsets[b.subject]);
   band_rows(b, m, false, &r.rs, &r.re);
   band_rows(b, m, true, &r.ts, &r.te);
   const int64_t mn = m < (int64_t)b.n ? m : (int64_t)b.n;
-  r.fast = W >= kSwMinWidth && W <= kSwMaxWidth && (int64_t)max_score * mn <= 32000 && r.rs <= r.re &&
+  r.fast = W >= tn.min_packed && W <= kSwMaxWidth && (int64_t)max_score * mn <= 32000 && r.rs <= r.re &&
            b.target < (1u << 21) && b.q0 < 65536 && r.re < 65536;
-  r.wide = r.fast && W >= kSwBandMinWidth;
+  r.wide = r.fast && W >= tn.wide_min;
   // narrow bands only: a medium band (W > 136) in a subject's warps would
   // make its narrow lanes wait on its width
-  r.tr = r.fast && W <= kSwC0 && r.ts <= r.te && r.te < 65536 && (r.te - r.ts + 16) / 16 < (r.re - r.rs + 16) / 16;
+  r.tr = tn.transpose && r.fast && !r.wide && W <= kSwC0 && r.ts <= r.te && r.te < 65536 &&
+         (r.te - r.ts + 16) / 16 < (r.re - r.rs + 16) / 16;
   return r;
 }
 // Bands per subject that would run with fewer strips transposed; each such
 // band draws a ticket (its arrival order, which varies from run to run: the
 // grouping of bands into warps does not change any score).
-__global__ void k_sw_tr_count(const Band* bands, uint64_t n, const uint64_t* s_offsets, int max_score,
+__global__ void k_sw_tr_count(const Band* bands, uint64_t n, const uint64_t* s_offsets, int max_score, SwTune tn,
                               uint32_t* count, uint32_t* ticket) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   const Band b = bands[i];
-  ticket[i] = sw_route(b, s_offsets, max_score).tr ? atomicAdd(count + b.subject, 1u) : 0xFFFFFFFFu;
+  ticket[i] = sw_route(b, s_offsets, max_score, tn).tr ? atomicAdd(count + b.subject, 1u) : 0xFFFFFFFFu;
 }
 
 // The two sort keys of the score pass: the key above, and rows (first-row
@@ -225,13 +236,13 @@ __global__ void k_sw_tr_count(const Band* bands, uint64_t n, const uint64_t* s_o
 // sorted by rows, then stably by key, so that bands next to each other cover
 // nearly the same rows.
 // rows[i] holds band i's ticket from k_sw_tr_count on entry.
-__global__ void k_sw_keys(const Band* bands, uint64_t n, const uint64_t* s_offsets, int max_score,
+__global__ void k_sw_keys(const Band* bands, uint64_t n, const uint64_t* s_offsets, int max_score, SwTune tn,
                           const uint32_t* tr_count, uint64_t* keys, uint32_t* rows, uint32_t* order) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   const Band b = bands[i];
   const uint64_t W = (uint64_t)(b.d1 - b.d0 + 1);
-  const SwRoute r = sw_route(b, s_offsets, max_score);
+  const SwRoute r = sw_route(b, s_offsets, max_score, tn);
   // A subject's transposed bands form warps of their own: only whole warps
   // of them are transposed, the rest stay with their query windows.
   const bool tr = r.tr && tr_count && rows[i] < (tr_count[b.subject] & ~31u);
@@ -560,12 +571,12 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
     tr_count = c->tr_count.as<uint32_t>(n_subjects);
     DRG_CUDA(cudaMemsetAsync(tr_count, 0, n_subjects * sizeof(uint32_t), c->stream));
     count_launch();
-    k_sw_tr_count<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(bc, n_bands, s.offsets, scr.max_score, tr_count,
-                                                                  rows);
+    k_sw_tr_count<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(bc, n_bands, s.offsets, scr.max_score,
+                                                                  sw_tune(c), tr_count, rows);
   }
   count_launch();
-  k_sw_keys<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(bc, n_bands, s.offsets, scr.max_score, tr_count, swk,
-                                                           rows, swo);
+  k_sw_keys<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(bc, n_bands, s.offsets, scr.max_score, sw_tune(c),
+                                                           tr_count, swk, rows, swo);
   // rows first, then a stable sort by (target, window, width)
   uint32_t* by_rows = dsort(c, rows, rows_s, swo, swo_r, n_bands, 0, 32).vals;
   count_launch();

@@ -70,6 +70,14 @@ class Hsp(C.Structure):
                 ("pad", C.c_uint32)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("sw_wide_min_width", C.c_int32), ("sw_min_packed_width", C.c_int32), ("sw_transpose", C.c_int32),
+                ("sort_small_tiles", C.c_int32)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 class SearchConfig(C.Structure):
     _fields_ = [("matrix", C.c_char_p), ("gap_open", C.c_int32), ("gap_extend", C.c_int32), ("evalue", C.c_double),
                 ("max_target_seqs", C.c_uint32), ("max_hsps", C.c_uint32), ("sensitivity", C.c_char_p),
@@ -123,6 +131,10 @@ _SIGNATURES = {
     "drg_seed_join": (C.c_int, [C.c_void_p, _P(SeedEntry), C.c_uint64, _P(SeedEntry), C.c_uint64, C.c_uint64,
                                 C.c_uint64, _P(_P(SeedHit)), _u64p]),
     "drg_seed_chunks": (C.c_int, [C.c_uint64, C.c_uint64, _u64p, _u64p]),
+    "drg_ctx_get_tuning": (C.c_int, [C.c_void_p, _P(Tuning)]),
+    "drg_ctx_set_tuning": (C.c_int, [C.c_void_p, _P(Tuning)]),
+    "drg_autotune": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, _P(SearchConfig), C.c_char_p, C.c_int32,
+                               _P(Tuning), _P(C.c_double), _P(C.c_double)]),
     "drg_radix_sort": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, _u32p, C.c_uint64, C.c_int32, C.c_int32,
                                  C.c_int32]),
     "drg_xdrop_batch": (C.c_int, [C.c_void_p, _u8p, _u64p, C.c_uint64, _u8p, _u64p, C.c_uint64, _P(XdropJob),
@@ -315,6 +327,27 @@ class Context:
                        dtype=[("key", "u8"), ("seq", "u4"), ("pos", "u4")])
         self.lib.drg_free(out)
         return arr
+
+    def tuning(self):
+        t = Tuning()
+        self._check(self.lib.drg_ctx_get_tuning(self.h, C.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, **kw):
+        t = Tuning()
+        self._check(self.lib.drg_ctx_get_tuning(self.h, C.byref(t)))
+        for k, v in kw.items():
+            setattr(t, k, int(v))
+        self._check(self.lib.drg_ctx_set_tuning(self.h, C.byref(t)))
+
+    def autotune(self, db, batch, config, cache_path=None, reps=2):
+        """drg_autotune: the best tuning for (db, batch, config), left in the
+        context; returns (tuning, ms under the starting tuning, ms best)."""
+        t, a, b = Tuning(), C.c_double(), C.c_double()
+        self._check(self.lib.drg_autotune(self.h, db.h, batch.h, C.byref(config),
+                                          None if cache_path is None else cache_path.encode(), reps, C.byref(t),
+                                          C.byref(a), C.byref(b)))
+        return t.as_dict(), a.value, b.value
 
     def radix_sort(self, keys, vals=None, begin_bit=0, end_bit=None, count_on_device=False):
         """The device radix sort (stable) of u32 or u64 keys, with optional

@@ -131,6 +131,23 @@ typedef struct {
   drg_run_stats stats;
 } drg_result;
 
+/* Tile and routing choices of a context (none changes a result).  The
+ * defaults are the first value of each list; drg_autotune picks among them.
+ *  sw_wide_min_width   score pass: bands at least this wide run in the lane-
+ *                      group band kernel instead of one band per lane
+ *                      (273; 137 = two bands per warp from 137, 545, 1701 = never)
+ *  sw_min_packed_width bands narrower than this run in int32 lanes (exact
+ *                      kernel) instead of 16-bit lanes (17, 33)
+ *  sw_transpose        short-subject bands may run with the subject as rows (1, 0)
+ *  sort_small_tiles    radix sort tiles of 8 (u32) / 6 (u64) keys per thread
+ *                      instead of 16 / 12 (0, 1) */
+typedef struct {
+  int32_t sw_wide_min_width;
+  int32_t sw_min_packed_width;
+  int32_t sw_transpose;
+  int32_t sort_small_tiles;
+} drg_tuning;
+
 /* ---- context --------------------------------------------------------- */
 /* One context per host thread; up to 8 contexts may be live in a process at
  * a time (each holds its own bank of constant tables, so contexts can search
@@ -140,6 +157,11 @@ void drg_ctx_destroy(drg_ctx* ctx);
 const char* drg_last_error(const drg_ctx* ctx);
 const char* drg_version(void);
 void drg_free(void* p);
+
+/* The context's tuning (no reference counterpart).  set rejects values
+ * outside the lists above with DRG_ERR_INVALID. */
+int drg_ctx_get_tuning(const drg_ctx* ctx, drg_tuning* out);
+int drg_ctx_set_tuning(drg_ctx* ctx, const drg_tuning* t);
 
 /* ---- stage entry points (seed.rs / ungapped.rs / gapped.rs) ------------ */
 
@@ -298,6 +320,18 @@ int drg_merge_frames(drg_result* res, uint64_t n_queries, const uint32_t* t_quer
                      uint64_t max_target_seqs);
 
 void drg_result_free(drg_result* res);
+
+/* Autotuner (no reference counterpart): times whole searches of `batch`
+ * against `db` under the tuning lists above (coordinate descent from the
+ * context's tuning, median of `reps` device-timed searches per candidate,
+ * a value kept when 1 % faster) and leaves the best in the context.  With a
+ * cache_path, a line "key wide packed transpose small_tiles" per workload
+ * kind (device, preset, powers of two of the query and database letters) is
+ * read first and appended after a tuning run.  ms_default / ms_best: the
+ * median search time under the starting and the chosen tuning (0 when the
+ * cache answered).  Results are the same under every tuning. */
+int drg_autotune(drg_ctx* ctx, const drg_db* db, const drg_batch* batch, const drg_search_config* cfg,
+                 const char* cache_path, int32_t reps, drg_tuning* out, double* ms_default, double* ms_best);
 
 /* ---- statistics (matrix.rs:164-200, alp.rs:108-163) ------------------- */
 int drg_matrix_evalue(const char* matrix, int32_t gap_open, int32_t gap_extend, int32_t raw, uint64_t qlen,

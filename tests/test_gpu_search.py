@@ -232,3 +232,47 @@ def test_per_stage_window_clip_and_cap(ctx, orc):
     got, _, _ = ctx.search_per_stage(dl, do, tl, to, drgpu.make_config(sensitivity="default", index_chunks=1))
     exp, _ = orc.search(db, queries, sensitivity="default", index_chunks=1, threads=8)
     assert as_tuples(got) == exp
+
+
+@pytest.mark.parametrize("tuning", [dict(sw_wide_min_width=137), dict(sw_wide_min_width=545),
+                                    dict(sw_wide_min_width=1701, sw_transpose=0),
+                                    dict(sw_min_packed_width=33, sort_small_tiles=1)])
+def test_tunings_give_identical_results(orc, tuning):
+    """Every tile and routing choice of the autotuner gives the oracle's HSPs."""
+    w = small(2, 24, 400, seed=3)
+    dl, do = drgpu.concat(w.db)
+    tl, to = drgpu.concat(w.queries)
+    c = drgpu.Context(0)
+    try:
+        c.set_tuning(**tuning)
+        assert all(c.tuning()[k] == v for k, v in tuning.items())
+        for sens in ("sensitive", "very-sensitive"):
+            got, _ = c.search(dl, do, tl, to, drgpu.make_config(sensitivity=sens))
+            exp, _ = orc.search(w.db, w.queries, sensitivity=sens, threads=8)
+            assert as_tuples(got) == exp
+    finally:
+        c.close()
+
+
+def test_autotune_picks_and_caches(tmp_path):
+    w = small(2, 60, 800, seed=4)
+    dl, do = drgpu.concat(w.db)
+    tl, to = drgpu.concat(w.queries)
+    c = drgpu.Context(0)
+    try:
+        db = drgpu.ResidentDb(c, dl, do)
+        b = drgpu.ResidentBatch(c, tl, to)
+        cfg = drgpu.make_config(sensitivity="sensitive")
+        cache = str(tmp_path / "tune.txt")
+        t1, ms0, ms1 = c.autotune(db, b, cfg, cache_path=cache, reps=1)
+        assert ms0 > 0 and 0 < ms1 <= ms0
+        assert c.tuning() == t1
+        c.set_tuning(sw_wide_min_width=1701)
+        t2, a, _ = c.autotune(db, b, cfg, cache_path=cache, reps=1)  # answered by the cache
+        assert t2 == t1 and a == 0 and c.tuning() == t1
+        with pytest.raises(drgpu.DrgError):
+            c.set_tuning(sw_wide_min_width=300)
+        b.close()
+        db.close()
+    finally:
+        c.close()
