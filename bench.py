@@ -61,7 +61,11 @@ def parse():
     p.add_argument("--no-very-sensitive", action="store_true", help="skip the very-sensitive leg")
     p.add_argument("--no-batching", action="store_true", help="skip the batched-vs-plain leg")
     p.add_argument("--blastx-reads", type=int, default=20000, help="reads in the blastx leg")
-    p.add_argument("--serve-requests", type=int, default=100, help="requests in the serving stream")
+    p.add_argument("--serve-requests", type=int, default=500, help="requests in the serving stream")
+    p.add_argument("--serve-repeats", type=int, default=3, help="replays of the stream per serving form")
+    p.add_argument("--batch-queries", type=int, default=50000, help="queries of the batched-vs-plain leg")
+    p.add_argument("--batch-db", type=int, default=2000, help="database sequences of the batched-vs-plain leg")
+    p.add_argument("--batch-sample", type=int, default=200, help="queries the oracle checks in that leg")
     p.add_argument("--queries", type=int, default=None,
                    help="search only the first N queries (a smaller case for ncu captures; not a bench line)")
     return p.parse_args()
@@ -204,86 +208,122 @@ def max_over_ranks(x, world):
     return float(t.item())
 
 
-def serve_stream(w, device, n_requests):
+def serve_stream(w, device, n_requests, repeats):
     """A Poisson request stream (20 requests/s, 1-2000 queries each, lengths
     lognormal mean 350 clipped 20-3000, presets uniform over fast / default /
     sensitive / very-sensitive) against the resident database, served plain
     (one request at a time, the seed index rebuilt per search as the reference
-    does) and continuously batched (2 worker contexts, each preset's seed
-    index resident)."""
+    does) and continuously batched (2 worker contexts, a 1M-letter batch
+    budget, each preset's seed index resident).  The stream is replayed
+    `repeats` times per form at its rate (forms alternating), then once with
+    every request queued at once (capacity)."""
     import numpy as np
     import drgpu
     from drgpu import serve
     dl, do = drgpu.concat(w.db)
+    rng = np.random.Generator(np.random.PCG64(20261208))
+    base = serve.poisson_stream(rng, n_requests, 20.0, 2000, ["fast", "default", "sensitive", "very-sensitive"])
     out = {"stream": f"{n_requests} requests, Poisson 20/s, 1-2000 queries each (lognormal mean 350, 20-3000 aa), "
-                     f"presets uniform over fast/default/sensitive/very-sensitive, resident "
-                     f"{len(w.db)}-sequence DB; latency = arrival to results on the host; *_capacity: the same "
-                     f"requests queued at once; plain: one request at a time, seed index rebuilt per search; "
-                     f"batched: 2 worker contexts, continuous batching, seed index resident per preset"}
-    # at the stream's rate (latency), and with every request queued at once
-    # (capacity: the throughput each form sustains)
-    for rate, tag in ((20.0, ""), (1e6, "_capacity")):
-        for name, workers, batched in (("plain", 1, False), ("batched", 2, True)):
-            rng = np.random.Generator(np.random.PCG64(20261208))
-            stream = serve.poisson_stream(rng, n_requests, rate, 2000,
-                                          ["fast", "default", "sensitive", "very-sensitive"])
-            srv = serve.Server(dl, do, workers=workers, batch=batched, device=device,
-                               index_budget=(16 << 30) if batched else 0)
-            try:
-                finished, span = serve.run_stream(srv, stream)
-            finally:
-                srv.close()
-            out[name + tag] = serve.latency_summary(finished, span)
+                     f"presets uniform over fast/default/sensitive/very-sensitive, resident {len(w.db)}-sequence DB; "
+                     f"latency = arrival to results on the host; {repeats} replays per form at the stream's rate "
+                     f"(median and range), then all requests queued at once (capacity); plain: one request at a "
+                     f"time, seed index rebuilt per search; batched: 2 worker contexts, continuous batching under "
+                     f"a 1M-letter batch budget, seed index resident per preset"}
+
+    def replay(batched, rate):
+        stream = [(t * 20.0 / rate, serve.Request(r.rid, r.preset, r.queries)) for t, r in base]
+        srv = serve.Server(dl, do, workers=2 if batched else 1, batch=batched, device=device,
+                           index_budget=(16 << 30) if batched else 0)
+        try:
+            finished, span = serve.run_stream(srv, stream)
+        finally:
+            srv.close()
+        return serve.latency_summary(finished, span)
+
+    runs = {"plain": [], "batched": []}
+    for _ in range(repeats):
+        for name in ("plain", "batched"):
+            runs[name].append(replay(name == "batched", 20.0))
+    for name, rs in runs.items():
+        summ = {}
+        for k in ("p50_s", "p99_s", "mean_s", "queries_per_s", "mean_batch_requests"):
+            vals = sorted(r[k] for r in rs)
+            summ[k] = statistics.median(vals)
+            summ[k + "_range"] = [vals[0], vals[-1]]
+        summ["requests"] = rs[0]["requests"]
+        summ["queries"] = rs[0]["queries"]
+        out[name] = summ
+    for name in ("plain", "batched"):
+        out[name + "_capacity"] = replay(name == "batched", 1e6)
     return out
 
 
-def batching_leg(ctx, n_queries=400, n_db=50000):
-    """Config-3 shaped, scaled (400 queries, lognormal mean 350, 20-2000 aa,
-    10 % with 1-20 planted homologs, against 50,000 sequences; --sensitive,
-    index chunks 4, the seed index resident).  plain: one search per query;
-    batched: one search of all queries, each its own request (per-request join
-    accounting), so that both give the same HSPs.  Wall time host to host."""
-    import numpy as np
+def batching_leg(ctx, n_queries, n_db, sample):
+    """Config-3 generator (lognormal mean 350, 20-2000 aa, 10 % of the queries
+    with 1-20 planted homologs), n_queries queries against an n_db-sequence
+    database, blastp --sensitive (4 index chunks), the whole batch in one call
+    from host buffers in both forms:
+
+      plain    drg_search_run_per_stage: search::run's own orchestration on
+               the host over the per-stage entry points (seed::build,
+               seed::join_into, ungapped::xdrop, gapped::extend_span drop-ins)
+      batched  drg_search_run: the fused device pipeline (hand-written radix
+               sorts, the join in query blocks under a hit budget, device-side
+               gate, packed score kernels over a work list sorted by band
+               area, one traceback launch), autotuned on the batch first
+
+    Both must give the same HSPs; the oracle checks the first `sample`
+    queries searched as their own batch (the join cap counts a batch's
+    queries, so a sample is its own search)."""
     import drgpu
     from drgpu import synth
-    w = synth.workload(3, n_queries=n_queries, n_db=n_db, seed_offset=0)
-    dl, do = drgpu.concat(w.db)
-    db = drgpu.ResidentDb(ctx, dl, do, index_budget=16 << 30)
-    cfg = drgpu.make_config(sensitivity="sensitive", index_chunks=4)
-    tl, to = drgpu.concat(w.queries)
-
-    def batched():
-        b = drgpu.ResidentBatch(ctx, tl, to, request=np.arange(len(w.queries), dtype=np.uint32))
-        try:
-            return drgpu.search_resident(ctx, db, b, cfg)[0]
-        finally:
-            b.close()
-
-    def plain():
-        out = []
-        for q in w.queries:
-            ql, qo = drgpu.concat([q])
-            b = drgpu.ResidentBatch(ctx, ql, qo)
-            try:
-                out.append(drgpu.search_resident(ctx, db, b, cfg)[0][0])
-            finally:
-                b.close()
-        return out
-
-    batched()  # builds the index entries
     t0 = time.perf_counter()
-    lb = batched()
+    w = synth.workload(3, n_queries=n_queries, n_db=n_db, seed_offset=0)
+    gen_s = time.perf_counter() - t0
+    dl, do = drgpu.concat(w.db)
+    tl, to = drgpu.concat(w.queries)
+    cfg = drgpu.make_config(sensitivity="sensitive")
+    # autotune on the batch (untimed), then the tuning stays in the context
+    db = drgpu.ResidentDb(ctx, dl, do)
+    b = drgpu.ResidentBatch(ctx, tl, to)
+    before = ctx.tuning()
+    tuned, ms_default, ms_tuned = ctx.autotune(db, b, cfg, reps=1)
+    b.close()
+    db.close()
+    ctx.search_counts(dl, do, tl, to, cfg)  # warm-up: sizes the context's buffers
+    t0 = time.perf_counter()
+    nb_hsps, _, bst = ctx.search_counts(dl, do, tl, to, cfg)
     tb = time.perf_counter() - t0
     t0 = time.perf_counter()
-    lp = plain()
+    lp, pst, np_hsps = ctx.search_per_stage(dl, do, tl, to, cfg)
     tp = time.perf_counter() - t0
-    same = [[h.key()[1:] for h in x] for x in lb] == [[h.key()[1:] for h in x] for x in lp]
-    db.close()
-    return {"workload": f"{n_queries} queries (config-3 generator) x {n_db:,}-sequence DB ({int(do[-1]):,} aa), "
-                        "blastp --sensitive, index chunks 4, seed index resident",
-            "plain_queries_per_s": n_queries / tp, "batched_queries_per_s": n_queries / tb,
-            "batched_over_plain": tp / tb, "identical_hsps": same,
-            "hsps": sum(len(x) for x in lb)}
+    lb, _ = ctx.search(dl, do, tl, to, cfg)
+    same = [[h.key() for h in x] for x in lb] == [[h.key() for h in x] for x in lp]
+    out = {"workload": f"{n_queries} queries (config-3 generator: lognormal mean 350, 20-2000 aa, 10 % with 1-20 "
+                       f"planted homologs) x {n_db:,}-sequence DB ({int(do[-1]):,} aa), blastp --sensitive, "
+                       "4 index chunks, one call from host buffers per form",
+           "plain": {"queries_per_s": n_queries / tp, "s": tp, "form": "drg_search_run_per_stage"},
+           "batched": {"queries_per_s": n_queries / tb, "s": tb, "device_ms": bst["ms_total"],
+                       "form": "drg_search_run",
+                       "stages_ms": {k: round(bst[k], 2) for k in ("ms_seed", "ms_join", "ms_sort", "ms_ungapped",
+                                                                   "ms_bands", "ms_sw", "ms_select", "ms_trace",
+                                                                   "ms_host")},
+                       "query_blocks": int(bst["query_blocks"]), "hit_passes": int(bst["hit_passes"])},
+           "autotune": {"start": before, "chosen": tuned, "search_ms_start": ms_default,
+                        "search_ms_chosen": ms_tuned},
+           "batched_over_plain": tp / tb, "identical_hsps": same and nb_hsps == np_hsps,
+           "hsps": nb_hsps, "hits": int(bst["hits"]), "bands": int(bst["bands"]),
+           "dp_cells_ref": int(bst["dp_cells_ref"]), "generate_s": gen_s}
+    ctx.set_tuning(**before)
+    if sample:
+        import pyoracle
+        qs = w.queries[:sample]
+        stl, sto = drgpu.concat(qs)
+        got, _ = ctx.search(dl, do, stl, sto, cfg)
+        exp, _ = pyoracle.search(w.db, qs, sensitivity="sensitive", threads=os.cpu_count() or 1)
+        out["oracle_sample"] = {"queries": sample, "identical": [[h.key() for h in x] for x in got] == exp,
+                                "hsps": sum(len(x) for x in exp)}
+    return out
 
 
 def blastx_leg(ctx, steps, warmup, n_reads, cpu_sample, with_cpu):
@@ -534,12 +574,13 @@ def main():
     # ---- serving: the same request stream, plain and continuously batched ---
     serving = None
     if not args.no_serve:
-        serving = serve_stream(w, local, args.serve_requests)
+        serving = serve_stream(w, local, args.serve_requests, args.serve_repeats)
 
     # ---- batched vs plain (config-3 shaped, scaled) --------------------------
     batching = None
     if not args.no_batching:
-        batching = batching_leg(ctx)
+        batching = batching_leg(ctx, args.batch_queries, args.batch_db,
+                                0 if args.no_cpu else args.batch_sample)
 
     # ---- blastx (config-4 shaped, scaled) ------------------------------------
     blastx = None

@@ -252,20 +252,40 @@ class HspRecord:
                 self.gaps, self.length, self.ops)
 
 
+class ResultArrays:
+    """A result copied out of the library in three bulk copies: hsps (numpy
+    structured array of drg_hsp), target_offsets (n_targets + 1) and ops.
+    lists() builds the per-target HspRecord lists on demand."""
+
+    def __init__(self, res: Result):
+        n, n_t = int(res.n_hsps), int(res.n_targets)
+        self.hsps = np.ctypeslib.as_array(res.hsps, shape=(n,)).copy() if n else np.zeros(0, _HSP_DTYPE)
+        self.target_offsets = (np.ctypeslib.as_array(res.target_offsets, shape=(n_t + 1,)).copy() if n_t
+                               else np.zeros(1, np.uint64))
+        self.ops = (np.ctypeslib.as_array(res.ops, shape=(int(res.n_ops),)).copy() if res.n_ops
+                    else np.zeros(0, np.uint32))
+
+    def lists(self, query_shift=0):
+        out = []
+        h, offs, ops = self.hsps, self.target_offsets.tolist(), self.ops
+        cols = [h[f].tolist() for f in ("query", "subject", "frame", "score", "q_begin", "q_end", "s_begin", "s_end",
+                                        "bits", "evalue", "identities", "positives", "mismatches", "gap_openings",
+                                        "gaps", "length", "ops_offset", "n_ops")]
+        for t in range(len(offs) - 1):
+            lst = []
+            for k in range(offs[t], offs[t + 1]):
+                o, n = cols[16][k], cols[17][k]
+                lst.append(HspRecord(cols[0][k] - query_shift, *(c[k] for c in cols[1:16]),
+                                     tuple(ops[o:o + n].tolist())))
+            out.append(lst)
+        return out
+
+
+_HSP_DTYPE = np.ctypeslib.as_array((Hsp * 1)()).dtype
+
+
 def _result_lists(res: Result):
-    out = []
-    n_t = res.n_targets
-    offs = [res.target_offsets[i] for i in range(n_t + 1)] if n_t else [0]
-    for t in range(n_t):
-        lst = []
-        for k in range(offs[t], offs[t + 1]):
-            h = res.hsps[k]
-            ops = tuple(res.ops[h.ops_offset + i] for i in range(h.n_ops))
-            lst.append(HspRecord(h.query, h.subject, h.frame, h.score, h.q_begin, h.q_end, h.s_begin, h.s_end,
-                                 h.bits, h.evalue, h.identities, h.positives, h.mismatches, h.gap_openings, h.gaps,
-                                 h.length, ops))
-        out.append(lst)
-    return out
+    return ResultArrays(res).lists()
 
 
 def make_config(sensitivity="default", matrix="BLOSUM62", gap_open=-1, gap_extend=-1, evalue=1e-3,

@@ -9,6 +9,12 @@ per request, so each request's HSP lists equal those of the request searched
 alone; requests that arrive while a batch runs wait only for the next free
 worker (continuous batching), and the workers' batches overlap on the GPU.
 
+The letter budget bounds a batch's work, so that a batch takes about as long
+as one large request: small requests share a batch, large ones run alone.
+Results come back to the host as three bulk copies per batch (HSP records,
+per-target offsets, alignment ops); Python records are built only when a
+request's results are read, outside the worker loop.
+
 The plain path (`workers=1, batch=False`) serves one request at a time.
 Latency is the wall time from a request's arrival to its results being back on
 the host; throughput is queries over the whole run.
@@ -19,11 +25,11 @@ import ctypes as C
 import statistics
 import threading
 import time
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 
 import numpy as np
 
-from . import (Context, HspRecord, ResidentBatch, ResidentDb, Result, _result_lists, concat, make_config)
+from . import Context, ResidentBatch, ResidentDb, Result, ResultArrays, concat, make_config
 
 
 @dataclass
@@ -33,12 +39,26 @@ class Request:
     queries: list
     arrival: float = 0.0          # seconds, on the server's clock
     done: float = 0.0
-    results: list = field(default_factory=list)  # per query: HSP records
     batch_size: int = 0           # requests in the batch that served it
+    raw: object = None            # (ResultArrays of the batch, first target, targets)
+
+    @property
+    def results(self):
+        """Per query: HSP records, query indices within the request."""
+        if self.raw is None:
+            return []
+        arrays, t0, n = self.raw
+        offs = arrays.target_offsets
+        sub = ResultArrays.__new__(ResultArrays)
+        sub.hsps = arrays.hsps[offs[t0]:offs[t0 + n]]
+        sub.target_offsets = offs[t0:t0 + n + 1] - offs[t0]
+        sub.ops = arrays.ops
+        return sub.lists(query_shift=t0)
 
 
 def search_batch(ctx: Context, db: ResidentDb, requests, preset: str, index_chunks=None):
-    """Search several requests of one preset as one batch; fills each request's results."""
+    """Search several requests of one preset as one batch; each request gets
+    its slice of the batch's results (copied to the host in bulk)."""
     seqs, rid = [], []
     for k, r in enumerate(requests):
         seqs.extend(r.queries)
@@ -49,14 +69,14 @@ def search_batch(ctx: Context, db: ResidentDb, requests, preset: str, index_chun
     res = Result()
     try:
         ctx._check(ctx.lib.drg_search_batch(ctx.h, db.h, batch.h, C.byref(cfg), C.byref(res)))
-        lists = _result_lists(res)
+        arrays = ResultArrays(res)
     finally:
         ctx.lib.drg_result_free(C.byref(res))
         batch.close()
     t = 0
     for r in requests:
         n = len(r.queries)
-        r.results = [[HspRecord(h.query - t, *h.key()[1:]) for h in lst] for lst in lists[t:t + n]]
+        r.raw = (arrays, t, n)
         r.batch_size = len(requests)
         t += n
     return requests
@@ -65,7 +85,7 @@ def search_batch(ctx: Context, db: ResidentDb, requests, preset: str, index_chun
 class Server:
     """Continuous-batching request loop over one resident database."""
 
-    def __init__(self, db_letters, db_offsets, workers=2, batch=True, budget_letters=4_000_000, device=0,
+    def __init__(self, db_letters, db_offsets, workers=2, batch=True, budget_letters=1_000_000, device=0,
                  index_chunks=None, index_budget=0):
         self.ctxs = [Context(device) for _ in range(workers)]
         # index_budget > 0: each preset's sorted reference seeds stay resident
