@@ -8,6 +8,8 @@
 // segment is on this diagonal and reaches spos" only ever compares hits of
 // the same run, so runs are independent.  Kept segments are written at their
 // hit's index and compacted afterwards, which preserves the push order.
+#include <climits>
+
 #include "kernels.h"
 
 namespace drg {
@@ -113,12 +115,182 @@ __device__ __forceinline__ unsigned long long xdrop_run(const XdropArgs& a, uint
   return nx;
 }
 
+// One direction of an X-drop extension in flight (ungapped.rs:46-83): steps
+// taken so far, the running score, the best score and the step that reached
+// it first.  Left: step k compares (qa-1-k, sa-1-k); right: (qa+k, sa+k).
+struct XdropDir {
+  const uint8_t* q;
+  const uint8_t* s;
+  int64_t qa, sa;
+  uint32_t bound;  // steps before a sequence end
+  uint32_t k;      // steps taken
+  int st, score;
+  uint32_t best;   // steps when the best was first reached (delta / len)
+  bool left;
+};
+
+constexpr uint32_t kXdropSerialSteps = 32;  // an extension longer than this is run by the whole warp
+
+// Serial steps, at most `limit`; true when the direction has stopped (the
+// reference's loop condition failed or a sequence ended).
+__device__ __forceinline__ bool xdrop_steps(XdropDir& d, int xd, uint32_t limit, const int8_t* mat) {
+  for (uint32_t i = 0; i < limit; ++i) {
+    if (!(d.score - d.st < xd && d.k < d.bound)) return true;
+    const int64_t qi = d.left ? d.qa - 1 - d.k : d.qa + d.k, si = d.left ? d.sa - 1 - d.k : d.sa + d.k;
+    d.st += mscore(d.q[qi], d.s[si], mat);
+    ++d.k;
+    if (d.st > d.score) {
+      d.score = d.st;
+      d.best = d.k;
+    }
+  }
+  return !(d.score - d.st < xd && d.k < d.bound);
+}
+
+// The whole warp runs one lane's direction to its end, 32 steps at a time:
+// lane l scores step k0 + l; prefix sums give the running score after each
+// step, prefix maxima the best before it; the first step whose condition
+// fails (or that is past a sequence end) ends the direction; the best's
+// first occurrence among the steps taken is where the reference's strict
+// "st > score" last fired.  Every lane returns the same state.
+__device__ XdropDir xdrop_warp(XdropDir d, int xd, const int8_t* mat) {
+  const uint32_t lane = threadIdx.x & 31;
+  for (;;) {
+    const uint32_t k = d.k + lane;
+    const bool valid = k < d.bound;
+    int sc = 0;
+    if (valid) {
+      const int64_t qi = d.left ? d.qa - 1 - k : d.qa + k, si = d.left ? d.sa - 1 - k : d.sa + k;
+      sc = mscore(d.q[qi], d.s[si], mat);
+    }
+    int sum = sc;  // inclusive prefix sum of the step scores
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xFFFFFFFFu, sum, o);
+      if (lane >= (uint32_t)o) sum += y;
+    }
+    const int st_after = d.st + sum;  // running score after this lane's step
+    int mx = valid ? st_after : INT_MIN;  // inclusive prefix max of the running score
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xFFFFFFFFu, mx, o);
+      if (lane >= (uint32_t)o) mx = max(mx, y);
+    }
+    const int best_before = max(d.score, lane == 0 ? INT_MIN : __shfl_up_sync(0xFFFFFFFFu, mx, 1));
+    const int st_before = st_after - sc;
+    const uint32_t stop = __ballot_sync(0xFFFFFFFFu, !valid || !(best_before - st_before < xd));
+    const uint32_t taken = stop ? (uint32_t)(__ffs(stop) - 1) : 32u;
+    if (taken > 0) {
+      const int new_st = __shfl_sync(0xFFFFFFFFu, st_after, taken - 1);
+      const int top = max(d.score, __shfl_sync(0xFFFFFFFFu, mx, taken - 1));
+      if (top > d.score) {
+        const uint32_t first = __ballot_sync(0xFFFFFFFFu, lane < taken && st_after == top);
+        d.best = d.k + (uint32_t)__ffs(first);  // steps up to and including the first maximum
+        d.score = top;
+      }
+      d.st = new_st;
+      d.k += taken;
+    }
+    if (taken < 32) return d;
+  }
+}
+
+// One thread per (target, subject, diagonal) run, as xdrop_run, except that
+// an extension still going after kXdropSerialSteps steps in one direction is
+// finished by the whole warp (xdrop_warp), so that a long true-homology
+// extension does not hold 31 idle lanes.  The hits of a run, the skip rule
+// (search.rs:184-191) and the cutoff stay in order per lane.
 __global__ void k_xdrop_runs(XdropArgs a) {
   __shared__ int8_t mat[625];
   stage_matrix(mat, a.slot);
   const uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint32_t lane = threadIdx.x & 31;
+  const HitKeyLayout L = a.layout;
+  bool live = r < a.n_runs;  // the lane still has hits to extend
+  uint64_t i = 0, run = 0;
+  const uint8_t *q = nullptr, *s = nullptr;
+  uint32_t qlen = 0, slen = 0;
+  int64_t diag = 0, last_end = -1;
+  if (live) {
+    i = a.run_head_idx[r];
+    run = a.hit_keys[i] >> L.pb;
+    const uint32_t t = (uint32_t)(a.hit_keys[i] >> (L.pb + L.db + L.sb));
+    const uint32_t sj = (uint32_t)((a.hit_keys[i] >> (L.pb + L.db)) & ((1ull << L.sb) - 1));
+    diag = (int64_t)((a.hit_keys[i] >> L.pb) & ((1ull << L.db) - 1)) - L.doff;
+    q = a.q_letters + a.q_offsets[t];
+    qlen = (uint32_t)(a.q_offsets[t + 1] - a.q_offsets[t]);
+    s = a.s_letters + a.s_offsets[sj];
+    slen = (uint32_t)(a.s_offsets[sj + 1] - a.s_offsets[sj]);
+  }
+  bool ext = false;     // an extension is in flight
+  XdropDir d{};         // its current direction
+  int left_score = 0;   // the left direction's best (the right one starts there)
+  uint32_t delta = 0;   // the left direction's best step
+  uint32_t qpos = 0, spos = 0;
   unsigned long long nx = 0;
-  if (r < a.n_runs) nx = xdrop_run(a, r, mat);
+  for (;;) {
+    bool needs_warp = false;
+    while (live) {
+      if (!ext) {
+        // the next hit of the run that the skip rule lets through
+        while (i < a.n_hits && (a.hit_keys[i] >> L.pb) == run) {
+          spos = (uint32_t)(a.hit_keys[i] & ((1ull << L.pb) - 1));
+          a.keep[i] = 0;
+          if (last_end < (int64_t)spos) break;
+          ++i;
+        }
+        if (!(i < a.n_hits && (a.hit_keys[i] >> L.pb) == run)) {
+          live = false;
+          break;
+        }
+        qpos = (uint32_t)(diag + spos);
+        d = XdropDir{q, s, qpos, spos, min(qpos, spos), 0, 0, 0, 0, true};
+        ext = true;
+        ++nx;
+      }
+      if (!xdrop_steps(d, a.xdrop, kXdropSerialSteps, mat)) {
+        needs_warp = true;
+        break;
+      }
+      if (d.left) {  // the right direction starts from the left's best
+        left_score = d.score;
+        delta = d.best;
+        d = XdropDir{q, s, qpos, spos, min(qlen - qpos, slen - spos), 0, left_score, left_score, 0, false};
+      } else {
+        SegmentOut seg;
+        seg.q_start = qpos - delta;
+        seg.s_start = spos - delta;
+        seg.len = d.best + delta;
+        seg.score = d.score;
+        if (seg.score >= a.cutoff) {
+          a.seg[i] = seg;
+          a.keep[i] = 1;
+          last_end = (int64_t)seg.s_start + seg.len;
+        }
+        ++i;
+        ext = false;
+      }
+    }
+    const uint32_t help = __ballot_sync(0xFFFFFFFFu, needs_warp);
+    if (__ballot_sync(0xFFFFFFFFu, live) == 0) break;
+    // the long directions, one at a time, by the whole warp
+    for (uint32_t m = help; m; m &= m - 1) {
+      const int src = __ffs(m) - 1;
+      XdropDir w;
+      w.q = reinterpret_cast<const uint8_t*>(__shfl_sync(0xFFFFFFFFu, reinterpret_cast<uint64_t>(d.q), src));
+      w.s = reinterpret_cast<const uint8_t*>(__shfl_sync(0xFFFFFFFFu, reinterpret_cast<uint64_t>(d.s), src));
+      w.qa = __shfl_sync(0xFFFFFFFFu, d.qa, src);
+      w.sa = __shfl_sync(0xFFFFFFFFu, d.sa, src);
+      w.bound = __shfl_sync(0xFFFFFFFFu, d.bound, src);
+      w.k = __shfl_sync(0xFFFFFFFFu, d.k, src);
+      w.st = __shfl_sync(0xFFFFFFFFu, d.st, src);
+      w.score = __shfl_sync(0xFFFFFFFFu, d.score, src);
+      w.best = __shfl_sync(0xFFFFFFFFu, d.best, src);
+      w.left = __shfl_sync(0xFFFFFFFFu, (int)d.left, src) != 0;
+      w = xdrop_warp(w, a.xdrop, mat);
+      if ((int)lane == src) d = w;  // the direction has stopped: the lane's loop moves on
+    }
+  }
   warp_sum_atomic(a.xdrop_count, nx);
 }
 

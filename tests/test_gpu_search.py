@@ -276,3 +276,23 @@ def test_autotune_picks_and_caches(tmp_path):
         db.close()
     finally:
         c.close()
+
+
+def test_long_extensions_run_by_the_warp(ctx, orc):
+    """Subjects holding exact or lightly mutated copies of 600-1500-aa queries:
+    their X-drop extensions run hundreds of cells, past the per-lane step
+    limit, so the warp finishes them (k_xdrop_runs); results must equal the
+    oracle's."""
+    r = np.random.Generator(np.random.PCG64(8181))
+    queries = [synth.random_protein(r, int(n)) for n in r.integers(600, 1500, 12)]
+    db = [synth.random_protein(r, int(n)) for n in r.integers(100, 800, 60)]
+    for k, q in enumerate(queries):
+        s = q.copy() if k % 2 == 0 else synth.mutate(r, q, 0.9, indel_rate=0.0)
+        db[5 * k] = np.concatenate([synth.random_protein(r, 40), s, synth.random_protein(r, 30)])
+    dl, do = drgpu.concat(db)
+    tl, to = drgpu.concat(queries)
+    for sens in ("fast", "sensitive"):
+        got, _ = ctx.search(dl, do, tl, to, drgpu.make_config(sensitivity=sens))
+        exp, _ = orc.search(db, queries, sensitivity=sens, threads=8)
+        assert as_tuples(got) == exp
+        assert sum(len(x) for x in exp) >= len(queries)
