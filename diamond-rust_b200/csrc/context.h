@@ -23,7 +23,7 @@ struct drg_ctx {
   std::string err;
   // seed stage
   drg::DevBuf q_keys, q_vals, q_keys_s, q_vals_s, r_keys, r_vals, r_keys_s, r_vals_s, cub_tmp;
-  drg::DevBuf run_keys, run_counts, run_qstart, run_rlo, run_rcount, run_hits, run_hit_off, counters;
+  drg::DevBuf run_keys, run_keys32, run_counts, run_qstart, run_rlo, run_rcount, run_hits, run_hit_off, counters;
   drg::DevBuf q_owner, r_owner, seed_filter, seed_counts, ref_first, hit_coarse, target_hits, run_qlo, run_qcount;
   // hits and ungapped stage
   drg::DevBuf hits, hits_s, hits_u, flags, idx, segs, seg_keys, segs_c, keep;

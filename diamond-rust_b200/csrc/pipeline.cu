@@ -156,16 +156,21 @@ __host__ __device__ __forceinline__ void band_rows(const Band& b, int64_t m, boo
 // After a run-length encoding of n sorted seed keys into io[0] runs (keys
 // rk): io[0] = runs of valid keys (the last run is dropped when it is the
 // "no seed" run), io[1] = valid keys.
-__global__ void k_valid_runs(const uint64_t* keys, uint64_t n, const uint64_t* rk, int64_t* io) {
+template <typename K>
+__global__ void k_valid_runs(const K* keys, uint64_t n, const K* rk, int64_t* io) {
   uint64_t lo = 0, hi = n;
   while (lo < hi) {
     const uint64_t m = (lo + hi) >> 1;
-    if (keys[m] < kNoSeed) lo = m + 1;
+    if (keys[m] < (K)kNoSeed) lo = m + 1;
     else hi = m;
   }
   const int64_t runs = io[0];
-  io[0] = runs > 0 && rk[runs - 1] == kNoSeed ? runs - 1 : runs;
+  io[0] = runs > 0 && rk[runs - 1] == (K)kNoSeed ? runs - 1 : runs;
   io[1] = (int64_t)lo;
+}
+__global__ void k_widen_keys(const uint32_t* in, uint64_t n, uint64_t* out) {
+  const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i < n) out[i] = in[i];
 }
 
 // Sorted band keys: out[0] = keys below kNoSeed (bands the packed kernels
@@ -921,37 +926,58 @@ struct Search {
 void Search::query_seeds(uint64_t* n_runs_out) {
   const int S = (int)shapes.size();
   const uint64_t N = q->total * (uint64_t)S;
-  uint64_t* keys = c->q_keys.as<uint64_t>(N);
   uint32_t* vals = c->q_vals.as<uint32_t>(N);
-  uint64_t* keys_s = c->q_keys_s.as<uint64_t>(N);
   uint32_t* vals_s = c->q_vals_s.as<uint32_t>(N);
-  launch_seed_enum(q->letters, q->offsets, q->owner, 0, q->total, S, keys, vals, c->slot, c->stream, q->request);
-  const int key_bits = q->request ? 64 : seed_key_bits;  // request ids sit above the seed key
-  {
-    // the sorted seeds stay in q_keys_s / q_vals_s (the join reads them there)
-    const SortResult<uint64_t> r = dsort(c, keys, keys_s, vals, vals_s, N, 0, key_bits);
-    if (r.keys != keys_s) {
-      c->q_keys.swap(c->q_keys_s);
-      c->q_vals.swap(c->q_vals_s);
-      keys_s = r.keys;
-    }
-  }
-  // runs of every key (the "no seed" keys, last, form one run of their own),
-  // then the valid keys and their runs counted in one kernel: one wait
   uint64_t* rk = c->run_keys.as<uint64_t>(N + 1);
   uint32_t* rc = c->run_counts.as<uint32_t>(N + 1);
+  int64_t* h = c->h_stage.as<int64_t>(2);
   uint64_t n_runs = 0;
-  if (N > 0) {
-    cub_call(c, [&](void* t, size_t& b) {
-      return cub::DeviceRunLengthEncode::Encode(t, b, keys_s, rk, rc, d_count, (int64_t)N, c->stream);
-    });
-    count_launch();
-    k_valid_runs<<<1, 1, 0, c->stream>>>(keys_s, N, rk, d_count);
-    int64_t* h = c->h_stage.as<int64_t>(2);
-    DRG_CUDA(cudaMemcpyAsync(h, d_count, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
-    DRG_CUDA(cudaStreamSynchronize(c->stream));
-    n_runs = (uint64_t)h[0];
-    st.query_seeds = (uint64_t)h[1];
+  // A seed key of at most 32 bits (and no request ids above it) is sorted as
+  // a 32-bit key: 8 bytes per entry and pass instead of 12.  The sorted
+  // values stay in q_vals_s (the join reads them there); run keys are kept
+  // as 64-bit words either way.
+  if (!q->request && seed_key_bits <= 32) {
+    uint32_t* keys = c->q_keys.as<uint32_t>(N);
+    uint32_t* keys_s = c->q_keys_s.as<uint32_t>(N);
+    launch_seed_enum(q->letters, q->offsets, q->owner, 0, q->total, S, keys, vals, c->slot, c->stream);
+    const SortResult<uint32_t> r = dsort(c, keys, keys_s, vals, vals_s, N, 0, seed_key_bits);
+    if (r.vals != vals_s) c->q_vals.swap(c->q_vals_s);
+    if (N > 0) {
+      uint32_t* rk32 = c->run_keys32.as<uint32_t>(N + 1);
+      cub_call(c, [&](void* t, size_t& b) {
+        return cub::DeviceRunLengthEncode::Encode(t, b, r.keys, rk32, rc, d_count, (int64_t)N, c->stream);
+      });
+      count_launch();
+      k_valid_runs<uint32_t><<<1, 1, 0, c->stream>>>(r.keys, N, rk32, d_count);
+      DRG_CUDA(cudaMemcpyAsync(h, d_count, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
+      DRG_CUDA(cudaStreamSynchronize(c->stream));
+      n_runs = (uint64_t)h[0];
+      st.query_seeds = (uint64_t)h[1];
+      if (n_runs > 0) {
+        count_launch();
+        k_widen_keys<<<ceil_div(n_runs, 256), 256, 0, c->stream>>>(rk32, n_runs, rk);
+      }
+    }
+  } else {
+    uint64_t* keys = c->q_keys.as<uint64_t>(N);
+    uint64_t* keys_s = c->q_keys_s.as<uint64_t>(N);
+    launch_seed_enum(q->letters, q->offsets, q->owner, 0, q->total, S, keys, vals, c->slot, c->stream, q->request);
+    const int key_bits = q->request ? 64 : seed_key_bits;  // request ids sit above the seed key
+    const SortResult<uint64_t> r = dsort(c, keys, keys_s, vals, vals_s, N, 0, key_bits);
+    if (r.vals != vals_s) c->q_vals.swap(c->q_vals_s);
+    // runs of every key (the "no seed" keys, last, form one run of their own),
+    // then the valid keys and their runs counted in one kernel: one wait
+    if (N > 0) {
+      cub_call(c, [&](void* t, size_t& b) {
+        return cub::DeviceRunLengthEncode::Encode(t, b, r.keys, rk, rc, d_count, (int64_t)N, c->stream);
+      });
+      count_launch();
+      k_valid_runs<uint64_t><<<1, 1, 0, c->stream>>>(r.keys, N, rk, d_count);
+      DRG_CUDA(cudaMemcpyAsync(h, d_count, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
+      DRG_CUDA(cudaStreamSynchronize(c->stream));
+      n_runs = (uint64_t)h[0];
+      st.query_seeds = (uint64_t)h[1];
+    }
   }
   uint32_t* qs = c->run_qstart.as<uint32_t>(n_runs + 1);
   if (n_runs > 0)
