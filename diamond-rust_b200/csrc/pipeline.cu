@@ -124,13 +124,18 @@ __host__ __device__ __forceinline__ int sw_class_of(uint32_t w) {
   return w <= (uint32_t)kSwC0 ? 0 : (w <= (uint32_t)kSwC1 ? 1 : (w <= (uint32_t)kSwC2 ? 2 : 3));
 }
 
-// Score-pass sort key, radix-sorted over bits kKeyLo..63:
-//   63 wide band (one warp per band, after every packed-kernel band),
-//   61 transposed band, 24..60 group (target << 16 | window start, or the
-//   subject of a transposed band), 13..23 width.  Not computed here: ~0.
+// Score-pass sort key, radix-sorted over bits kKeyLo..end:
+//   end - 1 wide band (one warp per band, after every packed-kernel band),
+//   end - 2 transposed band, 24..end - 3 group (target << 16 | window start,
+//   or the subject of a transposed band), 13..23 width.  Not computed: ~0.
 // (Medium bands share warps with the narrow bands of their group: giving
 // them warps of their own left most of those warps' lanes idle.)
-constexpr uint64_t kWideKey = 1ull << 63, kTransposedKey = 1ull << 61;
+// The two flags sit right above the group field, whose width the batch sets
+// (SwKeyBits), so the sort covers only the bits the keys use.
+struct SwKeyBits {
+  uint64_t transposed, wide;  // flag bits
+  int end;                    // bits [kKeyLo, end) are sorted
+};
 // Task and band-job sort keys: class or route (< 8) above a cost field whose
 // inverse orders longest first; the order only schedules, so costs saturate.
 constexpr int kCostBits = 24;
@@ -174,8 +179,8 @@ __global__ void k_widen_keys(const uint32_t* in, uint64_t n, uint64_t* out) {
 }
 
 // Sorted band keys: out[0] = keys below kNoSeed (bands the packed kernels
-// take), out[1] = keys below kWideKey (narrow bands, which sort first).
-__global__ void k_count_fast_narrow(const uint64_t* keys, uint64_t n, int64_t* out) {
+// take), out[1] = keys below the wide flag (narrow bands, which sort first).
+__global__ void k_count_fast_narrow(const uint64_t* keys, uint64_t n, uint64_t wide_key, int64_t* out) {
   uint64_t lo = 0, hi = n;
   while (lo < hi) {
     const uint64_t m = (lo + hi) >> 1;
@@ -187,7 +192,7 @@ __global__ void k_count_fast_narrow(const uint64_t* keys, uint64_t n, int64_t* o
   lo = 0;
   while (lo < hi) {
     const uint64_t m = (lo + hi) >> 1;
-    if (keys[m] < kWideKey) lo = m + 1;
+    if (keys[m] < wide_key) lo = m + 1;
     else hi = m;
   }
   out[1] = (int64_t)lo;
@@ -242,7 +247,7 @@ __global__ void k_sw_tr_count(const Band* bands, uint64_t n, const uint64_t* s_o
 // nearly the same rows.
 // rows[i] holds band i's ticket from k_sw_tr_count on entry.
 __global__ void k_sw_keys(const Band* bands, uint64_t n, const uint64_t* s_offsets, int max_score, SwTune tn,
-                          const uint32_t* tr_count, uint64_t* keys, uint32_t* rows, uint32_t* order) {
+                          SwKeyBits kb, const uint32_t* tr_count, uint64_t* keys, uint32_t* rows, uint32_t* order) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   const Band b = bands[i];
@@ -252,10 +257,10 @@ __global__ void k_sw_keys(const Band* bands, uint64_t n, const uint64_t* s_offse
   // of them are transposed, the rest stay with their query windows.
   const bool tr = r.tr && tr_count && rows[i] < (tr_count[b.subject] & ~31u);
   const int64_t rs = tr ? r.ts : r.rs, re = tr ? r.te : r.re;
-  const uint64_t group = tr ? (kTransposedKey | ((uint64_t)b.subject << kGroupShift))
+  const uint64_t group = tr ? (kb.transposed | ((uint64_t)b.subject << kGroupShift))
                             : ((((uint64_t)b.target << 16) | b.q0) << kGroupShift);
   keys[i] = !r.fast ? ~0ull
-                    : r.wide ? (kWideKey | (W << kWidthShift))
+                    : r.wide ? (kb.wide | (W << kWidthShift))
                              : (group | (W << kWidthShift));
   const uint32_t bucket = r.fast ? (uint32_t)(rs >> 4) : 0xFFFFu;
   const uint32_t last = r.fast ? (uint32_t)re : 0u;
@@ -280,14 +285,15 @@ __global__ void k_sw_task_flags(const uint32_t* gstart, uint64_t n, uint8_t* f) 
   if (s < n) f[s] = ((s - gstart[s]) % 32) == 0;
 }
 __global__ void k_sw_fill_tasks(const uint32_t* starts, uint64_t n_tasks, const uint64_t* keys, uint64_t n_fast,
-                                const uint32_t* order, const Band* bands, const uint64_t* s_offsets, bool row_limit,
+                                uint64_t transposed_key, const uint32_t* order, const Band* bands,
+                                const uint64_t* s_offsets, bool row_limit,
                                 SwTask* tasks, uint64_t* sort_key, uint32_t* sort_val, uint64_t* trace_size,
                                 unsigned long long* cells_gpu) {
   uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (t >= n_tasks) return;
   uint32_t s = starts[t];
   const uint64_t grp = keys[s] >> kGroupShift;
-  const bool transposed = (keys[s] & kTransposedKey) != 0;
+  const bool transposed = (keys[s] & transposed_key) != 0;
   uint32_t cnt = 0;
   int64_t row_first = INT64_MAX, row_last = 0;
   uint32_t wmin = 0xFFFFFFFFu, wmax = 0;
@@ -580,21 +586,31 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
                                                                   sw_tune(c), tr_count, rows);
   }
   count_launch();
-  k_sw_keys<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(bc, n_bands, s.offsets, scr.max_score, sw_tune(c),
+  // group field: target << 16 | window start, or the subject (transposed)
+  SwKeyBits kb;
+  {
+    const int gb = std::max(bits_for(qs.h_offsets->size() > 1 ? qs.h_offsets->size() - 2 : 0) + 16,
+                            bits_for(s.h_offsets->size() > 1 ? s.h_offsets->size() - 2 : 0));
+    kb.transposed = 1ull << (kGroupShift + gb);
+    kb.wide = 1ull << (kGroupShift + gb + 1);
+    kb.end = kGroupShift + gb + 2;
+    if (kb.end > 64) throw Error(DRG_ERR_INVALID, "score-pass key needs more than 64 bits");
+  }
+  k_sw_keys<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(bc, n_bands, s.offsets, scr.max_score, sw_tune(c), kb,
                                                            tr_count, swk, rows, swo);
   // rows first, then a stable sort by (target, window, width)
   uint32_t* by_rows = dsort(c, rows, rows_s, swo, swo_r, n_bands, 0, 32).vals;
   count_launch();
   k_gather_keys<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(swk, by_rows, n_bands, swk_r);
   {
-    const SortResult<uint64_t> r = dsort(c, swk_r, swks, by_rows, swos, n_bands, kKeyLo, 64);
+    const SortResult<uint64_t> r = dsort(c, swk_r, swks, by_rows, swos, n_bands, kKeyLo, kb.end);
     swks = r.keys;
     swos = r.vals;
   }
   uint64_t n_fast = 0, n_narrow = 0;
   {
     count_launch();
-    k_count_fast_narrow<<<1, 1, 0, c->stream>>>(swks, n_bands, d_count);
+    k_count_fast_narrow<<<1, 1, 0, c->stream>>>(swks, n_bands, kb.wide, d_count);
     int64_t* h = c->h_stage.as<int64_t>(2);
     DRG_CUDA(cudaMemcpyAsync(h, d_count, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
     DRG_CUDA(cudaStreamSynchronize(c->stream));
@@ -655,9 +671,9 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
       uint32_t* tval = c->task_val.as<uint32_t>(n_tasks);
       uint32_t* tval_s = c->task_val_s.as<uint32_t>(n_tasks);
       count_launch();
-      k_sw_fill_tasks<<<ceil_div(n_tasks, 128), 128, 0, c->stream>>>(tstart, n_tasks, swks, n_narrow, swos, bc,
-                                                                      s.offsets, false, tasks_u, tkey, tval, nullptr,
-                                                                      cells_gpu);
+      k_sw_fill_tasks<<<ceil_div(n_tasks, 128), 128, 0, c->stream>>>(tstart, n_tasks, swks, n_narrow,
+                                                                      kb.transposed, swos, bc, s.offsets, false,
+                                                                      tasks_u, tkey, tval, nullptr, cells_gpu);
       // by width class, longest warps first within a class
       const uint32_t* task_order = dsort(c, tkey, tkey_s, tval, tval_s, n_tasks, 0, kCostBits + 2).vals;
       count_launch();
