@@ -138,7 +138,7 @@ struct SwKeyBits {
 };
 // Task and band-job sort keys: class or route (< 8) above a cost field whose
 // inverse orders longest first; the order only schedules, so costs saturate.
-constexpr int kCostBits = 24;
+constexpr int kCostBits = 21;  // 2M column steps: above any warp but the rarest, so the keys sort in 3 passes
 constexpr uint64_t kCostMax = (1ull << kCostBits) - 1;
 constexpr int kGroupShift = 24, kWidthShift = 13, kKeyLo = 13;
 
@@ -326,7 +326,7 @@ __global__ void k_sw_fill_tasks(const uint32_t* starts, uint64_t n_tasks, const 
   tasks[t] = k;
   const uint64_t steps = (uint64_t)k.n_strips * (wmax + 16ull);
   const int cls = sw_class_of(wmax);
-  // class, then longest first (a scheduling order: 24 bits of steps, saturated, suffice)
+  // class, then longest first (a scheduling order: 21 bits of steps, saturated, suffice)
   sort_key[t] = ((uint64_t)cls << kCostBits) | (kCostMax - (steps < kCostMax ? steps : kCostMax));
   sort_val[t] = (uint32_t)t;
   if (trace_size) trace_size[t] = steps * 32ull;
