@@ -1081,17 +1081,25 @@ void Search::join_chunk(uint64_t c0, uint64_t c1, uint64_t n_runs) {
                                 vals, cnt, c->slot, c->stream);
     }
     // the kept count stays on the device: the sort, the bucket starts and the
-    // join read it there (no host wait); the valid count joins the counters
-    d_nr = reinterpret_cast<const uint64_t*>(cnt);
-    nr = (int64_t)N;  // capacity
+    // join read it there (no host wait); the valid count joins the counters.
+    // A chunk with more seed positions than one sort takes (2^30) reads the
+    // kept count first (the kept seeds are the ones its queries can join).
     count_launch();
     k_add_u64<<<1, 1, 0, c->stream>>>(d_counters + 7, cnt + 1);
+    uint64_t n_sort = N;
+    if (N < (1ull << 30)) {
+      d_nr = reinterpret_cast<const uint64_t*>(cnt);
+      nr = (int64_t)N;  // capacity
+    } else {
+      nr = (int64_t)fetch(c, cnt);
+      n_sort = (uint64_t)nr;
+    }
     if (key32) {
-      const SortResult<uint32_t> r = dsort(c, k32, ks32, vals, vs, N, 0, seed_key_bits, d_nr);
+      const SortResult<uint32_t> r = dsort(c, k32, ks32, vals, vs, n_sort, 0, seed_key_bits, d_nr);
       ks32 = r.keys;
       vs = r.vals;
     } else {
-      const SortResult<uint64_t> r = dsort(c, k64, ks64, vals, vs, N, 0, seed_key_bits, d_nr);
+      const SortResult<uint64_t> r = dsort(c, k64, ks64, vals, vs, n_sort, 0, seed_key_bits, d_nr);
       ks64 = r.keys;
       vs = r.vals;
     }
