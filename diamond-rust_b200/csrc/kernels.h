@@ -170,13 +170,20 @@ struct SegmentOut {  // ungapped.rs:11-17 plus the hit key it came from
 };
 
 // flags[i] = 1 when hit i starts a new (target, subject, diagonal) run.
-void launch_run_heads(const uint64_t* keys, uint64_t n, int shift, uint8_t* flags, cudaStream_t st);
+// flags[i] = 1 where key i >> shift differs from key i - 1 (i < n); with
+// d_n, n is *d_n and flags[i] = 0 for i in [*d_n, n).
+void launch_run_heads(const uint64_t* keys, uint64_t n, int shift, uint8_t* flags, cudaStream_t st,
+                      const int64_t* d_n = nullptr);
 
 struct XdropArgs {
   const uint64_t* hit_keys;
   uint64_t n_hits;
   const uint32_t* run_head_idx;  // compacted indices of run heads
   uint64_t n_runs;
+  // when set, n_hits / n_runs are device words written by earlier launches
+  // (the host values above then only bound them and size the grid)
+  const int64_t* d_n_hits;
+  const int64_t* d_n_runs;
   HitKeyLayout layout;
   const uint8_t* q_letters;
   const uint64_t* q_offsets;
@@ -213,6 +220,7 @@ struct BandArgs {
   uint64_t n_segs;
   const uint32_t* pair_head_idx;  // compacted indices of pair heads (n_pairs + 1, last = n_segs)
   uint64_t n_pairs;
+  const int64_t* d_n_pairs;  // when set, the pair count is this device word (n_pairs bounds it)
   HitKeyLayout layout;
   const uint64_t* q_offsets;
   Band* bands;     // indexed like segments

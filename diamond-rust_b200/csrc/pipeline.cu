@@ -62,6 +62,16 @@ void fetch_n(drg_ctx* c, std::vector<T>& out, const T* d, size_t n) {
   DRG_CUDA(cudaStreamSynchronize(c->stream));
 }
 
+// Indices i < n with flags[i] != 0, in order; their count goes to the
+// device word d_count (no wait).
+void select_indices_dev(drg_ctx* c, const uint8_t* flags, uint64_t n, uint32_t* out, int64_t* d_count) {
+  if (n == 0) return;
+  thrust::counting_iterator<uint32_t> it(0);
+  cub_call(c, [&](void* t, size_t& b) {
+    return cub::DeviceSelect::Flagged(t, b, it, flags, out, d_count, (int64_t)n, c->stream);
+  });
+}
+
 // Indices i < n with flags[i] != 0, in order.
 uint64_t select_indices(drg_ctx* c, const uint8_t* flags, uint64_t n, uint32_t* out, int64_t* d_count) {
   if (n == 0) return 0;
@@ -113,12 +123,15 @@ int64_t count_valid(drg_ctx* c, const K* keys, uint64_t n, int64_t* d_tmp) {
 
 __global__ void k_set_u64(uint64_t* p, uint64_t v) { *p = v; }
 __global__ void k_add_u64(unsigned long long* p, const unsigned long long* v) { *p += *v; }
-__global__ void k_set_u32(uint32_t* p, uint32_t v) { *p = v; }
 
-__global__ void k_rank0_flags(const Band* b, uint64_t n, uint8_t* f) {
+// flags of each pair's first band, over a bound n of the device count *d_n
+// (0 past the count)
+__global__ void k_rank0_flags_dev(const Band* b, uint64_t n, const int64_t* d_n, uint8_t* f) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (i < n) f[i] = b[i].rank == 0;
+  if (i < n) f[i] = i < (uint64_t)*d_n && b[i].rank == 0;
 }
+// p[*at] = *v (an index array's end marker at a device-side count)
+__global__ void k_set_at(uint32_t* p, const int64_t* at, const int64_t* v) { p[*at] = (uint32_t)*v; }
 
 __host__ __device__ __forceinline__ int sw_class_of(uint32_t w) {
   return w <= (uint32_t)kSwC0 ? 0 : (w <= (uint32_t)kSwC1 ? 1 : (w <= (uint32_t)kSwC2 ? 2 : 3));
@@ -1250,30 +1263,39 @@ void Search::process_hits(uint64_t pass_id) {
   if (n_hits == 0) return;
   const HitKeyLayout L = layout();
   const uint64_t* hk = acc;
+  // The stages up to the score pass run on counts that stay on the device
+  // (unique hits, diagonal runs, kept segments, pairs, bands), each bounded
+  // by n_hits: every buffer is sized for n_hits, each kernel reads its count
+  // from dc, and one wait at the end reads them all.
+  //   dc[0] unique hits  [1] diagonal runs  [2] kept segments  [3] pairs
+  //   [4] bands  [5] pair starts
+  int64_t* dc = c->pass_counts.as<int64_t>(8);
+  DRG_CUDA(cudaMemsetAsync(dc, 0, 8 * sizeof(int64_t), c->stream));
   // ---- sort + unique hits
   tm.start();
   uint64_t* hs = c->hits_s.as<uint64_t>(n_hits);
   uint64_t* hu = c->hits_u.as<uint64_t>(n_hits);
   hs = dsort<uint64_t>(c, const_cast<uint64_t*>(hk), hs, nullptr, nullptr, n_hits, 0, L.total()).keys;
   cub_call(c, [&](void* t, size_t& b) {
-    return cub::DeviceSelect::Unique(t, b, hs, hu, d_count, (int64_t)n_hits, c->stream);
+    return cub::DeviceSelect::Unique(t, b, hs, hu, dc + 0, (int64_t)n_hits, c->stream);
   });
-  const uint64_t n_u = (uint64_t)fetch(c, d_count);
-  st.unique_hits += n_u;
   tm.stop(&st.ms_sort);
   // ---- ungapped
   tm.start();
-  uint8_t* flags = c->flags.as<uint8_t>(n_u + 1);
-  uint32_t* idx = c->idx.as<uint32_t>(n_u + 1);
-  launch_run_heads(hu, n_u, L.pb, flags, c->stream);
-  const uint64_t n_runs_d = select_indices(c, flags, n_u, idx, d_count);
-  SegmentOut* segs = c->segs.as<SegmentOut>(n_u);
-  uint8_t* keep = c->keep.as<uint8_t>(n_u);
+  uint8_t* flags = c->flags.as<uint8_t>(n_hits + 1);
+  uint32_t* idx = c->idx.as<uint32_t>(n_hits + 1);
+  launch_run_heads(hu, n_hits, L.pb, flags, c->stream, dc + 0);
+  select_indices_dev(c, flags, n_hits, idx, dc + 1);
+  SegmentOut* segs = c->segs.as<SegmentOut>(n_hits);
+  uint8_t* keep = c->keep.as<uint8_t>(n_hits);
+  DRG_CUDA(cudaMemsetAsync(keep, 0, n_hits, c->stream));  // past the unique hits: not kept
   XdropArgs xa{};
   xa.hit_keys = hu;
-  xa.n_hits = n_u;
+  xa.n_hits = n_hits;
   xa.run_head_idx = idx;
-  xa.n_runs = n_runs_d;
+  xa.n_runs = n_hits;
+  xa.d_n_hits = dc + 0;
+  xa.d_n_runs = dc + 1;
   xa.layout = L;
   xa.q_letters = q->letters;
   xa.q_offsets = q->offsets;
@@ -1286,50 +1308,57 @@ void Search::process_hits(uint64_t pass_id) {
   xa.xdrop_count = d_counters + 0;
   xa.slot = c->slot;
   launch_xdrop_runs(xa, c->stream);
-  uint64_t* sk = c->seg_keys.as<uint64_t>(n_u);
-  SegmentOut* sc_ = c->segs_c.as<SegmentOut>(n_u);
+  uint64_t* sk = c->seg_keys.as<uint64_t>(n_hits);
+  SegmentOut* sc_ = c->segs_c.as<SegmentOut>(n_hits);
   cub_call(c, [&](void* t, size_t& b) {
-    return cub::DeviceSelect::Flagged(t, b, hu, keep, sk, d_count, (int64_t)n_u, c->stream);
+    return cub::DeviceSelect::Flagged(t, b, hu, keep, sk, dc + 2, (int64_t)n_hits, c->stream);
   });
-  const uint64_t n_segs = (uint64_t)fetch(c, d_count);
   cub_call(c, [&](void* t, size_t& b) {
-    return cub::DeviceSelect::Flagged(t, b, segs, keep, sc_, d_count, (int64_t)n_u, c->stream);
+    return cub::DeviceSelect::Flagged(t, b, segs, keep, sc_, dc + 2, (int64_t)n_hits, c->stream);
   });
-  st.segments += n_segs;
   tm.stop(&st.ms_ungapped);
-  if (n_segs == 0) return;
   // ---- bands
   tm.start();
-  launch_run_heads(sk, n_segs, L.pb + L.db, flags, c->stream);
-  const uint64_t n_pairs = select_indices(c, flags, n_segs, idx, d_count);
+  launch_run_heads(sk, n_hits, L.pb + L.db, flags, c->stream, dc + 2);
+  select_indices_dev(c, flags, n_hits, idx, dc + 3);
   count_launch();
-  k_set_u32<<<1, 1, 0, c->stream>>>(idx + n_pairs, (uint32_t)n_segs);
-  Band* bands = c->bands.as<Band>(n_segs);
-  uint8_t* bvalid = c->band_valid.as<uint8_t>(n_segs);
+  k_set_at<<<1, 1, 0, c->stream>>>(idx, dc + 3, dc + 2);  // idx[pairs] = segments
+  Band* bands = c->bands.as<Band>(n_hits);
+  uint8_t* bvalid = c->band_valid.as<uint8_t>(n_hits);
+  DRG_CUDA(cudaMemsetAsync(bvalid, 0, n_hits, c->stream));
   BandArgs ba{};
   ba.seg_keys = sk;
   ba.segs = sc_;
-  ba.n_segs = n_segs;
+  ba.n_segs = n_hits;
   ba.pair_head_idx = idx;
-  ba.n_pairs = n_pairs;
+  ba.n_pairs = n_hits;
+  ba.d_n_pairs = dc + 3;
   ba.layout = L;
   ba.q_offsets = q->offsets;
   ba.bands = bands;
   ba.valid = bvalid;
   launch_build_bands(ba, c->stream);
-  Band* bc = c->bands_c.as<Band>(n_segs);
+  Band* bc = c->bands_c.as<Band>(n_hits);
   cub_call(c, [&](void* t, size_t& b) {
-    return cub::DeviceSelect::Flagged(t, b, bands, bvalid, bc, d_count, (int64_t)n_segs, c->stream);
+    return cub::DeviceSelect::Flagged(t, b, bands, bvalid, bc, dc + 4, (int64_t)n_hits, c->stream);
   });
-  const uint64_t n_bands = (uint64_t)fetch(c, d_count);
+  uint32_t* pfirst = c->pair_first.as<uint32_t>(n_hits + 1);
+  count_launch();
+  k_rank0_flags_dev<<<ceil_div(n_hits, 256), 256, 0, c->stream>>>(bc, n_hits, dc + 4, flags);
+  select_indices_dev(c, flags, n_hits, pfirst, dc + 5);
+  count_launch();
+  k_set_at<<<1, 1, 0, c->stream>>>(pfirst, dc + 3, dc + 4);  // pfirst[pairs] = bands
+  // the one wait of these stages: their counts
+  int64_t* hc = c->h_stage.as<int64_t>(8);
+  DRG_CUDA(cudaMemcpyAsync(hc, dc, 8 * sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
+  DRG_CUDA(cudaStreamSynchronize(c->stream));
+  const uint64_t n_u = (uint64_t)hc[0], n_segs = (uint64_t)hc[2], n_pairs = (uint64_t)hc[3],
+                 n_bands = (uint64_t)hc[4];
+  st.unique_hits += n_u;
+  st.segments += n_segs;
   st.bands += n_bands;
-  uint32_t* pfirst = c->pair_first.as<uint32_t>(n_pairs + 1);
-  count_launch();
-  k_rank0_flags<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(bc, n_bands, flags);
-  select_indices(c, flags, n_bands, pfirst, d_count);
-  count_launch();
-  k_set_u32<<<1, 1, 0, c->stream>>>(pfirst + n_pairs, (uint32_t)n_bands);
   tm.stop(&st.ms_bands);
+  if (n_segs == 0 || n_bands == 0) return;
   // ---- banded SW scores
   tm.start();
   int32_t* scores = c->scores.as<int32_t>(n_bands);

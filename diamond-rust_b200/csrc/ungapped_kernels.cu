@@ -71,16 +71,22 @@ __device__ SegmentOut xdrop_dev(const uint8_t* __restrict__ q, uint32_t qlen, co
   return o;
 }
 
-__global__ void k_run_heads(const uint64_t* __restrict__ keys, uint64_t n, int shift, uint8_t* __restrict__ flags) {
+__global__ void k_run_heads(const uint64_t* __restrict__ keys, uint64_t n, int shift, uint8_t* __restrict__ flags,
+                            const int64_t* d_n) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
+  if (d_n && i >= (uint64_t)*d_n) {
+    flags[i] = 0;
+    return;
+  }
   flags[i] = (i == 0 || (keys[i] >> shift) != (keys[i - 1] >> shift)) ? 1 : 0;
 }
 
-void launch_run_heads(const uint64_t* keys, uint64_t n, int shift, uint8_t* flags, cudaStream_t st) {
+void launch_run_heads(const uint64_t* keys, uint64_t n, int shift, uint8_t* flags, cudaStream_t st,
+                      const int64_t* d_n) {
   if (n == 0) return;
   count_launch();
-  k_run_heads<<<ceil_div(n, 256), 256, 0, st>>>(keys, n, shift, flags);
+  k_run_heads<<<ceil_div(n, 256), 256, 0, st>>>(keys, n, shift, flags, d_n);
   DRG_CUDA(cudaGetLastError());
 }
 
@@ -206,6 +212,8 @@ __global__ void k_xdrop_runs(XdropArgs a) {
   const uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   const uint32_t lane = threadIdx.x & 31;
   const HitKeyLayout L = a.layout;
+  if (a.d_n_hits) a.n_hits = (uint64_t)*a.d_n_hits;
+  if (a.d_n_runs) a.n_runs = (uint64_t)*a.d_n_runs;
   bool live = r < a.n_runs;  // the lane still has hits to extend
   uint64_t i = 0, run = 0;
   const uint8_t *q = nullptr, *s = nullptr;
@@ -340,7 +348,7 @@ void launch_xdrop_jobs(const drg_xdrop_job* jobs, uint64_t n, const uint8_t* ql,
 // The window of gapped_hsp (search.rs:303-312) is applied to each band.
 __global__ void k_build_bands(BandArgs a) {
   uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (p >= a.n_pairs) return;
+  if (p >= a.n_pairs || (a.d_n_pairs && p >= (uint64_t)*a.d_n_pairs)) return;
   const HitKeyLayout L = a.layout;
   uint64_t b = a.pair_head_idx[p], e = a.pair_head_idx[p + 1];
   const uint64_t k0 = a.seg_keys[b];
