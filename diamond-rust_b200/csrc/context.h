@@ -38,7 +38,7 @@ struct drg_ctx {
   // blastx front end
   drg::DevBuf x_nt, x_nt_off, x_len, x_scratch_off, x_scratch, x_keep, x_kept_len, x_kept_index, x_kept_off,
       x_query, x_frame;
-  drg::DevBuf pass_counts;             // device-side counts of one pass of the stages after the join
+  drg::DevBuf pass_counts, sw_counts;             // device-side counts of one pass of the stages after the join
   drg::DevBuf sort_tmp, sort_err;  // radix sort scratch; its wait-timeout word (checked after the work)
   drg_tuning tuning{273, 17, 1, 0};  // tile and routing choices (include/drgpu.h)
   drg::HostBuf h_stage;

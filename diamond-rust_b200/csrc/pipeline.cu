@@ -288,21 +288,24 @@ __device__ __forceinline__ int64_t band_first_row(const Band& b) { return b.d0 +
 
 // Task heads: first band of each (target, window) group and every 32nd after
 // (a group's bands are in width order, so a warp's widths are close).
-__global__ void k_sw_group_start(const uint64_t* keys, uint64_t n, uint32_t* gstart) {
+// (d_n: the count is *d_n, n bounds it)
+__global__ void k_sw_group_start(const uint64_t* keys, uint64_t n, uint32_t* gstart, const int64_t* d_n) {
   uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (s >= n) return;
+  if (s >= n || (d_n && s >= (uint64_t)*d_n)) return;
   gstart[s] = (s == 0 || (keys[s] >> kGroupShift) != (keys[s - 1] >> kGroupShift)) ? (uint32_t)s : 0u;
 }
-__global__ void k_sw_task_flags(const uint32_t* gstart, uint64_t n, uint8_t* f) {
+__global__ void k_sw_task_flags(const uint32_t* gstart, uint64_t n, uint8_t* f, const int64_t* d_n) {
   uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (s < n) f[s] = ((s - gstart[s]) % 32) == 0;
+  if (s < n) f[s] = (!d_n || s < (uint64_t)*d_n) && ((s - gstart[s]) % 32) == 0;
 }
 __global__ void k_sw_fill_tasks(const uint32_t* starts, uint64_t n_tasks, const uint64_t* keys, uint64_t n_fast,
                                 uint64_t transposed_key, const uint32_t* order, const Band* bands,
                                 const uint64_t* s_offsets, bool row_limit,
                                 SwTask* tasks, uint64_t* sort_key, uint32_t* sort_val, uint64_t* trace_size,
-                                unsigned long long* cells_gpu) {
+                                unsigned long long* cells_gpu, const int64_t* d_n_tasks, const int64_t* d_n_fast) {
   uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (d_n_tasks) n_tasks = (uint64_t)*d_n_tasks;
+  if (d_n_fast) n_fast = (uint64_t)*d_n_fast;
   if (t >= n_tasks) return;
   uint32_t s = starts[t];
   const uint64_t grp = keys[s] >> kGroupShift;
@@ -349,13 +352,14 @@ __global__ void k_sw_fill_tasks(const uint32_t* starts, uint64_t n_tasks, const 
   }
 }
 
-__global__ void k_gather_tasks(const SwTask* in, const uint32_t* idx, uint64_t n, SwTask* out) {
+__global__ void k_gather_tasks(const SwTask* in, const uint32_t* idx, uint64_t n, SwTask* out, const int64_t* d_n) {
   uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (t < n) out[t] = in[idx[t]];
+  if (t < n && (!d_n || t < (uint64_t)*d_n)) out[t] = in[idx[t]];
 }
 
 // First task of classes 1, 2 and 3 (tasks are sorted by class).
-__global__ void k_task_bounds(const SwTask* tasks, uint64_t n, int64_t* out) {
+__global__ void k_task_bounds(const SwTask* tasks, uint64_t n, int64_t* out, const int64_t* d_n) {
+  if (d_n) n = (uint64_t)*d_n;
   for (int c = 0; c < kSwClasses - 1; ++c) {
     uint64_t lo = 0, hi = n;
     while (lo < hi) {
@@ -368,9 +372,9 @@ __global__ void k_task_bounds(const SwTask* tasks, uint64_t n, int64_t* out) {
 }
 
 // Longest warp of each width class, in column steps (strips x (W + 16)).
-__global__ void k_task_steps(const SwTask* tasks, uint64_t n, unsigned long long* mx) {
+__global__ void k_task_steps(const SwTask* tasks, uint64_t n, unsigned long long* mx, const int64_t* d_n) {
   uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (t >= n) return;
+  if (t >= n || (d_n && t >= (uint64_t)*d_n)) return;
   const SwTask k = tasks[t];
   atomicMax(mx + sw_class_of(k.width), (unsigned long long)k.n_strips * (k.width + 16ull));
 }
@@ -392,11 +396,10 @@ __global__ void k_compact_ops(const uint32_t* ops, const uint64_t* ops_off, cons
 
 // Jobs of the one-warp-per-band kernel for the first n bands of the sorted
 // order: rows [rs, re] (re limited to the best row when known), longest first.
-__global__ void k_band_jobs(const uint32_t* order, const uint64_t* keys, uint64_t n, const Band* bands,
-                            const uint64_t* s_offsets, bool trace, SwBandJob* jobs, uint64_t* sort_key,
-                            uint32_t* sort_val, unsigned long long* max_width) {
-  uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (k >= n) return;
+// The job of sorted band k (order[k] indexes bands) and its sort key.
+__device__ __forceinline__ void band_job(const uint32_t* order, uint64_t k, const Band* bands,
+                                         const uint64_t* s_offsets, bool trace, SwBandJob* jobs, uint64_t* sort_key,
+                                         uint32_t* sort_val, unsigned long long* max_width) {
   const uint32_t i = order[k];
   const Band b = bands[i];
   const int64_t m = (int64_t)(s_offsets[b.subject + 1] - s_offsets[b.subject]);
@@ -420,9 +423,30 @@ __global__ void k_band_jobs(const uint32_t* order, const uint64_t* keys, uint64_
   atomicMax(max_width, (unsigned long long)W);
   atomicAdd(max_width + 1 + route, 1ull);
 }
-__global__ void k_gather_band_jobs(const SwBandJob* in, const uint32_t* idx, uint64_t n, SwBandJob* out,
-                                   uint64_t* size) {
+__global__ void k_band_jobs(const uint32_t* order, const uint64_t* keys, uint64_t n, const Band* bands,
+                            const uint64_t* s_offsets, bool trace, SwBandJob* jobs, uint64_t* sort_key,
+                            uint32_t* sort_val, unsigned long long* max_width) {
   uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (k < n) band_job(order, k, bands, s_offsets, trace, jobs, sort_key, sort_val, max_width);
+}
+// Score pass on device counts: the wide bands are sorted positions
+// [cnt[1], cnt[0]) (after the narrow ones); n bounds their count, which is
+// also written to cnt[15] for the job sort.
+__global__ void k_band_jobs_dev(const uint32_t* order, int64_t* cnt, uint64_t n, const Band* bands,
+                                const uint64_t* s_offsets, SwBandJob* jobs, uint64_t* sort_key, uint32_t* sort_val,
+                                unsigned long long* max_width) {
+  uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t n_wide = (uint64_t)(cnt[0] - cnt[1]);
+  if (k == 0) cnt[15] = (int64_t)n_wide;
+  if (k < n && k < n_wide) band_job(order + cnt[1], k, bands, s_offsets, false, jobs, sort_key, sort_val, max_width);
+}
+__global__ void k_gather_band_jobs(const SwBandJob* in, const uint32_t* idx, uint64_t n, SwBandJob* out,
+                                   uint64_t* size, const int64_t* d_n = nullptr) {
+  uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (d_n) {  // device count: no sizes
+    if (k < n && k < (uint64_t)*d_n) out[k] = in[idx[k]];
+    return;
+  }
   if (k < n) {
     const SwBandJob j = in[idx[k]];
     out[k] = j;
@@ -621,157 +645,181 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
     swos = r.vals;
   }
   uint64_t n_fast = 0, n_narrow = 0;
-  {
-    count_launch();
-    k_count_fast_narrow<<<1, 1, 0, c->stream>>>(swks, n_bands, kb.wide, d_count);
+  // score pass counts, on the device until the one wait before the launches:
+  //   [0] fast bands  [1] narrow bands  [2] tasks  [3..5] class bounds
+  //   [6] wide max width  [7..10] wide jobs per route  [11..14] longest warp
+  //   per class  [15] wide bands
+  int64_t* cnt = c->sw_counts.as<int64_t>(16);
+  DRG_CUDA(cudaMemsetAsync(cnt, 0, 16 * sizeof(int64_t), c->stream));
+  count_launch();
+  k_count_fast_narrow<<<1, 1, 0, c->stream>>>(swks, n_bands, kb.wide, cnt);
+  TraceBand* tb = nullptr;
+  if (trace) {
     int64_t* h = c->h_stage.as<int64_t>(2);
-    DRG_CUDA(cudaMemcpyAsync(h, d_count, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
+    DRG_CUDA(cudaMemcpyAsync(h, cnt, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
     DRG_CUDA(cudaStreamSynchronize(c->stream));
     n_fast = (uint64_t)h[0];
     n_narrow = (uint64_t)h[1];
-  }
-  TraceBand* tb = nullptr;
-  if (trace) {
     tb = c->tband.as<TraceBand>(n_bands);
     DRG_CUDA(cudaMemsetAsync(tb, 0xFF, n_bands * sizeof(TraceBand), c->stream));  // score -1: not traced
-  }
-  if (n_fast > 0 && trace) {
-    // traceback: one warp per band (few, long bands)
-    const BandJobs bj = make_band_jobs(c, swos, swks, n_fast, bc, s.offsets, true);
-    SwBandArgs ba = band_args(bc, bj, qs, s, scr);
-    ba.trace = c->trace.as<uint2>(bj.trace_words + 8);  // the walk reads 8-word windows
-    ba.tband = tb;
-    cudaEvent_t e0 = log->event(), e1 = log->event();
-    DRG_CUDA(cudaEventRecord(e0, c->stream));
-    // each band's walk (gapped.rs:205-279) runs in the band kernel right
-    // after its DP
-    ba.walk.trace = ba.trace;
-    ba.walk.q_letters = qs.letters;
-    ba.walk.q_offsets = qs.offsets;
-    ba.walk.s_letters = s.letters;
-    ba.walk.s_offsets = s.offsets;
-    ba.walk.ops_off = d_ops_off;
-    ba.walk.rev = c->rev.as<uint8_t>((*h_ops_off)[n_bands] + 16);
-    ba.walk.ops = ops;
-    ba.walk.out = out;
-    ba.walk.exact_below = scr.max_score + 1;
-    launch_band_routes(ba, bj, true, c->stream);
-    DRG_CUDA(cudaEventRecord(e1, c->stream));
-    log->span(e0, e1, &st.ms_trace_kernel);
-  } else if (n_fast > 0) {
-    // score pass: warps of 32 narrow bands (packed inter-band kernel) and, on
-    // the side stream, one warp per band for the wide ones
-    const BandJobs wide = make_band_jobs(c, swos + n_narrow, swks + n_narrow, n_fast - n_narrow, bc, s.offsets,
-                                         false);
-    uint64_t n_tasks = 0;
-    SwTask* tasks = nullptr;
-    int64_t bounds[kSwClasses - 1] = {0, 0, 0};
-    if (n_narrow > 0) {
-      uint32_t* gstart = c->idx.as<uint32_t>(n_narrow + 1);
-      count_launch();
-      k_sw_group_start<<<ceil_div(n_narrow, 256), 256, 0, c->stream>>>(swks, n_narrow, gstart);
-      cub_call(c, [&](void* t, size_t& b) {
-        return cub::DeviceScan::InclusiveScan(t, b, gstart, gstart, cub::Max(), (int64_t)n_narrow, c->stream);
-      });
-      count_launch();
-      k_sw_task_flags<<<ceil_div(n_narrow, 256), 256, 0, c->stream>>>(gstart, n_narrow, flags);
-      uint32_t* tstart = c->sel_idx.as<uint32_t>(n_narrow + 1);
-      n_tasks = select_indices(c, flags, n_narrow, tstart, d_count);
-      SwTask* tasks_u = c->sw_tasks_u.as<SwTask>(n_tasks);
-      tasks = c->sw_tasks.as<SwTask>(n_tasks);
-      uint64_t* tkey = c->task_key.as<uint64_t>(n_tasks);
-      uint64_t* tkey_s = c->task_key_s.as<uint64_t>(n_tasks);
-      uint32_t* tval = c->task_val.as<uint32_t>(n_tasks);
-      uint32_t* tval_s = c->task_val_s.as<uint32_t>(n_tasks);
-      count_launch();
-      k_sw_fill_tasks<<<ceil_div(n_tasks, 128), 128, 0, c->stream>>>(tstart, n_tasks, swks, n_narrow,
-                                                                      kb.transposed, swos, bc, s.offsets, false,
-                                                                      tasks_u, tkey, tval, nullptr, cells_gpu);
-      // by width class, longest warps first within a class
-      const uint32_t* task_order = dsort(c, tkey, tkey_s, tval, tval_s, n_tasks, 0, kCostBits + 2).vals;
-      count_launch();
-      k_gather_tasks<<<ceil_div(n_tasks, 256), 256, 0, c->stream>>>(tasks_u, task_order, n_tasks, tasks);
-      // task_max holds the per-class step maxima, then the class bounds
-      int64_t* dbounds = reinterpret_cast<int64_t*>(c->task_max.as<unsigned long long>(2 * kSwClasses)) + kSwClasses;
-      count_launch();
-      k_task_bounds<<<1, 1, 0, c->stream>>>(tasks, n_tasks, dbounds);
-      DRG_CUDA(cudaMemcpyAsync(bounds, dbounds, sizeof(bounds), cudaMemcpyDeviceToHost, c->stream));
+    if (n_fast > 0) {
+      // traceback: one warp per band (few, long bands)
+      const BandJobs bj = make_band_jobs(c, swos, swks, n_fast, bc, s.offsets, true);
+      SwBandArgs ba = band_args(bc, bj, qs, s, scr);
+      ba.trace = c->trace.as<uint2>(bj.trace_words + 8);  // the walk reads 8-word windows
+      ba.tband = tb;
+      cudaEvent_t e0 = log->event(), e1 = log->event();
+      DRG_CUDA(cudaEventRecord(e0, c->stream));
+      // each band's walk (gapped.rs:205-279) runs in the band kernel right
+      // after its DP
+      ba.walk.trace = ba.trace;
+      ba.walk.q_letters = qs.letters;
+      ba.walk.q_offsets = qs.offsets;
+      ba.walk.s_letters = s.letters;
+      ba.walk.s_offsets = s.offsets;
+      ba.walk.ops_off = d_ops_off;
+      ba.walk.rev = c->rev.as<uint8_t>((*h_ops_off)[n_bands] + 16);
+      ba.walk.ops = ops;
+      ba.walk.out = out;
+      ba.walk.exact_below = scr.max_score + 1;
+      launch_band_routes(ba, bj, true, c->stream);
+      DRG_CUDA(cudaEventRecord(e1, c->stream));
+      log->span(e0, e1, &st.ms_trace_kernel);
     }
-    unsigned long long* dmax = c->task_max.as<unsigned long long>(2 * kSwClasses);
-    DRG_CUDA(cudaMemsetAsync(dmax, 0, kSwClasses * sizeof(unsigned long long), c->stream));
-    if (n_tasks > 0) {
-      count_launch();
-      k_task_steps<<<ceil_div(n_tasks, 256), 256, 0, c->stream>>>(tasks, n_tasks, dmax);
-    }
-    unsigned long long hmax[kSwClasses];
-    DRG_CUDA(cudaMemcpyAsync(hmax, dmax, sizeof(hmax), cudaMemcpyDeviceToHost, c->stream));
+  } else {
+    // ---- wide bands (positions [narrow, fast) of the sorted order): band-
+    // kernel jobs by route, then longest first
+    SwBandJob* jobs_u = c->band_jobs_u.as<SwBandJob>(n_bands);
+    SwBandJob* wjobs = c->band_jobs.as<SwBandJob>(n_bands);
+    uint64_t* jkey = c->bj_key.as<uint64_t>(n_bands);
+    uint64_t* jkey_s = c->bj_key_s.as<uint64_t>(n_bands);
+    uint32_t* jval = c->bj_val.as<uint32_t>(n_bands);
+    uint32_t* jval_s = c->bj_val_s.as<uint32_t>(n_bands);
+    count_launch();
+    k_band_jobs_dev<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(
+        swos, cnt, n_bands, bc, s.offsets, jobs_u, jkey, jval, reinterpret_cast<unsigned long long*>(cnt + 6));
+    const uint32_t* jorder =
+        dsort(c, jkey, jkey_s, jval, jval_s, n_bands, 0, kCostBits + 3, reinterpret_cast<const uint64_t*>(cnt + 15))
+            .vals;
+    count_launch();
+    k_gather_band_jobs<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(jobs_u, jorder, n_bands, wjobs, nullptr,
+                                                                        cnt + 15);
+    // ---- narrow bands: warps of up to 32 bands of one group
+    uint32_t* gstart = c->idx.as<uint32_t>(n_bands + 1);
+    count_launch();
+    k_sw_group_start<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(swks, n_bands, gstart, cnt + 1);
+    cub_call(c, [&](void* t, size_t& b) {
+      return cub::DeviceScan::InclusiveScan(t, b, gstart, gstart, cub::Max(), (int64_t)n_bands, c->stream);
+    });
+    count_launch();
+    k_sw_task_flags<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(gstart, n_bands, flags, cnt + 1);
+    uint32_t* tstart = c->sel_idx.as<uint32_t>(n_bands + 1);
+    select_indices_dev(c, flags, n_bands, tstart, cnt + 2);
+    SwTask* tasks_u = c->sw_tasks_u.as<SwTask>(n_bands);
+    SwTask* tasks = c->sw_tasks.as<SwTask>(n_bands);
+    uint64_t* tkey = c->task_key.as<uint64_t>(n_bands);
+    uint64_t* tkey_s = c->task_key_s.as<uint64_t>(n_bands);
+    uint32_t* tval = c->task_val.as<uint32_t>(n_bands);
+    uint32_t* tval_s = c->task_val_s.as<uint32_t>(n_bands);
+    count_launch();
+    k_sw_fill_tasks<<<ceil_div(n_bands, 128), 128, 0, c->stream>>>(tstart, n_bands, swks, n_bands, kb.transposed,
+                                                                    swos, bc, s.offsets, false, tasks_u, tkey, tval,
+                                                                    nullptr, cells_gpu, cnt + 2, cnt + 1);
+    // by width class, longest warps first within a class
+    const uint32_t* task_order =
+        dsort(c, tkey, tkey_s, tval, tval_s, n_bands, 0, kCostBits + 2, reinterpret_cast<const uint64_t*>(cnt + 2))
+            .vals;
+    count_launch();
+    k_gather_tasks<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(tasks_u, task_order, n_bands, tasks, cnt + 2);
+    count_launch();
+    k_task_bounds<<<1, 1, 0, c->stream>>>(tasks, n_bands, cnt + 3, cnt + 2);
+    count_launch();
+    k_task_steps<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(tasks, n_bands,
+                                                                 reinterpret_cast<unsigned long long*>(cnt + 11),
+                                                                 cnt + 2);
+    // ---- the one wait: every count the launches need
+    int64_t* h = c->h_stage.as<int64_t>(16);
+    DRG_CUDA(cudaMemcpyAsync(h, cnt, 16 * sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
     DRG_CUDA(cudaStreamSynchronize(c->stream));
-    SwScoreArgs sa{};
-    sa.bands = bc;
-    sa.order = swos;
-    sa.tasks = tasks;
-    sa.q_letters = qs.dp_letters();
-    sa.q_offsets = qs.offsets;
-    sa.s_letters = s.dp_letters();
-    sa.s_offsets = s.offsets;
-    sa.gap_open = scr.gap_open;
-    sa.gap_extend = scr.gap_extend;
-    sa.score = scores;
-    sa.best_row = best_row;
-    sa.cells_eval = cells_gpu;
-    std::memcpy(sa.scores625, scr.scores, 625);
-    uint64_t lo[kSwClasses], hi[kSwClasses];
-    for (int k = 0; k < kSwClasses; ++k) {
-      lo[k] = k == 0 ? 0 : (uint64_t)bounds[k - 1];
-      hi[k] = k == kSwClasses - 1 ? n_tasks : (uint64_t)bounds[k];
-    }
-    // The bulk class runs on the main stream; the wider classes and the wide
-    // bands run on the side stream, queued first so that the long warps start
-    // early and the pass ends on the bulk class's shortest tasks.
-    std::array<cudaEvent_t, 2 * kSwClasses + 3> ev;
-    for (auto& e : ev) e = log->event();
-    const int fork = 2 * kSwClasses, wide0 = fork + 1, wide1 = fork + 2;
-    DRG_CUDA(cudaEventRecord(ev[fork], c->stream));
-    DRG_CUDA(cudaStreamWaitEvent(c->side, ev[fork], 0));
-    auto launch_cls = [&](int cls) {
-      cudaStream_t sc = cls == 0 ? c->stream : c->side;
-      sa.task_lo = lo[cls];
-      sa.task_hi = hi[cls];
-      DRG_CUDA(cudaEventRecord(ev[2 * cls], sc));
-      if (hi[cls] > lo[cls]) {
-        launch_sw_class(sa, cls, sc);
+    n_fast = (uint64_t)h[0];
+    n_narrow = (uint64_t)h[1];
+    const uint64_t n_tasks = (uint64_t)h[2];
+    int64_t bounds[kSwClasses - 1] = {h[3], h[4], h[5]};
+    unsigned long long hmax[kSwClasses];
+    for (int k = 0; k < kSwClasses; ++k) hmax[k] = (unsigned long long)h[11 + k];
+    BandJobs wide;
+    wide.jobs = wjobs;
+    wide.n = n_fast - n_narrow;
+    wide.max_width = (int)h[6];
+    for (int k = 0; k < 4; ++k) wide.route_lo[k + 1] = wide.route_lo[k] + (uint64_t)h[7 + k];
+    if (n_fast > 0) {
+      SwScoreArgs sa{};
+      sa.bands = bc;
+      sa.order = swos;
+      sa.tasks = tasks;
+      sa.q_letters = qs.dp_letters();
+      sa.q_offsets = qs.offsets;
+      sa.s_letters = s.dp_letters();
+      sa.s_offsets = s.offsets;
+      sa.gap_open = scr.gap_open;
+      sa.gap_extend = scr.gap_extend;
+      sa.score = scores;
+      sa.best_row = best_row;
+      sa.cells_eval = cells_gpu;
+      std::memcpy(sa.scores625, scr.scores, 625);
+      uint64_t lo[kSwClasses], hi[kSwClasses];
+      for (int k = 0; k < kSwClasses; ++k) {
+        lo[k] = k == 0 ? 0 : (uint64_t)bounds[k - 1];
+        hi[k] = k == kSwClasses - 1 ? n_tasks : (uint64_t)bounds[k];
+      }
+      // The bulk class runs on the main stream; the wider classes and the wide
+      // bands run on the side stream, queued first so that the long warps start
+      // early and the pass ends on the bulk class's shortest tasks.
+      std::array<cudaEvent_t, 2 * kSwClasses + 3> ev;
+      for (auto& e : ev) e = log->event();
+      const int fork = 2 * kSwClasses, wide0 = fork + 1, wide1 = fork + 2;
+      DRG_CUDA(cudaEventRecord(ev[fork], c->stream));
+      DRG_CUDA(cudaStreamWaitEvent(c->side, ev[fork], 0));
+      auto launch_cls = [&](int cls) {
+        cudaStream_t sc = cls == 0 ? c->stream : c->side;
+        sa.task_lo = lo[cls];
+        sa.task_hi = hi[cls];
+        DRG_CUDA(cudaEventRecord(ev[2 * cls], sc));
+        if (hi[cls] > lo[cls]) {
+          launch_sw_class(sa, cls, sc);
+          st.sw_launches += 1;
+        }
+        DRG_CUDA(cudaEventRecord(ev[2 * cls + 1], sc));
+      };
+      DRG_CUDA(cudaEventRecord(ev[wide0], c->side));
+      if (wide.n > 0) {
+        SwBandArgs ba = band_args(bc, wide, qs, s, scr);
+        ba.score = scores;
+        ba.best_row = best_row;
+        launch_band_routes(ba, wide, false, c->side);
         st.sw_launches += 1;
       }
-      DRG_CUDA(cudaEventRecord(ev[2 * cls + 1], sc));
-    };
-    DRG_CUDA(cudaEventRecord(ev[wide0], c->side));
-    if (wide.n > 0) {
-      SwBandArgs ba = band_args(bc, wide, qs, s, scr);
-      ba.score = scores;
-      ba.best_row = best_row;
-      launch_band_routes(ba, wide, false, c->side);
-      st.sw_launches += 1;
+      DRG_CUDA(cudaEventRecord(ev[wide1], c->side));
+      for (int cls = kSwClasses - 1; cls >= 1; --cls) launch_cls(cls);
+      launch_cls(0);
+      const int side_end = 2 * 1 + 1;  // class 1 is the side stream's last launch
+      DRG_CUDA(cudaStreamWaitEvent(c->stream, ev[side_end], 0));
+      for (int k = 0; k < kSwClasses; ++k) {
+        st.sw_class_tasks[k] += hi[k] - lo[k];
+        if (hmax[k] > st.sw_class_max_steps[k]) st.sw_class_max_steps[k] = hmax[k];
+      }
+      st.sw_wide_bands += wide.n;
+      drg_run_stats* stp = &st;
+      log->later([ev, fork, wide0, wide1, side_end, stp] {
+        float cls_ms[kSwClasses], side_span = 0, wide_ms = 0;
+        for (int k = 0; k < kSwClasses; ++k) DRG_CUDA(cudaEventElapsedTime(&cls_ms[k], ev[2 * k], ev[2 * k + 1]));
+        DRG_CUDA(cudaEventElapsedTime(&side_span, ev[fork], ev[side_end]));
+        DRG_CUDA(cudaEventElapsedTime(&wide_ms, ev[wide0], ev[wide1]));
+        stp->ms_sw_kernel += cls_ms[0] > side_span ? cls_ms[0] : side_span;  // wall of the concurrent launches
+        for (int k = 0; k < kSwClasses; ++k) stp->ms_sw_class[k] += cls_ms[k];
+        stp->ms_sw_wide += wide_ms;
+      });
     }
-    DRG_CUDA(cudaEventRecord(ev[wide1], c->side));
-    for (int cls = kSwClasses - 1; cls >= 1; --cls) launch_cls(cls);
-    launch_cls(0);
-    const int side_end = 2 * 1 + 1;  // class 1 is the side stream's last launch
-    DRG_CUDA(cudaStreamWaitEvent(c->stream, ev[side_end], 0));
-    for (int k = 0; k < kSwClasses; ++k) {
-      st.sw_class_tasks[k] += hi[k] - lo[k];
-      if (hmax[k] > st.sw_class_max_steps[k]) st.sw_class_max_steps[k] = hmax[k];
-    }
-    st.sw_wide_bands += wide.n;
-    drg_run_stats* stp = &st;
-    log->later([ev, fork, wide0, wide1, side_end, stp] {
-      float cls_ms[kSwClasses], side_span = 0, wide_ms = 0;
-      for (int k = 0; k < kSwClasses; ++k) DRG_CUDA(cudaEventElapsedTime(&cls_ms[k], ev[2 * k], ev[2 * k + 1]));
-      DRG_CUDA(cudaEventElapsedTime(&side_span, ev[fork], ev[side_end]));
-      DRG_CUDA(cudaEventElapsedTime(&wide_ms, ev[wide0], ev[wide1]));
-      stp->ms_sw_kernel += cls_ms[0] > side_span ? cls_ms[0] : side_span;  // wall of the concurrent launches
-      for (int k = 0; k < kSwClasses; ++k) stp->ms_sw_class[k] += cls_ms[k];
-      stp->ms_sw_wide += wide_ms;
-    });
   }
   // the exact kernel for the bands the packed kernel did not settle
   count_launch();
