@@ -182,7 +182,8 @@ __device__ XdropDir xdrop_warp(XdropDir d, int xd, const int8_t* mat) {
       const int y = __shfl_up_sync(0xFFFFFFFFu, mx, o);
       if (lane >= (uint32_t)o) mx = max(mx, y);
     }
-    const int best_before = max(d.score, lane == 0 ? INT_MIN : __shfl_up_sync(0xFFFFFFFFu, mx, 1));
+    const int mx_prev = __shfl_up_sync(0xFFFFFFFFu, mx, 1);  // every lane takes part in the shuffle
+    const int best_before = max(d.score, lane == 0 ? INT_MIN : mx_prev);
     const int st_before = st_after - sc;
     const uint32_t stop = __ballot_sync(0xFFFFFFFFu, !valid || !(best_before - st_before < xd));
     const uint32_t taken = stop ? (uint32_t)(__ffs(stop) - 1) : 32u;
