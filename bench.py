@@ -260,6 +260,21 @@ def serve_stream(w, device, n_requests, repeats):
     return out
 
 
+def seed_stage_of(st, db_letters, query_letters):
+    """Seed enumeration + sorts + join of one search against the HBM roofline:
+    algorithmic bytes = the letters read once per shape, each seed entry of
+    both sides written and read once (16 B), each hit written once (16 B)."""
+    S = int(st["seed_shapes"])
+    b = S * (db_letters + query_letters) + 16 * (int(st["ref_seeds"]) + int(st["query_seeds"])) + 16 * int(st["hits"])
+    ms = st["ms_seed"] + st["ms_join"] + st["ms_sort"]
+    peak = measured_peaks().get("hbm_gbs")
+    gbs = b / (ms / 1000.0) / 1e9 if ms > 0 else None
+    return {"bound": "hbm", "ms": ms, "algorithmic_bytes": b, "achieved_gbs": gbs, "peak_gbs": peak,
+            "frac": gbs / peak if gbs and peak else None,
+            "peak_source": "hbm_gbs of fallback" if measured_peaks().get("fallback")
+            else "MEASURED_PEAKS.json hbm_gbs (of measured)"}
+
+
 def batching_leg(ctx, n_queries, n_db, sample, batched_only=False):
     """Config-3 generator (lognormal mean 350, 20-2000 aa, 10 % of the queries
     with 1-20 planted homologs), n_queries queries against an n_db-sequence
@@ -298,6 +313,7 @@ def batching_leg(ctx, n_queries, n_db, sample, batched_only=False):
                                                                         "ms_ungapped", "ms_bands", "ms_sw",
                                                                         "ms_select", "ms_trace", "ms_host")},
                             "query_blocks": int(bst["query_blocks"]), "hit_passes": int(bst["hit_passes"])},
+                "seed_stage": seed_stage_of(bst, int(do[-1]), int(to[-1])),
                 "hsps": nb_hsps, "hits": int(bst["hits"]), "bands": int(bst["bands"]),
                 "dp_cells_ref": int(bst["dp_cells_ref"]), "generate_s": gen_s}
     # autotune on the batch (untimed), then the tuning stays in the context
@@ -328,6 +344,7 @@ def batching_leg(ctx, n_queries, n_db, sample, batched_only=False):
                        "query_blocks": int(bst["query_blocks"]), "hit_passes": int(bst["hit_passes"])},
            "autotune": {"start": before, "chosen": tuned, "search_ms_start": ms_default,
                         "search_ms_chosen": ms_tuned},
+           "seed_stage": seed_stage_of(bst, int(do[-1]), int(to[-1])),
            "batched_over_plain": tp / tb, "identical_hsps": same and nb_hsps == np_hsps,
            "hsps": nb_hsps, "hits": int(bst["hits"]), "bands": int(bst["bands"]),
            "dp_cells_ref": int(bst["dp_cells_ref"]), "generate_s": gen_s}
