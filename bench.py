@@ -500,6 +500,10 @@ def main():
     batch = drgpu.ResidentBatch(ctx, tl, to)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
+    # the library's autotuner picks the context's tile and routing choices on
+    # this batch (untimed; results are the same under every choice)
+    tuned, tune_ms_default, tune_ms_best = ctx.autotune(db, batch, cfg, reps=2)
+
     # ---- resident (value) -------------------------------------------------
     for _ in range(args.warmup):
         drgpu.search_resident(ctx, db, batch, cfg, want_lists=False)
@@ -683,6 +687,8 @@ def main():
             "seed_stage": seed_stage,
             "blastx": blastx,
             "batching": batching,
+            "tuning": {"chosen": tuned, "search_ms_default": tune_ms_default, "search_ms_chosen": tune_ms_best,
+                       "what": "drg_autotune on the timed batch before the warm-up (untimed)"},
             "gpu_launches": int(launches),
             "cpu_baseline": cpu,
             "parity_sample": parity,

@@ -135,7 +135,11 @@ struct XdropDir {
   bool left;
 };
 
-constexpr uint32_t kXdropSerialSteps = 32;  // an extension longer than this is run by the whole warp
+// An extension still running after this many cells in one direction is
+// finished by the whole warp.  Random hits mostly stop within 20-60 cells:
+// with a limit of 32 many of them took the warp path (X-drop stage 0.57 ->
+// 0.73 ms at 1,000 queries); true homologies run for hundreds.
+constexpr uint32_t kXdropSerialSteps = 128;
 
 // Serial steps, at most `limit`; true when the direction has stopped (the
 // reference's loop condition failed or a sequence ended).
@@ -203,7 +207,7 @@ __device__ XdropDir xdrop_warp(XdropDir d, int xd, const int8_t* mat) {
 }
 
 // One thread per (target, subject, diagonal) run, as xdrop_run, except that
-// an extension still going after kXdropSerialSteps steps in one direction is
+// an extension still going after kXdropSerialSteps cells in one direction is
 // finished by the whole warp (xdrop_warp), so that a long true-homology
 // extension does not hold 31 idle lanes.  The hits of a run, the skip rule
 // (search.rs:184-191) and the cutoff stay in order per lane.

@@ -280,8 +280,8 @@ def test_autotune_picks_and_caches(tmp_path):
 
 def test_long_extensions_run_by_the_warp(ctx, orc):
     """Subjects holding exact or lightly mutated copies of 600-1500-aa queries:
-    their X-drop extensions run hundreds of cells, past the per-lane step
-    limit, so the warp finishes them (k_xdrop_runs); results must equal the
+    their X-drop extensions run hundreds of cells, past the per-lane limit of
+    128, so the warp finishes them (k_xdrop_runs); results must equal the
     oracle's."""
     r = np.random.Generator(np.random.PCG64(8181))
     queries = [synth.random_protein(r, int(n)) for n in r.integers(600, 1500, 12)]
