@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "kernels.h"
 #include "host/pool.h"
 #include "index_cache.h"
 #include "drgpu.h"
@@ -39,7 +40,8 @@ struct drg_ctx {
   drg::DevBuf x_nt, x_nt_off, x_len, x_scratch_off, x_scratch, x_keep, x_kept_len, x_kept_index, x_kept_off,
       x_query, x_frame;
   drg::DevBuf pass_counts, sw_counts;             // device-side counts of one pass of the stages after the join
-  drg::DevBuf sort_tmp, sort_err;  // radix sort scratch; its wait-timeout word (checked after the work)
+  drg::SortScratch sort_tmp;
+  drg::DevBuf sort_err;  // radix sort scratch; its wait-timeout word (checked after the work)
   drg_tuning tuning{273, 17, 1, 0};  // tile and routing choices (include/drgpu.h)
   drg::HostBuf h_stage;
   cudaEvent_t ev[16] = {};

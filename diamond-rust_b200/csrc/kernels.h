@@ -330,6 +330,12 @@ int sw_width_class(int width);  // 0..3, or -1 for the exact kernel
 void launch_sw_class(const SwScoreArgs& a, int cls, cudaStream_t st);  // score mode
 
 // ---- device radix sort (radix_sort.cu) --------------------------------------
+// The sort's scratch and the epoch of its last pass (look-back words carry
+// the epoch of the pass that wrote them).
+struct SortScratch {
+  DevBuf buf;
+  uint32_t epoch = 0;
+};
 // Where the sorted keys (and values) ended up: the LSD passes alternate between
 // the two buffers of each array.
 template <typename K>
@@ -347,7 +353,7 @@ struct SortResult {
 // No host wait.
 template <typename K>
 SortResult<K> radix_sort(K* keys, K* keys_alt, uint32_t* vals, uint32_t* vals_alt, uint64_t n_max,
-                         const uint64_t* d_n, int begin_bit, int end_bit, DevBuf& temp, uint32_t* d_err,
+                         const uint64_t* d_n, int begin_bit, int end_bit, SortScratch& temp, uint32_t* d_err,
                          cudaStream_t st, bool small_tiles = false);
 
 // ---- exact DP with traceback (sw_exact.cu) ----------------------------------

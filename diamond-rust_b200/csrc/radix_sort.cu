@@ -11,7 +11,9 @@
 //                   threads x ITEMS keys is loaded with 128-bit loads through
 //                   shared memory, ranked stably (per-warp __match_any_sync,
 //                   then a scan over warps), its global position per digit
-//                   found by decoupled look-back over the preceding tiles, and
+//                   found by decoupled look-back over the preceding tiles
+//                   (words tagged with the pass's epoch, so the look-back
+//                   area is never cleared between passes), and
 //                   scattered through shared memory so that the stores of one
 //                   digit run are contiguous.
 //
@@ -34,7 +36,13 @@ namespace {
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kBins = 256;
-constexpr uint32_t kFlagAggregate = 1u << 30, kFlagInclusive = 2u << 30, kValueMask = (1u << 30) - 1;
+// Look-back word: epoch (16 bits, the pass's tag) | status (2 bits:
+// 1 aggregate, 2 inclusive) | count (46 bits).  A word of another epoch reads
+// as "not ready", so the look-back area needs no clearing between passes.
+constexpr uint64_t kAggregate = 1ull << 46, kInclusive = 2ull << 46, kCountMask = (1ull << 46) - 1;
+__device__ __forceinline__ uint64_t lb_word(uint32_t epoch, uint64_t status, uint64_t count) {
+  return ((uint64_t)epoch << 48) | status | (count & kCountMask);
+}
 constexpr int kSpinLimit = 1 << 22;
 
 // Keys per thread of a tile: large tiles (16 u32 / 12 u64 keys per thread,
@@ -150,7 +158,7 @@ __device__ __forceinline__ void onesweep_tile(OnesweepShared<K, VALS, SMALL>& s,
                                               const K* __restrict__ kin, K* __restrict__ kout,
                                               const uint32_t* __restrict__ vin, uint32_t* __restrict__ vout,
                                               int shift, int dbits, const uint32_t* __restrict__ digit_start,
-                                              uint32_t* lookback, uint32_t* err) {
+                                              uint64_t* lookback, uint32_t epoch, uint32_t* err) {
   using Sh = OnesweepShared<K, VALS, SMALL>;
   constexpr int kItems = Sh::kItems, kTile = Sh::kTile;
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
@@ -210,27 +218,27 @@ __device__ __forceinline__ void onesweep_tile(OnesweepShared<K, VALS, SMALL>& s,
   // ---- decoupled look-back: this tile's count of digit t, and the counts of
   // the tiles before it
   const uint32_t mine = count - (t == kBins - 1 ? (uint32_t)(kTile - valid) : 0u);
-  volatile uint32_t* lb = lookback;
+  volatile uint64_t* lb = lookback;
   uint32_t excl = 0;
   if (tile == 0) {
-    lb[t] = kFlagInclusive | mine;
+    lb[t] = lb_word(epoch, kInclusive, mine);
   } else {
-    lb[(uint64_t)tile * kBins + t] = kFlagAggregate | mine;
+    lb[(uint64_t)tile * kBins + t] = lb_word(epoch, kAggregate, mine);
     for (int64_t p = (int64_t)tile - 1; p >= 0; --p) {
-      uint32_t v;
+      uint64_t v;
       int it = 0;
-      while (((v = lb[(uint64_t)p * kBins + t]) & ~kValueMask) == 0) {
+      while (((v = lb[(uint64_t)p * kBins + t]) >> 48) != epoch || (v & ~kCountMask & ((1ull << 48) - 1)) == 0) {
         if (++it > kSpinLimit) {
           atomicOr(err, 1u);
-          v = kFlagInclusive;
+          v = lb_word(epoch, kInclusive, 0);
           break;
         }
         if (it > 64) __nanosleep(64);
       }
-      excl += v & kValueMask;
-      if ((v & ~kValueMask) == kFlagInclusive) break;
+      excl += (uint32_t)(v & kCountMask);
+      if ((v & kInclusive) != 0) break;
     }
-    lb[(uint64_t)tile * kBins + t] = kFlagInclusive | ((excl + mine) & kValueMask);
+    lb[(uint64_t)tile * kBins + t] = lb_word(epoch, kInclusive, excl + mine);
   }
   s.global_base[t] = digit_start[t] + excl - local_start;
   __syncthreads();
@@ -271,8 +279,8 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const K* __restric
                                                               uint32_t* __restrict__ vout, const uint64_t* d_n,
                                                               uint64_t n_host, int shift, int dbits,
                                                               const uint32_t* __restrict__ digit_start,
-                                                              uint32_t* lookback, uint32_t* tile_counter,
-                                                              uint32_t* err) {
+                                                              uint64_t* lookback, uint32_t epoch,
+                                                              uint32_t* tile_counter, uint32_t* err) {
   using Sh = OnesweepShared<K, VALS, SMALL>;
   __shared__ Sh s;
   const uint64_t n = sort_count(d_n, n_host);
@@ -282,7 +290,8 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const K* __restric
     __syncthreads();
     const uint32_t tile = s.tile;
     if ((uint64_t)tile * Sh::kTile >= n) return;  // every thread sees the same tile
-    onesweep_tile<K, VALS, SMALL>(s, tile, n, kin, kout, vin, vout, shift, dbits, digit_start, lookback, err);
+    onesweep_tile<K, VALS, SMALL>(s, tile, n, kin, kout, vin, vout, shift, dbits, digit_start, lookback, epoch,
+                                  err);
     __syncthreads();  // the next tile reuses the shared state
   }
 }
@@ -322,7 +331,7 @@ SortPlan plan(uint64_t n_max, int begin_bit, int end_bit, bool small) {
   p.start_off = p.hist_off + (size_t)p.passes * kBins * 4;
   p.ctr_off = p.start_off + (size_t)p.passes * kBins * 4;
   p.lb_off = (p.ctr_off + 8 * 4 + 255) & ~size_t(255);
-  p.bytes = p.lb_off + (size_t)p.passes * p.tiles * kBins * 4;
+  p.bytes = p.lb_off + (size_t)p.tiles * kBins * 8;  // one look-back area, reused by every pass (epochs)
   return p;
 }
 
@@ -330,19 +339,25 @@ SortPlan plan(uint64_t n_max, int begin_bit, int end_bit, bool small) {
 
 template <typename K>
 SortResult<K> radix_sort(K* keys, K* keys_alt, uint32_t* vals, uint32_t* vals_alt, uint64_t n_max,
-                         const uint64_t* d_n, int begin_bit, int end_bit, DevBuf& temp, uint32_t* d_err,
+                         const uint64_t* d_n, int begin_bit, int end_bit, SortScratch& temp, uint32_t* d_err,
                          cudaStream_t st, bool small_tiles) {
   SortResult<K> r{keys, vals};
   if (n_max >= (1ull << 30)) throw Error(DRG_ERR_INVALID, "radix sort: at most 2^30 - 1 keys per sort");
   if (end_bit > (int)(8 * sizeof(K))) end_bit = 8 * sizeof(K);
   const SortPlan p = plan<K>(n_max, begin_bit, end_bit, small_tiles);
   if (p.passes == 0 || (n_max == 0 && !d_n)) return r;
-  uint8_t* tb = static_cast<uint8_t*>(temp.ensure(p.bytes));
+  void* before = temp.buf.p;
+  uint8_t* tb = static_cast<uint8_t*>(temp.buf.ensure(p.bytes));
   uint32_t* hist = reinterpret_cast<uint32_t*>(tb + p.hist_off);
   uint32_t* start = reinterpret_cast<uint32_t*>(tb + p.start_off);
   uint32_t* ctr = reinterpret_cast<uint32_t*>(tb + p.ctr_off);
-  uint32_t* lb = reinterpret_cast<uint32_t*>(tb + p.lb_off);
-  DRG_CUDA(cudaMemsetAsync(tb, 0, p.bytes, st));
+  uint64_t* lb = reinterpret_cast<uint64_t*>(tb + p.lb_off);
+  // new memory, or epochs about to wrap: clear the look-back area once
+  if (tb != before || temp.epoch + (uint32_t)p.passes >= 0xFFFFu) {
+    DRG_CUDA(cudaMemsetAsync(tb, 0, temp.buf.cap, st));
+    temp.epoch = 0;
+  }
+  DRG_CUDA(cudaMemsetAsync(tb, 0, p.lb_off, st));  // histograms, digit starts, tile counters
   const int hist_blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>((n_max + 4095) / 4096, 148 * 4));
   count_launch();
   k_radix_hist<K><<<hist_blocks, kSortThreads, 0, st>>>(keys, d_n, n_max, begin_bit, end_bit, p.passes, p.dbits,
@@ -357,10 +372,10 @@ SortResult<K> radix_sort(K* keys, K* keys_alt, uint32_t* vals, uint32_t* vals_al
     const int shift = begin_bit + pass * p.dbits;
     const int db = std::min(p.dbits, end_bit - shift);
     count_launch();
-    uint32_t* lbp = lb + (size_t)pass * p.tiles * kBins;
+    const uint32_t epoch = ++temp.epoch;  // 1..65534
     auto launch = [&](auto kernel, int resident) {
       const unsigned grid = (unsigned)std::min<uint64_t>(p.tiles, (uint64_t)resident);
-      kernel<<<grid, kSortThreads, 0, st>>>(ki, ko, vi, vo, d_n, n_max, shift, db, start + pass * kBins, lbp,
+      kernel<<<grid, kSortThreads, 0, st>>>(ki, ko, vi, vo, d_n, n_max, shift, db, start + pass * kBins, lb, epoch,
                                             ctr + pass, d_err);
     };
     if (vals && small_tiles)
@@ -381,8 +396,10 @@ SortResult<K> radix_sort(K* keys, K* keys_alt, uint32_t* vals, uint32_t* vals_al
 }
 
 template SortResult<uint32_t> radix_sort<uint32_t>(uint32_t*, uint32_t*, uint32_t*, uint32_t*, uint64_t,
-                                                   const uint64_t*, int, int, DevBuf&, uint32_t*, cudaStream_t, bool);
+                                                   const uint64_t*, int, int, SortScratch&, uint32_t*, cudaStream_t,
+                                                   bool);
 template SortResult<uint64_t> radix_sort<uint64_t>(uint64_t*, uint64_t*, uint32_t*, uint32_t*, uint64_t,
-                                                   const uint64_t*, int, int, DevBuf&, uint32_t*, cudaStream_t, bool);
+                                                   const uint64_t*, int, int, SortScratch&, uint32_t*, cudaStream_t,
+                                                   bool);
 
 }  // namespace drg
