@@ -497,11 +497,12 @@ __global__ void k_state_flags(const uint8_t* state, uint64_t n, uint8_t* f) {
   if (i < n) f[i] = state[i] >= 2;
 }
 
-__global__ void k_gather_bands(const uint32_t* idx, uint64_t n, const Band* bands, const int32_t* score,
-                               const int32_t* best_row, const uint8_t* state, Band* out_b, int32_t* out_s,
-                               uint8_t* out_st) {
+// (n bounds the device-side count *d_n)
+__global__ void k_gather_bands_dev(const uint32_t* idx, uint64_t n, const int64_t* d_n, const Band* bands,
+                                   const int32_t* score, const int32_t* best_row, const uint8_t* state, Band* out_b,
+                                   int32_t* out_s, uint8_t* out_st) {
   uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (k >= n) return;
+  if (k >= n || k >= (uint64_t)*d_n) return;
   uint32_t i = idx[k];
   Band b = bands[i];
   b.pad = best_row ? (uint32_t)best_row[i] : 0u;  // first row of the best: the traceback needs no row below
@@ -1440,21 +1441,28 @@ void Search::process_hits(uint64_t pass_id) {
   launch_select(ga, c->stream);
   count_launch();
   k_state_flags<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(state, n_bands, flags);
+  // the kept and undecided bands, gathered on their device-side count: one
+  // wait for the count, one for the records (pinned staging)
   uint32_t* sel = c->sel_idx.as<uint32_t>(n_bands + 1);
-  const uint64_t n_sel = select_indices(c, flags, n_bands, sel, d_count);
+  int64_t* dsel = c->pass_counts.as<int64_t>(8) + 6;
+  select_indices_dev(c, flags, n_bands, sel, dsel);
+  Band* gb = c->sel_bands.as<Band>(n_bands);
+  int32_t* gs = reinterpret_cast<int32_t*>(c->exact_out.as<uint8_t>(n_bands * 5 + 16));
+  uint8_t* gst = reinterpret_cast<uint8_t*>(gs + n_bands);
+  count_launch();
+  k_gather_bands_dev<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(sel, n_bands, dsel, bc, scores, best_row, state,
+                                                                      gb, gs, gst);
+  const uint64_t n_sel = (uint64_t)fetch(c, dsel);
   if (n_sel > 0) {
-    Band* gb = c->sel_bands.as<Band>(n_sel);
-    int32_t* gs = reinterpret_cast<int32_t*>(c->exact_out.as<uint8_t>(n_sel * 5 + 16));
-    uint8_t* gst = reinterpret_cast<uint8_t*>(gs + n_sel);
-    count_launch();
-    k_gather_bands<<<ceil_div(n_sel, 256), 256, 0, c->stream>>>(sel, n_sel, bc, scores, best_row, state, gb, gs,
-                                                                  gst);
-    std::vector<Band> hb;
-    std::vector<int32_t> hs_;
-    std::vector<uint8_t> hst;
-    fetch_n(c, hb, gb, n_sel);
-    fetch_n(c, hs_, gs, n_sel);
-    fetch_n(c, hst, gst, n_sel);
+    const size_t rec = sizeof(Band) + sizeof(int32_t) + 1;
+    uint8_t* h = c->h_stage.as<uint8_t>(n_sel * rec + 16);
+    Band* hb = reinterpret_cast<Band*>(h);
+    int32_t* hs_ = reinterpret_cast<int32_t*>(h + n_sel * sizeof(Band));
+    uint8_t* hst = reinterpret_cast<uint8_t*>(hs_ + n_sel);
+    DRG_CUDA(cudaMemcpyAsync(hb, gb, n_sel * sizeof(Band), cudaMemcpyDeviceToHost, c->stream));
+    DRG_CUDA(cudaMemcpyAsync(hs_, gs, n_sel * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    DRG_CUDA(cudaMemcpyAsync(hst, gst, n_sel, cudaMemcpyDeviceToHost, c->stream));
+    DRG_CUDA(cudaStreamSynchronize(c->stream));
     for (uint64_t k = 0; k < n_sel; ++k) {
       Candidate cd;
       cd.band = hb[k];
