@@ -1597,11 +1597,19 @@ void Search::finish(drg_result* out) {
     cub_call(c, [&](void* t, size_t& b) {
       return cub::DeviceScan::ExclusiveSum(t, b, cnt, coff, (int64_t)nj + 1, c->stream);
     });
-    const uint64_t n_used = fetch(c, coff + nj);
-    uint32_t* cops = c->ops_compact.as<uint32_t>(n_used + 1);
+    // compacted into a buffer of the bands' slot total (an upper bound of the
+    // ops used); the records and the used count come back in one wait
+    uint32_t* cops = c->ops_compact.as<uint32_t>(ops_off[nj] + 1);
     count_launch();
     k_compact_ops<<<ceil_div(nj, 128), 128, 0, c->stream>>>(dops, doff, dout, coff, nj, cops);
-    fetch_n(c, eo, dout, nj);
+    uint8_t* hst = c->h_stage.as<uint8_t>(nj * sizeof(ExactOut) + 16);
+    DRG_CUDA(cudaMemcpyAsync(hst, dout, nj * sizeof(ExactOut), cudaMemcpyDeviceToHost, c->stream));
+    DRG_CUDA(cudaMemcpyAsync(hst + nj * sizeof(ExactOut), coff + nj, sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                             c->stream));
+    DRG_CUDA(cudaStreamSynchronize(c->stream));
+    eo.assign(reinterpret_cast<const ExactOut*>(hst), reinterpret_cast<const ExactOut*>(hst) + nj);
+    uint64_t n_used = 0;
+    std::memcpy(&n_used, hst + nj * sizeof(ExactOut), sizeof(uint64_t));
     fetch_n(c, ops_all, cops, n_used);
     tm.stop(&st.ms_trace);
   }
