@@ -71,6 +71,22 @@ __device__ __forceinline__ void sw_step(SRegs& R, Lane& L, int c, const uint8_t*
   uint32_t hd = R.htop_old;
 #pragma unroll
   for (int p = 0; p < kPairs; ++p) {
+    // Pairs whose two halves are both outside the band at this compile-time
+    // step are not computed: left of it in the prologue (C < p), right of it
+    // in a one-width epilogue (C >= p + 9).  They take the values the masks
+    // below would give (H = 0, H - oc = -oc, F = -inf) and hand the next
+    // pair the same E/H the masked computation would; in the prologue every
+    // pair below is skipped too, and the E of pair 7 is first read by row 8
+    // at step 9, when pair 7 is computed again.
+    if ((MODE == 1 && C < p) || (MODE == 2 && C >= p + 9)) {
+      hd = R.H[p];
+      R.H[p] = 0;
+      R.Hm[p] = noc2;
+      R.F[p] = kNeg2;
+      hm_up = noc2;
+      e_up = kNeg2;
+      continue;
+    }
     const uint32_t sc = prmt(p < 4 ? lo8.x : lo8.y, p < 4 ? hi8.x : hi8.y, pick_sel(p & 3));
     const uint32_t d = add2(hd, sc);
     uint32_t e = __viaddmax_s16x2(e_up, nge2, hm_up);
