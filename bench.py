@@ -606,8 +606,9 @@ def main():
         d2h = n_h * ctypes.sizeof(drgpu.Hsp) + n_ops * 4 + len(to) * 8
     e2e_s = max_over_ranks(e2e_s, world)
     h2d = int(dl.nbytes + do.nbytes + tl.nbytes + to.nbytes + len(w.queries) * 5)
-    e2e = {"value": world * len(w.queries) * args.steps / e2e_s, "unit": "queries/s",
-           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(d2h)}
+    e2e = None if args.no_e2e else {
+        "value": world * len(w.queries) * args.steps / e2e_s, "unit": "queries/s",
+        "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(d2h)}
 
     # ---- serving: the same request stream, plain and continuously batched ---
     serving = None
