@@ -311,6 +311,8 @@ int onesweep_resident_blocks() {
   return r;
 }
 
+constexpr int kMaxPasses = 8;  // 64-bit keys in 8-bit digits
+
 struct SortPlan {
   int passes = 0, dbits = 8;
   uint64_t tiles = 0;
@@ -327,10 +329,13 @@ SortPlan plan(uint64_t n_max, int begin_bit, int end_bit, bool small) {
   const uint64_t tile =
       (uint64_t)kSortThreads * (small ? SortItems<K, true>::value : SortItems<K, false>::value);
   p.tiles = n_max == 0 ? 1 : (n_max + tile - 1) / tile;
+  // Histograms, digit starts and tile counters are laid out for the most
+  // passes any sort takes, so that the look-back area starts at the same
+  // offset in every sort and holds nothing but look-back words (or zeros).
   p.hist_off = 0;
-  p.start_off = p.hist_off + (size_t)p.passes * kBins * 4;
-  p.ctr_off = p.start_off + (size_t)p.passes * kBins * 4;
-  p.lb_off = (p.ctr_off + 8 * 4 + 255) & ~size_t(255);
+  p.start_off = p.hist_off + (size_t)kMaxPasses * kBins * 4;
+  p.ctr_off = p.start_off + (size_t)kMaxPasses * kBins * 4;
+  p.lb_off = (p.ctr_off + kMaxPasses * 4 + 255) & ~size_t(255);
   p.bytes = p.lb_off + (size_t)p.tiles * kBins * 8;  // one look-back area, reused by every pass (epochs)
   return p;
 }
@@ -346,14 +351,16 @@ SortResult<K> radix_sort(K* keys, K* keys_alt, uint32_t* vals, uint32_t* vals_al
   if (end_bit > (int)(8 * sizeof(K))) end_bit = 8 * sizeof(K);
   const SortPlan p = plan<K>(n_max, begin_bit, end_bit, small_tiles);
   if (p.passes == 0 || (n_max == 0 && !d_n)) return r;
-  void* before = temp.buf.p;
+  // (a reallocation shows in the capacity: the new block may start at the
+  // old address, holding another buffer's stale words)
+  const size_t cap_before = temp.buf.cap;
   uint8_t* tb = static_cast<uint8_t*>(temp.buf.ensure(p.bytes));
   uint32_t* hist = reinterpret_cast<uint32_t*>(tb + p.hist_off);
   uint32_t* start = reinterpret_cast<uint32_t*>(tb + p.start_off);
   uint32_t* ctr = reinterpret_cast<uint32_t*>(tb + p.ctr_off);
   uint64_t* lb = reinterpret_cast<uint64_t*>(tb + p.lb_off);
   // new memory, or epochs about to wrap: clear the look-back area once
-  if (tb != before || temp.epoch + (uint32_t)p.passes >= 0xFFFFu) {
+  if (temp.buf.cap != cap_before || temp.epoch + (uint32_t)p.passes >= 0xFFFFu) {
     DRG_CUDA(cudaMemsetAsync(tb, 0, temp.buf.cap, st));
     temp.epoch = 0;
   }

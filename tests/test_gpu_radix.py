@@ -64,3 +64,24 @@ def test_sort_keys_only_skewed(ctx, on_device):
     keys = (r.integers(0, 4, n, dtype=np.uint64) << np.uint64(20)) | r.integers(0, 3, n, dtype=np.uint64)
     gk, _ = ctx.radix_sort(keys, None, 0, 40, count_on_device=on_device)
     assert np.array_equal(gk, np.sort(keys, kind="stable"))
+
+
+def test_sort_sequence_shares_scratch(ctx):
+    # Sorts of different pass counts and growing sizes one after another on
+    # one context: they share the look-back area (its words carry the pass's
+    # epoch), which must never hold another sort's histograms or stale words
+    # of a reallocated block.
+    r = np.random.Generator(np.random.PCG64(99))
+    plan = [(np.uint64, 0, 64, 300000), (np.uint32, 0, 8, 5000), (np.uint64, 0, 16, 2000000),
+            (np.uint32, 0, 32, 70000), (np.uint64, 20, 30, 4000000), (np.uint32, 3, 11, 9000),
+            (np.uint64, 0, 64, 1 << 20), (np.uint32, 0, 24, 6000000), (np.uint64, 0, 8, 100)]
+    for rep in range(3):
+        for dtype, begin, end, n in plan:
+            hi = 1 << 63 if dtype == np.uint64 else 1 << 32
+            keys = r.integers(0, hi, n, dtype=np.uint64).astype(dtype)
+            keys[::5] = keys[1]
+            vals = np.arange(n, dtype=np.uint32)
+            gk, gv = ctx.radix_sort(keys, vals, begin, end, count_on_device=bool(rep & 1))
+            _, ev = expect(keys, begin, end)
+            assert np.array_equal(gv, ev), (rep, dtype, begin, end, n)
+            assert np.array_equal(gk, keys[ev])
