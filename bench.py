@@ -215,28 +215,36 @@ def serve_stream(w, device, n_requests, repeats):
     lognormal mean 350 clipped 20-3000, presets uniform over fast / default /
     sensitive / very-sensitive) against the resident database, served plain
     (one request at a time, the seed index rebuilt per search as the reference
-    does) and continuously batched (2 worker contexts, a 1M-letter batch
-    budget, each preset's seed index resident).  The stream is replayed
-    `repeats` times per form at its rate (forms alternating), then once with
-    every request queued at once (capacity)."""
+    does) and continuously batched (2 worker contexts taking turns on the
+    GPU, a 1M-letter batch budget, each preset's seed index resident).  Both
+    are warmed first; the stream is replayed `repeats` times per form at its
+    rate (forms alternating), then once with every request queued at once
+    (capacity)."""
     import numpy as np
     import drgpu
     from drgpu import serve
     dl, do = drgpu.concat(w.db)
     rng = np.random.Generator(np.random.PCG64(20261208))
-    base = serve.poisson_stream(rng, n_requests, 20.0, 2000, ["fast", "default", "sensitive", "very-sensitive"])
+    presets = ["fast", "default", "sensitive", "very-sensitive"]
+    base = serve.poisson_stream(rng, n_requests, 20.0, 2000, presets)
+
     out = {"stream": f"{n_requests} requests, Poisson 20/s, 1-2000 queries each (lognormal mean 350, 20-3000 aa), "
                      f"presets uniform over fast/default/sensitive/very-sensitive, resident {len(w.db)}-sequence DB; "
                      f"latency = arrival to results on the host; {repeats} replays per form at the stream's rate "
                      f"(median and range), then all requests queued at once (capacity); plain: one request at a "
-                     f"time, seed index rebuilt per search; batched: 2 worker contexts, continuous batching under "
-                     f"a 1M-letter batch budget, seed index resident per preset"}
+                     f"time, seed index rebuilt per search; batched: 2 worker contexts taking turns on the GPU "
+                     f"(host work of one beside the other's search), continuous batching under a 1M-letter "
+                     f"batch budget, seed index resident per preset; both forms warmed with one search per "
+                     f"preset of the stream's largest request before it starts"}
+
+    warm_queries = max((r for _, r in base), key=lambda r: len(r.queries)).queries
 
     def replay(batched, rate):
         stream = [(t * 20.0 / rate, serve.Request(r.rid, r.preset, r.queries)) for t, r in base]
         srv = serve.Server(dl, do, workers=2 if batched else 1, batch=batched, device=device,
                            index_budget=(16 << 30) if batched else 0)
         try:
+            srv.warm(presets, warm_queries)  # both forms: scratch at working size before the stream
             finished, span = serve.run_stream(srv, stream)
         finally:
             srv.close()

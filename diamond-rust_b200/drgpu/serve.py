@@ -7,7 +7,14 @@ the oldest one, up to a budget of query letters, as one batch
 (drg_batch_create_requests) and searches it.  The batch's join cap is counted
 per request, so each request's HSP lists equal those of the request searched
 alone; requests that arrive while a batch runs wait only for the next free
-worker (continuous batching), and the workers' batches overlap on the GPU.
+worker (continuous batching).
+
+The workers' searches take turns on the GPU (one search at a time, in the
+order the workers reached the GPU): a search fills the GPU by itself, and two
+searches side by side each take about twice as long, which lengthens the tail
+of the latency.  What a worker does on the host (assembling the next batch's
+letters, building Python records of the last one) overlaps the other worker's
+search.
 
 The letter budget bounds a batch's work, so that a batch takes about as long
 as one large request: small requests share a batch, large ones run alone.
@@ -56,23 +63,35 @@ class Request:
         return sub.lists(query_shift=t0)
 
 
-def search_batch(ctx: Context, db: ResidentDb, requests, preset: str, index_chunks=None):
-    """Search several requests of one preset as one batch; each request gets
-    its slice of the batch's results (copied to the host in bulk)."""
+def batch_arrays(requests):
+    """The letters, offsets and request ids of several requests' queries, in
+    request order (host work, no GPU)."""
     seqs, rid = [], []
     for k, r in enumerate(requests):
         seqs.extend(r.queries)
         rid.extend([k] * len(r.queries))
     letters, offsets = concat(seqs)
-    batch = ResidentBatch(ctx, letters, offsets, request=np.asarray(rid, np.uint32))
+    return letters, offsets, np.asarray(rid, np.uint32)
+
+
+def search_batch(ctx: Context, db: ResidentDb, requests, preset: str, index_chunks=None, arrays=None,
+                 gpu_turn=None):
+    """Search several requests of one preset as one batch; each request gets
+    its slice of the batch's results (copied to the host in bulk).  `arrays`
+    (from batch_arrays) may be built ahead; `gpu_turn`, a lock, is held while
+    the batch is on the GPU (upload, search, results, release)."""
+    letters, offsets, rid = arrays if arrays is not None else batch_arrays(requests)
     cfg = make_config(sensitivity=preset, index_chunks=index_chunks)
     res = Result()
-    try:
-        ctx._check(ctx.lib.drg_search_batch(ctx.h, db.h, batch.h, C.byref(cfg), C.byref(res)))
-        arrays = ResultArrays(res)
-    finally:
-        ctx.lib.drg_result_free(C.byref(res))
-        batch.close()
+    turn = gpu_turn if gpu_turn is not None else _NoLock()
+    with turn:
+        batch = ResidentBatch(ctx, letters, offsets, request=rid)
+        try:
+            ctx._check(ctx.lib.drg_search_batch(ctx.h, db.h, batch.h, C.byref(cfg), C.byref(res)))
+            arrays = ResultArrays(res)
+        finally:
+            ctx.lib.drg_result_free(C.byref(res))
+            batch.close()
     t = 0
     for r in requests:
         n = len(r.queries)
@@ -80,6 +99,14 @@ def search_batch(ctx: Context, db: ResidentDb, requests, preset: str, index_chun
         r.batch_size = len(requests)
         t += n
     return requests
+
+
+class _NoLock:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        return False
 
 
 class Server:
@@ -95,6 +122,7 @@ class Server:
         self.index_chunks = index_chunks
         self.pending: list[Request] = []
         self.lock = threading.Condition()
+        self.gpu_turn = threading.Lock()  # one search on the GPU at a time
         self.closed = False
         self.finished: list[Request] = []
         self.t0 = time.perf_counter()
@@ -141,7 +169,8 @@ class Server:
                     return
                 reqs = self._take()
             try:
-                search_batch(ctx, self.db, reqs, reqs[0].preset, self.index_chunks)
+                arrays = batch_arrays(reqs)  # host work, beside the other worker's search
+                search_batch(ctx, self.db, reqs, reqs[0].preset, self.index_chunks, arrays, self.gpu_turn)
             except BaseException as e:  # surfaced by close()
                 self.errors.append(e)
             t = self.now()
@@ -150,6 +179,15 @@ class Server:
                     r.done = t
                 self.finished.extend(reqs)
                 self.lock.notify_all()
+
+    def warm(self, presets, queries):
+        """Searches `queries` once per preset before serving (untimed): the
+        contexts' scratch buffers grow to their working size and, with an
+        index budget, each preset's seed index is built."""
+        for ctx in self.ctxs:
+            for preset in presets:
+                search_batch(ctx, self.db, [Request(-1, preset, list(queries))], preset, self.index_chunks,
+                             gpu_turn=self.gpu_turn)
 
     def close(self):
         with self.lock:

@@ -102,8 +102,9 @@ def test_server_stream_continuous_batching():
     # admitted as one batch whatever the speed of the GPU
     stream = serve.poisson_stream(rng, 24, rate=1e6, max_queries=12,
                                   presets=["fast", "default", "sensitive", "very-sensitive"], q_hi=600)
-    srv = serve.Server(dl, do, workers=2, batch=True)
+    srv = serve.Server(dl, do, workers=2, batch=True, index_budget=1 << 30)
     try:
+        srv.warm(["fast", "very-sensitive"], w.queries[:3])  # grows scratch, builds two presets' indexes
         finished, span = serve.run_stream(srv, stream)
     finally:
         srv.close()
