@@ -324,6 +324,9 @@ constexpr int kSwMinWidth = 17;   // narrower bands use the exact kernel
 constexpr int kSwC0 = 136, kSwC1 = 272, kSwC2 = 544, kSwC3 = 1700;
 constexpr int kSwClassMax[4] = {kSwC0, kSwC1, kSwC2, kSwC3};  // 4, 2, 1, 1 warps per block
 constexpr int kSwMaxWidth = 1700;                       // wider bands use the exact kernel
+// The packed kernel's profile bytes hold a score plus the open cost (gap open
+// + extend): with larger open costs its bands go to the band kernel.
+constexpr int kSwMaxOpenCost = 64;
 constexpr int kSwBandMinWidth = kSwC1 + 1;  // score pass: wider bands run one warp per band
 constexpr int kSwClasses = 4;
 int sw_width_class(int width);  // 0..3, or -1 for the exact kernel

@@ -216,8 +216,10 @@ __global__ void k_count_fast_narrow(const uint64_t* keys, uint64_t n, uint64_t w
 struct SwTune {
   int wide_min, min_packed, transpose;
 };
-SwTune sw_tune(const drg_ctx* c) {
-  return SwTune{c->tuning.sw_wide_min_width, c->tuning.sw_min_packed_width, c->tuning.sw_transpose};
+SwTune sw_tune(const drg_ctx* c, const Scoring& scr) {
+  SwTune t{c->tuning.sw_wide_min_width, c->tuning.sw_min_packed_width, c->tuning.sw_transpose};
+  if (scr.gap_open + scr.gap_extend > kSwMaxOpenCost) t.wide_min = t.min_packed;  // no packed-kernel bands
+  return t;
 }
 
 // Which kernel a band goes to: the packed kernel (fast), its wide-band
@@ -621,7 +623,7 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
     DRG_CUDA(cudaMemsetAsync(tr_count, 0, n_subjects * sizeof(uint32_t), c->stream));
     count_launch();
     k_sw_tr_count<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(bc, n_bands, s.offsets, scr.max_score,
-                                                                  sw_tune(c), tr_count, rows);
+                                                                  sw_tune(c, scr), tr_count, rows);
   }
   count_launch();
   // group field: target << 16 | window start, or the subject (transposed)
@@ -634,7 +636,7 @@ void run_bands(drg_ctx* c, const Band* bc, uint64_t n_bands, const DevSeqs& qs, 
     kb.end = kGroupShift + gb + 2;
     if (kb.end > 64) throw Error(DRG_ERR_INVALID, "score-pass key needs more than 64 bits");
   }
-  k_sw_keys<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(bc, n_bands, s.offsets, scr.max_score, sw_tune(c), kb,
+  k_sw_keys<<<ceil_div(n_bands, 256), 256, 0, c->stream>>>(bc, n_bands, s.offsets, scr.max_score, sw_tune(c, scr), kb,
                                                            tr_count, swk, rows, swo);
   // rows first, then a stable sort by (target, window, width)
   uint32_t* by_rows = dsort(c, rows, rows_s, swo, swo_r, n_bands, 0, 32).vals;

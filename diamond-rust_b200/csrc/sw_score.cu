@@ -15,9 +15,19 @@
 //   H      = max(0, D, E, F)
 // Row 8's "pair above" is row 7, taken from the previous step; row 0's is the
 // previous strip's last row, kept in a per-thread ring in shared memory.  The
-// ring holds W + 1 words (H | E << 16): a strip reads the previous strip's
-// word for column c and then overwrites the slot of column c - 1, which is
-// the word the next strip needs at its column c - 17.
+// ring holds W + 1 words (H - oc | E << 16): a strip reads the previous
+// strip's word for column c and then overwrites the slot of column c - 1,
+// which is the word the next strip needs at its column c - 17.
+//
+// A pair update is five half-rate DPX/PRMT operations and one full-rate max:
+//   sc = the pair's two scores (one byte permute)
+//   F  = max(F - ge, H - oc)            (viaddmax)
+//   X  = max(D, F, 0)                   (viaddmax.relu: D = Hdiag + sc fused)
+//   E  = max(E - ge, H - oc)            (viaddmax, the step's vertical chain)
+//   H  = max(X, E)                      (max.s16x2, full rate)
+//   H - oc                              (add, shared by the next E and F)
+// Pair 0's diagonal operand comes from the ring and row 7 in the H - oc form
+// (that is what the ring keeps), so the profile rows 0 and 8 carry + oc.
 //
 // Exactness: values equal the reference's int32 DP while the band's best is
 // below 2^15 (bands that could exceed it are not given to this kernel).
@@ -45,7 +55,7 @@ using namespace sw;
 struct SRegs {
   uint32_t H[kPairs], Hm[kPairs], F[kPairs];
   uint32_t E7;        // E of pair 7 at the previous step
-  uint32_t htop_old;  // top H of the previous step (D operand of pair 0)
+  uint32_t hmtop_old; // H - oc above pair 0 at the previous step (its D operand, profile + oc)
   const uint8_t* prow_prev;  // profile row of the previous column's residue
   uint32_t mx0, mx1;  // maximum H of the strip so far, folded over rows
 };
@@ -53,8 +63,9 @@ struct SRegs {
 // One column step.  MODE 0: middle (all rows in band), 1: prologue step
 // C (= c), 2: epilogue step C (= c - W) of a warp whose bands share one
 // width, 3: step past the narrowest band of a warp with mixed widths
-// (cw = c - this lane's W, masks computed at run time).  rp holds the (H, E)
-// word of the row above at column c; wp receives row 15's word of column c - 1.
+// (cw = c - this lane's W, masks computed at run time).  rp holds the
+// (H - oc, E) word of the row above row 0 at column c; wp receives row 15's
+// word of column c - 1.
 template <int MODE, int C>
 __device__ __forceinline__ void sw_step(SRegs& R, Lane& L, int c, const uint8_t* __restrict__ prof,
                                         const uint32_t* __restrict__ rp, uint32_t* __restrict__ wp, uint32_t noc2,
@@ -64,11 +75,11 @@ __device__ __forceinline__ void sw_step(SRegs& R, Lane& L, int c, const uint8_t*
   const uint2 lo8 = *reinterpret_cast<const uint2*>(prow);
   const uint2 hi8 = *reinterpret_cast<const uint2*>(R.prow_prev + 8);
   R.prow_prev = prow;
-  const uint32_t rw = *rp;  // (H, E) of the row above row 0, column c
-  const uint32_t htop = prmt(rw, R.H[kPairs - 1], 0x5410);
+  const uint32_t rw = *rp;  // (H - oc, E) of the row above row 0, column c
+  const uint32_t hm_top = prmt(rw, R.Hm[kPairs - 1], 0x5410);
+  uint32_t hm_up = hm_top;
   uint32_t e_up = prmt(rw, R.E7, 0x5432);
-  uint32_t hm_up = add2(htop, noc2);
-  uint32_t hd = R.htop_old;
+  uint32_t hd = R.hmtop_old;
 #pragma unroll
   for (int p = 0; p < kPairs; ++p) {
     // Pairs whose two halves are both outside the band at this compile-time
@@ -88,10 +99,10 @@ __device__ __forceinline__ void sw_step(SRegs& R, Lane& L, int c, const uint8_t*
       continue;
     }
     const uint32_t sc = prmt(p < 4 ? lo8.x : lo8.y, p < 4 ? hi8.x : hi8.y, pick_sel(p & 3));
-    const uint32_t d = add2(hd, sc);
-    uint32_t e = __viaddmax_s16x2(e_up, nge2, hm_up);
     uint32_t f = __viaddmax_s16x2(R.F[p], nge2, R.Hm[p]);
-    uint32_t h = __vimax3_s16x2_relu(d, e, f);
+    const uint32_t x = __viaddmax_s16x2_relu(hd, sc, f);  // max(D, F, 0)
+    uint32_t e = __viaddmax_s16x2(e_up, nge2, hm_up);
+    uint32_t h = max2(x, e);
     if (MODE == 1) {
       // left of the band: row p at column C (low), row p+8 at column C-1 (high)
       const bool lo_left = C < p;
@@ -129,8 +140,8 @@ __device__ __forceinline__ void sw_step(SRegs& R, Lane& L, int c, const uint8_t*
   R.mx0 = __vimax3_s16x2(R.mx0, R.H[2], R.H[3]);
   R.mx1 = __vimax3_s16x2(R.mx1, R.H[6], R.H[7]);
   R.E7 = e_up;
-  *wp = prmt(R.H[kPairs - 1], R.E7, 0x7632);  // (H, E) of row 15 at column c - 1
-  R.htop_old = htop;
+  *wp = prmt(R.Hm[kPairs - 1], R.E7, 0x7632);  // (H - oc, E) of row 15 at column c - 1
+  R.hmtop_old = hm_top;
 }
 
 // The ring of one lane: W + 1 words at stride `stride`; rp reads column c,
@@ -199,11 +210,14 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS >= 2 ? 3 : 1) k_sw(SwScoreAr
   Lane L;
   L.s = tr ? qw : sj;  // column letters
   L.m = tr ? (int)band.n : m_s;
-  const uint32_t noc2 = (uint32_t)(uint16_t)(-(a.gap_open + a.gap_extend)) * 0x10001u;
+  const int oc = a.gap_open + a.gap_extend;  // at most kSwMaxOpenCost (profile bytes carry it)
+  const uint32_t noc2 = (uint32_t)(uint16_t)(-oc) * 0x10001u;
   const uint32_t nge2 = (uint32_t)(uint16_t)(-a.gap_extend) * 0x10001u;
+  // dead cell word: H = 0 (H - oc = -oc), E = -inf
+  const uint32_t dead = 0xC0000000u | (noc2 & 0xFFFFu);
   // the row above the first strip is row 0 of the reference: H = 0, and its
   // E is -inf; column Wl - 1 is outside row 0's band on the right.
-  for (int g = 0; g < buf; ++g) ring[g * stride] = 0xC0000000u;
+  for (int g = 0; g < buf; ++g) ring[g * stride] = dead;
   ring[(Wl - 1) * stride] = kNeg2;
   RingPtr rg;
   rg.begin = ring;
@@ -216,7 +230,8 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS >= 2 ? 3 : 1) k_sw(SwScoreAr
   for (uint32_t k = 0; k < task.n_strips; ++k) {
     const int i0 = (int)task.row_first + (int)(k * kRows);
     // strip profile: prof[res * stride + r] = S(query letter, subject letter)
-    // of row i0 + r against column residue res
+    // of row i0 + r against column residue res, + oc in rows 0 and 8 (their
+    // diagonal operand is H - oc)
     __syncwarp();
     for (int e = lane; e < 26 * kRows; e += 32) {
       int res = e >> 4, r = e & 15;
@@ -227,6 +242,7 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS >= 2 ? 3 : 1) k_sw(SwScoreAr
         const int row = (int)min((uint32_t)q[i - 1], 24u);
         v = tr ? mat[res * 25 + row] : mat[row * 25 + res];
       }
+      if ((r & 7) == 0) v += oc;
       prof[res * kProfStride + r] = (uint8_t)(int8_t)v;
     }
     __syncwarp();
@@ -256,7 +272,8 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS >= 2 ? 3 : 1) k_sw(SwScoreAr
       rg.rp = ring + slot * stride;
       rg.wp = ring + (slot == 0 ? buf - 1 : slot - 1) * stride;
     }
-    R.htop_old = *rg.wp & 0xFFFFu;  // column c_begin - 1 of the row above
+    // H - oc of column c_begin - 1 of the row above; row 7 not yet computed: H = 0
+    R.hmtop_old = (*rg.wp & 0xFFFFu) | (noc2 & 0xFFFF0000u);
     {
       const int jm1 = L.jbase + c_begin - 2;  // column c_begin - 1
       R.prow_prev = prof + subject_residue(L, jm1) * kProfStride;
@@ -302,7 +319,7 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS >= 2 ? 3 : 1) k_sw(SwScoreAr
     for (int x = kRows - 1; x <= c_begin - 2; ++x) {
       int ls = base + x;
       ls = ls >= buf ? ls - buf : ls;
-      ring[ls * stride] = 0xC0000000u;
+      ring[ls * stride] = dead;
     }
     if (c_end < W + kRows) {
       const int x_hi = min(W + kRows - 1, max(c_end - 1, 2 * kRows - 1));
