@@ -135,6 +135,13 @@ struct SeedParams {
   double lnfact[33];       // ln n!, summed in the reference's order
   int shape_shift;         // seed key = request << request_shift | shape << shape_shift | key
   int request_shift;
+  // Complexity test by the product P of the seed's bucket-count factorials
+  // (set by upload_seed_params): P <= p_accept[w] passes the cut, P >=
+  // p_reject[w] fails it, and in between the reference's double sum decides.
+  uint64_t p_accept[kMaxWeight + 1];
+  uint64_t p_reject[kMaxWeight + 1];
+  int key32;   // size^weight < 2^32 for every shape
+  int prod32;  // every weight <= 12 (P < 2^32)
 };
 
 }  // namespace drg

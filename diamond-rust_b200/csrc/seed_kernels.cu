@@ -7,10 +7,12 @@
 // s at letter i.  Letters of a sequence batch are contiguous in HBM, so the w
 // reads of a seed hit one or two 32-byte sectors shared by neighbouring
 // threads.  Seeds are written as 64-bit keys (request | shape | key) with a
-// 32-bit payload (the global letter index) and radix-sorted by CUB (stable:
-// equal keys share a shape and stay in letter order, as in the reference's
-// build); the join walks query key runs and binary-searches the sorted
-// reference keys.
+// 32-bit payload (the global letter index) and sorted by the device radix
+// sort (stable: equal keys share a shape and stay in letter order, as in the
+// reference's build); the join walks query key runs and binary-searches the
+// sorted reference keys.
+#include <cmath>
+
 #include "kernels.h"
 
 namespace drg {
@@ -20,11 +22,41 @@ namespace drg {
 __constant__ ShapeTable c_shapes[kConstSlots];
 __constant__ SeedParams c_seed[kConstSlots];
 
-void upload_seed_params(const ShapeTable& shapes, const SeedParams& p, int slot, cudaStream_t st) {
+// The complexity test (seed.rs:58-75) keeps a seed of weight w when
+// e = ln w! - sum over buckets of ln c_b! >= cut, that is when the integer
+// P = prod c_b! is at most T_w = exp(ln w! - cut).  P decides outright when it
+// lies outside T_w (1 -+ 1e-7): e then differs from the cut by more than
+// 1e-7, far above the 1e-13 rounding of the reference's double sum.  Closer
+// to T_w the device evaluates that sum in the reference's order.
+void seed_cut_bounds(SeedParams& p) {
+  for (int w = 0; w <= kMaxWeight; ++w) {
+    if (!(p.cut > 0.0)) {
+      p.p_accept[w] = UINT64_MAX;
+      p.p_reject[w] = UINT64_MAX;
+      continue;
+    }
+    const double t = std::exp(p.lnfact[w] - p.cut);
+    const double lo = t * (1.0 - 1e-7), hi = t * (1.0 + 1e-7);
+    p.p_accept[w] = lo < 1.0 ? 0 : (lo >= 1.8e19 ? UINT64_MAX : (uint64_t)std::floor(lo));
+    p.p_reject[w] = hi >= 1.8e19 ? UINT64_MAX : (uint64_t)std::ceil(hi);
+  }
+}
+
+void upload_seed_params(const ShapeTable& shapes, const SeedParams& params, int slot, cudaStream_t st) {
+  SeedParams p = params;
+  seed_cut_bounds(p);
+  p.key32 = 1;
+  p.prod32 = 1;
+  for (int s = 0; s < shapes.n; ++s) {
+    double mx = 1.0;
+    for (int k = 0; k < shapes.weight[s]; ++k) mx *= (double)p.size;
+    if (mx > 4294967295.0) p.key32 = 0;
+    if (shapes.weight[s] > 12) p.prod32 = 0;
+  }
   DRG_CUDA(cudaMemcpyToSymbolAsync(c_shapes, &shapes, sizeof(ShapeTable), slot * sizeof(ShapeTable),
                                    cudaMemcpyHostToDevice, st));
   DRG_CUDA(cudaMemcpyToSymbolAsync(c_seed, &p, sizeof(SeedParams), slot * sizeof(SeedParams),
-                                   cudaMemcpyHostToDevice, st));
+                                   cudaMemcpyHostToDevice, st));  // pageable source: staged before return
 }
 
 __global__ void k_letter_owner(const uint64_t* __restrict__ offsets, uint64_t n_seqs, uint64_t lo, uint64_t hi,
@@ -94,8 +126,6 @@ constexpr int kEnumBlock = 256;
 
 struct EnumTables {
   uint8_t rb[kEnumBlock + kMaxSpan];
-  double lnfact[33];
-  double lnstep[33];  // lnfact[j] - lnfact[j - 1]
 };
 
 __device__ __forceinline__ void stage_enum_tables(const uint8_t* __restrict__ letters, uint64_t base, uint64_t hi,
@@ -110,56 +140,56 @@ __device__ __forceinline__ void stage_enum_tables(const uint8_t* __restrict__ le
     }
     t.rb[j] = b;
   }
-  if (threadIdx.x < 33) {
-    t.lnfact[threadIdx.x] = sp.lnfact[threadIdx.x];
-    t.lnstep[threadIdx.x] = threadIdx.x ? sp.lnfact[threadIdx.x] - sp.lnfact[threadIdx.x - 1] : 0.0;
-  }
   __syncthreads();
 }
 
 // One seed from the staged buckets at rb: the reduced key and the
-// log-multinomial complexity test (seed.rs).  The counts live in three
-// 64-bit words (8 buckets x 8 bits each).  The reference's entropy is
-// lnfact[w] minus lnfact[c_b] for b = 0, 1, ... in bucket order; the same
-// quantity is first summed per letter as ln(count after the letter), which
-// differs from the bucket-ordered double result by under 1e-12.  Only when
-// that sum lies within 1e-9 of the cut is the bucket-ordered value computed,
-// so the decision is the reference's.
-__device__ __forceinline__ bool seed_at(const uint8_t* rb, int s, int slot, const EnumTables& t,
-                                        uint64_t* key_out) {
+// complexity test (seed.rs).  Bucket counts live in 5-bit fields of two
+// words (buckets 0-11 and 12-23), updated without branches; P collects the
+// count after each letter, so that P = prod over buckets of c_b!.  KT holds
+// the key (32 bits when size^w fits), PT the product (32 bits when w <= 12).
+template <typename KT, typename PT>
+__device__ __forceinline__ bool seed_at_t(const uint8_t* rb, int s, int slot, uint64_t* key_out) {
   const ShapeTable& shp = c_shapes[slot];
   const SeedParams& sp = c_seed[slot];
   const int w = shp.weight[s];
-  const uint64_t size = sp.size;
-  uint64_t key = 0, c0 = 0, c1 = 0, c2 = 0;
-  double acc = 0.0;
+  const KT size = (KT)sp.size;
+  KT key = 0;
+  uint64_t lo = 0, hi = 0;
+  PT prod = 1;
   for (int k = 0; k < w; ++k) {
     const uint32_t b = rb[shp.pos[s][k]];
     if (b >= 24) return false;
-    key = key * size + b;
-    const int sh = 8 * (b & 7);
+    key = key * size + (KT)b;
+    const bool up = b >= 12;
+    const uint32_t sh = 5 * (up ? b - 12 : b);
     const uint64_t inc = 1ull << sh;
-    uint64_t word;
-    if (b < 8) word = (c0 += inc);
-    else if (b < 16) word = (c1 += inc);
-    else word = (c2 += inc);
-    acc += t.lnstep[(word >> sh) & 0xffu];
+    lo += up ? 0ull : inc;
+    hi += up ? inc : 0ull;
+    prod *= (PT)(((up ? hi : lo) >> sh) & 31u);
   }
-  const double cut = sp.cut;
-  if (cut > 0.0) {
-    double e = t.lnfact[w] - acc;
-    if (fabs(e - cut) <= 1e-9) {
-      e = t.lnfact[w];
-      for (int b = 0; b < (int)size; ++b) {
-        uint64_t word = b < 8 ? c0 : (b < 16 ? c1 : c2);
-        uint32_t c = (uint32_t)(word >> (8 * (b & 7))) & 0xffu;
-        if (c > 0) e = __dsub_rn(e, t.lnfact[c]);
+  if (sp.cut > 0.0) {
+    const uint64_t P = (uint64_t)prod;
+    if (P > sp.p_accept[w]) {
+      if (P >= sp.p_reject[w]) return false;
+      // within 1e-7 of the cut: ln w! minus ln c_b! in bucket order, as the
+      // reference sums it
+      double e = sp.lnfact[w];
+      for (int b = 0; b < (int)sp.size; ++b) {
+        const uint32_t c = (uint32_t)(((b < 12 ? lo : hi) >> (5 * (b < 12 ? b : b - 12))) & 31u);
+        if (c > 0) e = __dsub_rn(e, sp.lnfact[c]);
       }
+      if (!(e >= sp.cut)) return false;
     }
-    if (!(e >= cut)) return false;
   }
-  *key_out = key;
+  *key_out = (uint64_t)key;
   return true;
+}
+
+__device__ __forceinline__ bool seed_at(const uint8_t* rb, int s, int slot, uint64_t* key_out) {
+  const SeedParams& sp = c_seed[slot];
+  if (sp.key32 && sp.prod32) return seed_at_t<uint32_t, uint32_t>(rb, s, slot, key_out);
+  return seed_at_t<uint64_t, uint64_t>(rb, s, slot, key_out);
 }
 
 // K = uint32_t: the caller guarantees that the seed key (with the request,
@@ -181,7 +211,7 @@ __global__ void k_seed_enum(const uint8_t* __restrict__ letters, const uint64_t*
   const uint64_t req = request ? (uint64_t)request[seq] << sp.request_shift : 0;
   for (int s = 0; s < n_shapes; ++s) {
     uint64_t key = 0;
-    const bool ok = g + c_shapes[slot].span[s] <= end && seed_at(tab.rb + threadIdx.x, s, slot, tab, &key);
+    const bool ok = g + c_shapes[slot].span[s] <= end && seed_at(tab.rb + threadIdx.x, s, slot, &key);
     keys[s * L + i] = ok ? (K)(req | ((uint64_t)s << sp.shape_shift) | key) : (K)kNoSeed;
     vals[s * L + i] = (uint32_t)g;
   }
@@ -267,7 +297,7 @@ __global__ void __launch_bounds__(kFilterBlock)
     const int s1 = min(n_shapes, s0 + kFilterGroup);
     for (int s = s0; s < s1; ++s) {
       uint64_t key = 0;
-      if (in && g + c_shapes[slot].span[s] <= end && seed_at(tab.rb + threadIdx.x, s, slot, tab, &key)) {
+      if (in && g + c_shapes[slot].span[s] <= end && seed_at(tab.rb + threadIdx.x, s, slot, &key)) {
         ++valid;
         const uint64_t k = ((uint64_t)s << sp.shape_shift) | key;
         const uint32_t h = seed_key_hash(k, log2_bits);

@@ -247,10 +247,12 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS >= 2 ? 3 : 1) k_sw(SwScoreAr
     }
     __syncwarp();
     L.jbase = i0 - d1;
+    // column c_begin - 1 of the strip: dead cells (H = 0, so H - oc = -oc,
+    // which is also pair 0's diagonal operand and row 8's E source)
 #pragma unroll
     for (int p = 0; p < kPairs; ++p) {
       R.H[p] = 0;
-      R.Hm[p] = kNeg2;
+      R.Hm[p] = noc2;
       R.F[p] = kNeg2;
     }
     R.mx0 = R.mx1 = 0;
