@@ -216,7 +216,8 @@ def serve_stream(w, device, n_requests, repeats):
     sensitive / very-sensitive) against the resident database, served plain
     (one request at a time, the seed index rebuilt per search as the reference
     does) and continuously batched (2 worker contexts taking turns on the
-    GPU, a 1M-letter batch budget, each preset's seed index resident).  Both
+    GPU, admission capped at max(64k letters, the oldest request's letters),
+    each preset's seed index resident).  Both
     are warmed first; the stream is replayed `repeats` times per form at its
     rate (forms alternating), then once with every request queued at once
     (capacity)."""
@@ -233,16 +234,21 @@ def serve_stream(w, device, n_requests, repeats):
                      f"latency = arrival to results on the host; {repeats} replays per form at the stream's rate "
                      f"(median and range), then all requests queued at once (capacity); plain: one request at a "
                      f"time, seed index rebuilt per search; batched: 2 worker contexts taking turns on the GPU "
-                     f"(host work of one beside the other's search), continuous batching under a 1M-letter "
-                     f"batch budget, seed index resident per preset; both forms warmed with one search per "
-                     f"preset of the stream's largest request before it starts"}
+                     f"(host work of one beside the other's search), continuous batching (a batch holds at most "
+                     f"max(64k letters, its oldest request's letters)), seed index resident and tuning autotuned "
+                     f"per preset; both forms warmed with one search per preset of the stream's largest request "
+                     f"before it starts (the batched form autotunes on it, once per run: later servers read "
+                     f"the tuning cache)"}
 
     warm_queries = max((r for _, r in base), key=lambda r: len(r.queries)).queries
+    import tempfile
+    tune_fd, tune_cache = tempfile.mkstemp(prefix="drgpu_serve_tuning_", suffix=".txt")
+    os.close(tune_fd)
 
     def replay(batched, rate):
         stream = [(t * 20.0 / rate, serve.Request(r.rid, r.preset, r.queries)) for t, r in base]
         srv = serve.Server(dl, do, workers=2 if batched else 1, batch=batched, device=device,
-                           index_budget=(16 << 30) if batched else 0)
+                           index_budget=(16 << 30) if batched else 0, tune_cache=tune_cache if batched else None)
         try:
             srv.warm(presets, warm_queries)  # both forms: scratch at working size before the stream
             finished, span = serve.run_stream(srv, stream)
@@ -265,6 +271,7 @@ def serve_stream(w, device, n_requests, repeats):
         out[name] = summ
     for name in ("plain", "batched"):
         out[name + "_capacity"] = replay(name == "batched", 1e6)
+    os.unlink(tune_cache)
     return out
 
 

@@ -242,7 +242,7 @@ int drg_radix_sort(drg_ctx* c, void* keys, int32_t key_bytes, uint32_t* vals, ui
       end_bit > 8 * key_bytes)
     return DRG_ERR_INVALID;
   API_BEGIN(c)
-  if (n >= (1ull << 30)) throw Error(DRG_ERR_INVALID, "radix sort: at most 2^30 - 1 keys");
+  if (n >= (1ull << 32)) throw Error(DRG_ERR_INVALID, "radix sort: at most 2^32 - 1 keys");
   // with the count on the device, the buffers hold a larger capacity (tiles
   // past the count are never taken), as when a sort follows the kernel that
   // counted its input

@@ -68,6 +68,7 @@ struct drg_batch {
   uint64_t* offsets = nullptr;
   uint32_t* owner = nullptr;
   uint32_t* request = nullptr;  // device: request of each target (null: one request)
+  uint32_t max_request = 0;     // largest request id (the seed keys' request field width)
   std::vector<uint64_t> h_offsets;
   std::vector<uint32_t> query;
   std::vector<uint8_t> frame;

@@ -327,6 +327,10 @@ constexpr int kSwMaxWidth = 1700;                       // wider bands use the e
 // The packed kernel's profile bytes hold a score plus the open cost (gap open
 // + extend): with larger open costs its bands go to the band kernel.
 constexpr int kSwMaxOpenCost = 64;
+// Bands whose best can reach this bound are not packed: every H of the packed
+// kernel stays below 0x7C00 (its strip maximum folds H on the FMA pipe as
+// half-precision bit patterns) and far from the 16-bit limit.
+constexpr int kSwPackedMaxBest = 31743;
 constexpr int kSwBandMinWidth = kSwC1 + 1;  // score pass: wider bands run one warp per band
 constexpr int kSwClasses = 4;
 int sw_width_class(int width);  // 0..3, or -1 for the exact kernel
@@ -349,7 +353,7 @@ struct SortResult {
 // Stable LSD sort of keys[0, n) by bits [begin_bit, end_bit), with optional u32
 // values (vals == nullptr: keys only).  n is *d_n when d_n is set (a count
 // written by an earlier launch; n_max bounds it and sizes the grids), else
-// n_max; n < 2^30.  keys_alt / vals_alt are buffers of the same capacity;
+// n_max; n < 2^32.  keys_alt / vals_alt are buffers of the same capacity;
 // both buffers of each array are overwritten.  temp is the sort's scratch;
 // *d_err becomes non-zero if a tile's bounded wait for an earlier tile gave up
 // (the outputs are then not valid).  small_tiles: half the keys per tile.

@@ -236,7 +236,7 @@ __device__ __forceinline__ SwRoute sw_route(const Band& b, const uint64_t* s_off
   band_rows(b, m, false, &r.rs, &r.re);
   band_rows(b, m, true, &r.ts, &r.te);
   const int64_t mn = m < (int64_t)b.n ? m : (int64_t)b.n;
-  r.fast = W >= tn.min_packed && W <= kSwMaxWidth && (int64_t)max_score * mn <= 32000 && r.rs <= r.re &&
+  r.fast = W >= tn.min_packed && W <= kSwMaxWidth && (int64_t)max_score * mn <= kSwPackedMaxBest && r.rs <= r.re &&
            b.target < (1u << 21) && b.q0 < 65536 && r.re < 65536;
   r.wide = r.fast && W >= tn.wide_min;
   // narrow bands only: a medium band (W > 136) in a subject's warps would
@@ -1042,7 +1042,10 @@ void Search::query_seeds(uint64_t* n_runs_out) {
     uint64_t* keys = c->q_keys.as<uint64_t>(N);
     uint64_t* keys_s = c->q_keys_s.as<uint64_t>(N);
     launch_seed_enum(q->letters, q->offsets, q->owner, 0, q->total, S, keys, vals, c->slot, c->stream, q->request);
-    const int key_bits = q->request ? 64 : seed_key_bits;  // request ids sit above the seed key
+    // request ids sit above the seed key: the sort covers their field up to
+    // the batch's largest id ("no seed" keys, all ones, still sort last: a
+    // valid key's shape field has a zero bit)
+    const int key_bits = q->request ? std::min(64, seed_key_bits + bits_for(q->max_request)) : seed_key_bits;
     const SortResult<uint64_t> r = dsort(c, keys, keys_s, vals, vals_s, N, 0, key_bits);
     if (r.vals != vals_s) c->q_vals.swap(c->q_vals_s);
     // runs of every key (the "no seed" keys, last, form one run of their own),
@@ -1146,12 +1149,12 @@ void Search::join_chunk(uint64_t c0, uint64_t c1, uint64_t n_runs) {
     }
     // the kept count stays on the device: the sort, the bucket starts and the
     // join read it there (no host wait); the valid count joins the counters.
-    // A chunk with more seed positions than one sort takes (2^30) reads the
-    // kept count first (the kept seeds are the ones its queries can join).
+    // A chunk with more seed positions than one sort takes (2^32 - 1) reads
+    // the kept count first (the kept seeds are the ones its queries can join).
     count_launch();
     k_add_u64<<<1, 1, 0, c->stream>>>(d_counters + 7, cnt + 1);
     uint64_t n_sort = N;
-    if (N < (1ull << 30)) {
+    if (N < (1ull << 32)) {
       d_nr = reinterpret_cast<const uint64_t*>(cnt);
       nr = (int64_t)N;  // capacity
     } else {
@@ -1816,9 +1819,15 @@ drg_batch* make_batch(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offs
       DRG_CUDA(cudaMemcpyAsync(b->letters, letters, b->total, cudaMemcpyHostToDevice, ctx->stream));
     DRG_CUDA(cudaMemcpyAsync(b->offsets, offsets, (n + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, ctx->stream));
     launch_letter_owner(b->offsets, n, 0, b->total, b->owner, ctx->stream);
-    if (request && n > 0) {  // per-request join accounting
-      for (uint64_t i = 0; i < n; ++i)
-        if (request[i] > kMaxRequests) throw Error(DRG_ERR_INVALID, "request id out of range");
+    // per-request join accounting; a batch of one request counts over the
+    // whole batch, which is the plain search (narrower seed keys)
+    bool several = false;
+    for (uint64_t i = 0; request && i < n; ++i) {
+      if (request[i] > kMaxRequests) throw Error(DRG_ERR_INVALID, "request id out of range");
+      several = several || request[i] != request[0];
+      b->max_request = std::max(b->max_request, request[i]);
+    }
+    if (several) {
       pool_alloc(ctx, &b->request, n * sizeof(uint32_t));
       DRG_CUDA(cudaMemcpyAsync(b->request, request, n * sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
     }

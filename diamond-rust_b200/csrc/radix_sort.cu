@@ -251,7 +251,8 @@ __device__ __forceinline__ void onesweep_tile(OnesweepShared<K, VALS, SMALL>& s,
     s.digit[p] = (uint8_t)dig[j];
   }
   __syncthreads();
-  // (32-bit arithmetic: global_base may be "negative", positions are < 2^30)
+  // (32-bit arithmetic: global_base may be "negative"; every position is
+  // below n < 2^32, so the sum modulo 2^32 is the position)
   for (int i = t; i < valid; i += kSortThreads) {
     const uint32_t o = s.global_base[s.digit[i]] + (uint32_t)i;
     if (o < n) kout[o] = s.stage.keys[i];
@@ -347,7 +348,7 @@ SortResult<K> radix_sort(K* keys, K* keys_alt, uint32_t* vals, uint32_t* vals_al
                          const uint64_t* d_n, int begin_bit, int end_bit, SortScratch& temp, uint32_t* d_err,
                          cudaStream_t st, bool small_tiles) {
   SortResult<K> r{keys, vals};
-  if (n_max >= (1ull << 30)) throw Error(DRG_ERR_INVALID, "radix sort: at most 2^30 - 1 keys per sort");
+  if (n_max >= (1ull << 32)) throw Error(DRG_ERR_INVALID, "radix sort: at most 2^32 - 1 keys per sort");
   if (end_bit > (int)(8 * sizeof(K))) end_bit = 8 * sizeof(K);
   const SortPlan p = plan<K>(n_max, begin_bit, end_bit, small_tiles);
   if (p.passes == 0 || (n_max == 0 && !d_n)) return r;

@@ -37,6 +37,15 @@ __device__ __forceinline__ uint32_t max2_relu(uint32_t a, uint32_t b) {
   asm("max.s16x2.relu %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
   return r;
 }
+// Maximum of two pairs of non-negative 16-bit integers below 0x7C00 on the
+// FMA pipe: such bit patterns are zero, subnormal or finite positive halves,
+// ordered like the integers, and max.f16x2 (no flush to zero) returns one of
+// its inputs.
+__device__ __forceinline__ uint32_t max2_pos_f16(uint32_t a, uint32_t b) {
+  uint32_t r;
+  asm("max.f16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+  return r;
+}
 // keep halves selected by k (0xFFFF per kept half), replace the others with v
 __device__ __forceinline__ uint32_t sel2(uint32_t x, uint32_t k, uint32_t v) { return (x & k) | (v & ~k); }
 

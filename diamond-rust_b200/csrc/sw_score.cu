@@ -30,7 +30,8 @@
 // (that is what the ring keeps), so the profile rows 0 and 8 carry + oc.
 //
 // Exactness: values equal the reference's int32 DP while the band's best is
-// below 2^15 (bands that could exceed it are not given to this kernel).
+// below 31744 = 0x7C00 (bands that could reach it are not given to this
+// kernel); the strip maximum relies on that bound (max2_pos_f16).
 // Cells with j < 0, j > m or rows past the query read a sentinel residue
 // scoring -64; they can neither raise the maximum above the true band maximum
 // nor feed an in-band cell.  Rows past m + d1 are not computed: the reference
@@ -134,11 +135,12 @@ __device__ __forceinline__ void sw_step(SRegs& R, Lane& L, int c, const uint8_t*
     hm_up = hm;
     e_up = e;
   }
-  // the strip's maximum, two accumulators of four pairs each
-  R.mx0 = __vimax3_s16x2(R.mx0, R.H[0], R.H[1]);
-  R.mx1 = __vimax3_s16x2(R.mx1, R.H[4], R.H[5]);
-  R.mx0 = __vimax3_s16x2(R.mx0, R.H[2], R.H[3]);
-  R.mx1 = __vimax3_s16x2(R.mx1, R.H[6], R.H[7]);
+  // the strip's maximum, two accumulators of four pairs each, on the FMA
+  // pipe (H is in [0, 0x7C00): see max2_pos_f16), beside the ALU's DP work
+  R.mx0 = max2_pos_f16(R.mx0, max2_pos_f16(R.H[0], R.H[1]));
+  R.mx1 = max2_pos_f16(R.mx1, max2_pos_f16(R.H[4], R.H[5]));
+  R.mx0 = max2_pos_f16(R.mx0, max2_pos_f16(R.H[2], R.H[3]));
+  R.mx1 = max2_pos_f16(R.mx1, max2_pos_f16(R.H[6], R.H[7]));
   R.E7 = e_up;
   *wp = prmt(R.Hm[kPairs - 1], R.E7, 0x7632);  // (H - oc, E) of row 15 at column c - 1
   R.hmtop_old = hm_top;

@@ -14,10 +14,16 @@ order the workers reached the GPU): a search fills the GPU by itself, and two
 searches side by side each take about twice as long, which lengthens the tail
 of the latency.  What a worker does on the host (assembling the next batch's
 letters, building Python records of the last one) overlaps the other worker's
-search.
+search.  Under a backlog (8 or more requests queued behind a batch) the
+searches overlap instead: each fills the GPU while the other waits on the
+host, which raises throughput when latency is set by the queue anyway.
 
-The letter budget bounds a batch's work, so that a batch takes about as long
-as one large request: small requests share a batch, large ones run alone.
+Admission protects the oldest request: a batch holds at most max(64k
+letters, the oldest request's letters) (merge_floor, merge_ratio), so small
+requests share a batch while a large request runs alone and is not delayed by
+the work of requests behind it.  (With a plain letter budget of 1M letters,
+large requests of one preset merged, and the tail of the latency grew with
+the merged batches' work.)  The letter budget caps any batch.
 Results come back to the host as three bulk copies per batch (HSP records,
 per-target offsets, alignment ops); Python records are built only when a
 request's results are read, outside the worker loop.
@@ -113,12 +119,29 @@ class Server:
     """Continuous-batching request loop over one resident database."""
 
     def __init__(self, db_letters, db_offsets, workers=2, batch=True, budget_letters=1_000_000, device=0,
-                 index_chunks=None, index_budget=0):
+                 index_chunks=None, index_budget=0, merge_ratio=1.0, merge_floor=64_000, tune_cache=None,
+                 overlap_backlog=8):
         self.ctxs = [Context(device) for _ in range(workers)]
         # index_budget > 0: each preset's sorted reference seeds stay resident
         self.db = ResidentDb(self.ctxs[0], db_letters, db_offsets, index_budget=index_budget)
         self.batch = batch
         self.budget = budget_letters
+        # a batch holds at most max(merge_floor, merge_ratio x its oldest
+        # request's letters) (and the budget): later requests merged into a
+        # large request delay it by their work, small ones barely
+        self.merge_ratio = merge_ratio
+        self.merge_floor = merge_floor
+        # tune_cache (a file path): warm() autotunes each preset on its warm-up
+        # request (drg_autotune, results cached in the file) and each batch of
+        # that preset runs with its tuning; no tuning changes any result
+        self.tune_cache = tune_cache
+        self.tunings: dict = {}
+        self.base_tuning = self.ctxs[0].tuning()
+        # with at least this many requests still queued behind a batch, the
+        # batch does not wait for its turn: under a backlog the searches
+        # overlap on the GPU, filling each other's host phases (throughput);
+        # otherwise they take turns (latency)
+        self.overlap_backlog = overlap_backlog
         self.index_chunks = index_chunks
         self.pending: list[Request] = []
         self.lock = threading.Condition()
@@ -148,11 +171,15 @@ class Server:
             self.pending.pop(0)
             return [head]
         take, used = [], 0
+        cap = self.budget
+        if self.merge_ratio is not None:
+            head_size = sum(len(q) for q in head.queries)
+            cap = min(cap, max(self.merge_floor, self.merge_ratio * head_size))
         for r in list(self.pending):
             if r.preset != head.preset:
                 continue
             size = sum(len(q) for q in r.queries)
-            if take and used + size > self.budget:
+            if take and used + size > cap:
                 break
             take.append(r)
             used += size
@@ -168,9 +195,13 @@ class Server:
                 if not self.pending and self.closed:
                     return
                 reqs = self._take()
+                backlog = self.batch and len(self.pending) >= self.overlap_backlog
             try:
+                if self.tunings:
+                    ctx.set_tuning(**self.tunings.get(reqs[0].preset, self.base_tuning))
                 arrays = batch_arrays(reqs)  # host work, beside the other worker's search
-                search_batch(ctx, self.db, reqs, reqs[0].preset, self.index_chunks, arrays, self.gpu_turn)
+                search_batch(ctx, self.db, reqs, reqs[0].preset, self.index_chunks, arrays,
+                             None if backlog else self.gpu_turn)
             except BaseException as e:  # surfaced by close()
                 self.errors.append(e)
             t = self.now()
@@ -184,8 +215,23 @@ class Server:
         """Searches `queries` once per preset before serving (untimed): the
         contexts' scratch buffers grow to their working size and, with an
         index budget, each preset's seed index is built."""
+        if self.tune_cache:
+            letters, offsets = concat(list(queries))
+            with self.gpu_turn:
+                ctx = self.ctxs[0]
+                batch = ResidentBatch(ctx, letters, offsets)
+                try:
+                    for preset in presets:
+                        cfg = make_config(sensitivity=preset, index_chunks=self.index_chunks)
+                        start = ctx.tuning()
+                        self.tunings[preset] = ctx.autotune(self.db, batch, cfg, cache_path=self.tune_cache)[0]
+                        ctx.set_tuning(**start)
+                finally:
+                    batch.close()
         for ctx in self.ctxs:
             for preset in presets:
+                if self.tunings:
+                    ctx.set_tuning(**self.tunings.get(preset, self.base_tuning))
                 search_batch(ctx, self.db, [Request(-1, preset, list(queries))], preset, self.index_chunks,
                              gpu_turn=self.gpu_turn)
 

@@ -182,7 +182,7 @@ int drg_seed_join(drg_ctx* ctx, const drg_seed_entry* query, uint64_t n_query, c
  * sort_unstable_by_key) and align_target's hit sort (search.rs:178), from host
  * buffers: keys (key_bytes 4 or 8) and, when vals is not NULL, u32 values are
  * sorted in place by bits [begin_bit, end_bit) of the key, stably (equal keys
- * keep their order).  n < 2^30.  count_on_device = 1 hands the sort its count
+ * keep their order).  n < 2^32.  count_on_device = 1 hands the sort its count
  * in device memory, as the search does when a sort follows the kernel that
  * counted its input. */
 int drg_radix_sort(drg_ctx* ctx, void* keys, int32_t key_bytes, uint32_t* vals, uint64_t n, int32_t begin_bit,
@@ -263,7 +263,8 @@ int drg_batch_create(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offse
  * query occurrences per request (search.rs:109-131 counts them over the whole
  * run), so every request's HSPs equal those of a search of its targets alone;
  * all requests of a batch share the database and the search configuration.
- * No reference counterpart: search::run serves one request per call. */
+ * A batch whose targets all carry one request id is searched as a plain
+ * batch.  No reference counterpart: search::run serves one request per call. */
 int drg_batch_create_requests(drg_ctx* ctx, const uint8_t* letters, const uint64_t* offsets,
                               const uint32_t* query_index, const uint8_t* frame, const uint32_t* request,
                               uint64_t n_targets, drg_batch** out);

@@ -94,7 +94,7 @@ def test_mixed_batches_equal_alone(ctx, preset):
         db.close()
 
 
-def test_server_stream_continuous_batching():
+def test_server_stream_continuous_batching(tmp_path):
     w = synth.workload(2, n_queries=10, n_db=1200, seed_offset=33)
     dl, do = drgpu.concat(w.db)
     rng = np.random.Generator(np.random.PCG64(5))
@@ -102,9 +102,13 @@ def test_server_stream_continuous_batching():
     # admitted as one batch whatever the speed of the GPU
     stream = serve.poisson_stream(rng, 24, rate=1e6, max_queries=12,
                                   presets=["fast", "default", "sensitive", "very-sensitive"], q_hi=600)
-    srv = serve.Server(dl, do, workers=2, batch=True, index_budget=1 << 30)
+    srv = serve.Server(dl, do, workers=2, batch=True, index_budget=1 << 30, tune_cache=str(tmp_path / "tune.txt"))
     try:
-        srv.warm(["fast", "very-sensitive"], w.queries[:3])  # grows scratch, builds two presets' indexes
+        # grows scratch, builds two presets' indexes and autotunes them (the
+        # other presets run with the base tuning)
+        srv.warm(["fast", "very-sensitive"], w.queries[:3])
+        assert set(srv.tunings) == {"fast", "very-sensitive"}
+        assert (tmp_path / "tune.txt").read_text().count("\n") == 2
         finished, span = serve.run_stream(srv, stream)
     finally:
         srv.close()
