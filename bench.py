@@ -61,6 +61,7 @@ def parse():
     p.add_argument("--no-very-sensitive", action="store_true", help="skip the very-sensitive leg")
     p.add_argument("--no-batching", action="store_true", help="skip the batched-vs-plain leg")
     p.add_argument("--blastx-reads", type=int, default=20000, help="reads in the blastx leg")
+    p.add_argument("--blastx-db", type=int, default=20000, help="database sequences of the blastx leg")
     p.add_argument("--serve-requests", type=int, default=500, help="requests in the serving stream")
     p.add_argument("--serve-repeats", type=int, default=3, help="replays of the stream per serving form")
     p.add_argument("--batch-queries", type=int, default=50000, help="queries of the batched-vs-plain leg")
@@ -375,7 +376,7 @@ def batching_leg(ctx, n_queries, n_db, sample, batched_only=False):
     return out
 
 
-def blastx_leg(ctx, steps, warmup, n_reads, cpu_sample, with_cpu):
+def blastx_leg(ctx, steps, warmup, n_reads, cpu_sample, with_cpu, n_db=20000):
     """blastx (--fast) end to end through the C ABI: reads from host memory,
     six-frame translation and ORF masking on the device
     (drg_batch_create_blastx), search, merge_frames, results on the host.
@@ -383,7 +384,7 @@ def blastx_leg(ctx, steps, warmup, n_reads, cpu_sample, with_cpu):
     import numpy as np
     import drgpu
     from drgpu import synth
-    w = synth.read_workload(n_reads=n_reads, n_db=20000, seed_offset=0)
+    w = synth.read_workload(n_reads=n_reads, n_db=n_db, seed_offset=0)
     dl, do = drgpu.concat(w.db)
     db = drgpu.ResidentDb(ctx, dl, do)
     cfg = drgpu.make_config(sensitivity="fast")
@@ -405,8 +406,9 @@ def blastx_leg(ctx, steps, warmup, n_reads, cpu_sample, with_cpu):
         dt, st, hsps, frames = one()
         total += dt
         search_ms += st["ms_total"]
-    out = {"workload": f"{n_reads} reads (150-300 nt, 30 % reverse-translated DB fragments) x 20,000-sequence "
-                       f"synthetic DB, blastx --fast, BLOSUM62 11/1, e 1e-3, k 25", "reads_per_s": n_reads * steps / total,
+    out = {"workload": f"{n_reads} reads (150-300 nt, 30 % reverse-translated DB fragments) x {n_db:,}-sequence "
+                       f"synthetic DB ({int(do[-1]):,} aa), blastx --fast, BLOSUM62 11/1, e 1e-3, k 25",
+           "reads_per_s": n_reads * steps / total,
            "ms_per_step": 1000.0 * total / steps, "search_ms_per_step": search_ms / steps, "frames": frames,
            "hsps": hsps, "h2d_nt_bytes_per_step": nt_bytes,
            "what": "wall time per step: reads uploaded, translated on the GPU, searched, merged per read"}
@@ -640,7 +642,7 @@ def main():
     blastx = None
     if not args.no_blastx:
         blastx = blastx_leg(ctx, args.steps, max(1, args.warmup), args.blastx_reads, 2000,
-                            rank == 0 and world == 1 and not args.no_cpu)
+                            rank == 0 and world == 1 and not args.no_cpu, args.blastx_db)
 
     # ---- CPU baseline and sample parity (rank 0, N = 1) ---------------------
     cpu = None
