@@ -94,9 +94,14 @@ void launch_bucket_first(const uint32_t* keys, uint64_t n, int shift, uint32_t n
                          const uint64_t* d_n = nullptr);
 
 // Layout of the packed 64-bit hit key (target, subject, diag + doff, spos).
+// Hit key: target - t_base (tb bits) | subject (sb) | diagonal + doff (db) |
+// subject position (pb).  A batch whose full key would pass 64 bits is
+// searched in target windows of at most 2^tb targets, t_base the window's
+// first target.
 struct HitKeyLayout {
   int tb, sb, db, pb;
   int64_t doff;
+  uint32_t t_base = 0;
   int total() const { return tb + sb + db + pb; }
 };
 

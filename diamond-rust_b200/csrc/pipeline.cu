@@ -968,19 +968,33 @@ struct Search {
     return k;
   }
 
+  // The hit key of the current target window [t_base, t_base + t_window).
   HitKeyLayout layout() const {
     HitKeyLayout L;
-    L.tb = bits_for(q->n > 0 ? q->n - 1 : 0);
+    L.tb = bits_for(t_window > 0 ? t_window - 1 : 0);
     L.sb = bits_for(db->n > 0 ? db->n - 1 : 0);
     L.doff = (int64_t)db->max_len;
     L.db = bits_for((uint64_t)q->max_len + db->max_len);
     L.pb = bits_for(db->max_len);
     if (L.tb < 1) L.tb = 1;
     if (L.sb < 1) L.sb = 1;
-    if (L.total() > 64)
-      throw Error(DRG_ERR_INVALID, "batch too large: hit key needs " + std::to_string(L.total()) + " bits");
+    L.t_base = (uint32_t)t_base;
     return L;
   }
+  // Targets per window: all of them when the full key fits 64 bits, else as
+  // many as the bits left beside subject, diagonal and position allow (the
+  // join then runs in blocks of at most that many targets).
+  void set_target_window() {
+    t_base = 0;
+    t_window = q->n;
+    const int rest = bits_for(db->n > 0 ? db->n - 1 : 0) + bits_for((uint64_t)q->max_len + db->max_len) +
+                     bits_for(db->max_len);
+    if (std::max(1, bits_for(q->n > 0 ? q->n - 1 : 0)) + std::max(1, rest) <= 64) return;
+    if (rest > 63)
+      throw Error(DRG_ERR_INVALID, "database too large: hit key needs " + std::to_string(rest + 1) + " bits");
+    t_window = 1ull << (64 - rest);
+  }
+  uint64_t t_base = 0, t_window = 0;
 
   void run(drg_result* out);
   void query_seeds(uint64_t* n_runs);
@@ -1256,7 +1270,7 @@ void Search::join_chunk(uint64_t c0, uint64_t c1, uint64_t n_runs) {
     acc_n += n_hits;
   };
   const uint64_t n_hits = scan_hits();
-  if (n_hits <= hit_budget || q->n == 1) {
+  if ((n_hits <= hit_budget || q->n == 1) && q->n <= t_window) {
     // the stages after the join run on hits of several chunks at once, up to
     // the budget (a subject lives in one chunk: pairs never span passes)
     if (acc_n > 0 && acc_n + n_hits > hit_budget) {
@@ -1270,7 +1284,8 @@ void Search::join_chunk(uint64_t c0, uint64_t c1, uint64_t n_runs) {
     return;
   }
   // ---- query blocks: consecutive targets whose hits stay under the budget
-  // (a target is never split: its pairs are then all in one pass)
+  // and that fit one target window of the hit key (a target is never split:
+  // its pairs are then all in one pass)
   unsigned long long* thits = c->target_hits.as<unsigned long long>(q->n);
   DRG_CUDA(cudaMemsetAsync(thits, 0, q->n * sizeof(unsigned long long), c->stream));
   launch_target_hits(c->run_counts.as<uint32_t>(0), c->run_qstart.as<uint32_t>(0), rcnt, rhits, n_runs,
@@ -1280,7 +1295,7 @@ void Search::join_chunk(uint64_t c0, uint64_t c1, uint64_t n_runs) {
   std::vector<std::pair<uint64_t, uint64_t>> blocks;
   for (uint64_t t0 = 0; t0 < q->n;) {
     uint64_t t1 = t0, sum = 0;
-    while (t1 < q->n && (t1 == t0 || sum + th[t1] <= hit_budget)) sum += th[t1++];
+    while (t1 < q->n && t1 - t0 < t_window && (t1 == t0 || sum + th[t1] <= hit_budget)) sum += th[t1++];
     blocks.push_back({t0, t1});
     t0 = t1;
   }
@@ -1292,6 +1307,7 @@ void Search::join_chunk(uint64_t c0, uint64_t c1, uint64_t n_runs) {
   uint32_t* qlo = c->run_qlo.as<uint32_t>(n_runs + 1);
   uint32_t* qcnt = c->run_qcount.as<uint32_t>(n_runs + 1);
   for (auto [t0, t1] : blocks) {
+    t_base = t0;  // the hit keys of this block (expand, then process_hits)
     JoinBlock jb{c->q_vals_s.as<uint32_t>(0), c->run_qstart.as<uint32_t>(0), q->h_offsets[t0], q->h_offsets[t1], qlo,
                  qcnt};
     const uint64_t key_mask = (1ull << seed_key_bits) - 1;
@@ -1307,6 +1323,7 @@ void Search::join_chunk(uint64_t c0, uint64_t c1, uint64_t n_runs) {
     process_hits(pass++);
     tm.start();
   }
+  t_base = 0;
   tm.stop(&st.ms_join);
 }
 
@@ -1688,6 +1705,7 @@ void Search::run(drg_result* out) {
     out->stats = st;
     return;
   }
+  set_target_window();
   Timer tm(c, &times);
   tm.start();
   uint64_t n_runs = 0;

@@ -546,7 +546,7 @@ __global__ void k_join_expand(JoinExpandArgs a) {
     int64_t qpos = (int64_t)qg - (int64_t)a.q_offsets[t];
     int64_t spos = (int64_t)rg - (int64_t)a.r_offsets[s];
     const HitKeyLayout& L = a.layout;
-    uint64_t key = (uint64_t)t;
+    uint64_t key = (uint64_t)(t - L.t_base);
     key = (key << L.sb) | (uint64_t)s;
     key = (key << L.db) | (uint64_t)(qpos - spos + L.doff);
     key = (key << L.pb) | (uint64_t)spos;

@@ -96,7 +96,7 @@ __device__ __forceinline__ unsigned long long xdrop_run(const XdropArgs& a, uint
   uint64_t i = a.run_head_idx[r];
   const HitKeyLayout L = a.layout;
   const uint64_t run = a.hit_keys[i] >> L.pb;
-  const uint32_t t = (uint32_t)(a.hit_keys[i] >> (L.pb + L.db + L.sb));
+  const uint32_t t = (uint32_t)(a.hit_keys[i] >> (L.pb + L.db + L.sb)) + L.t_base;
   const uint32_t sj = (uint32_t)((a.hit_keys[i] >> (L.pb + L.db)) & ((1ull << L.sb) - 1));
   const int64_t diag = (int64_t)((a.hit_keys[i] >> L.pb) & ((1ull << L.db) - 1)) - L.doff;
   const uint8_t* q = a.q_letters + a.q_offsets[t];
@@ -227,7 +227,7 @@ __global__ void k_xdrop_runs(XdropArgs a) {
   if (live) {
     i = a.run_head_idx[r];
     run = a.hit_keys[i] >> L.pb;
-    const uint32_t t = (uint32_t)(a.hit_keys[i] >> (L.pb + L.db + L.sb));
+    const uint32_t t = (uint32_t)(a.hit_keys[i] >> (L.pb + L.db + L.sb)) + L.t_base;
     const uint32_t sj = (uint32_t)((a.hit_keys[i] >> (L.pb + L.db)) & ((1ull << L.sb) - 1));
     diag = (int64_t)((a.hit_keys[i] >> L.pb) & ((1ull << L.db) - 1)) - L.doff;
     q = a.q_letters + a.q_offsets[t];
@@ -357,7 +357,7 @@ __global__ void k_build_bands(BandArgs a) {
   const HitKeyLayout L = a.layout;
   uint64_t b = a.pair_head_idx[p], e = a.pair_head_idx[p + 1];
   const uint64_t k0 = a.seg_keys[b];
-  const uint32_t t = (uint32_t)(k0 >> (L.pb + L.db + L.sb));
+  const uint32_t t = (uint32_t)(k0 >> (L.pb + L.db + L.sb)) + L.t_base;
   const uint32_t sj = (uint32_t)((k0 >> (L.pb + L.db)) & ((1ull << L.sb) - 1));
   const uint32_t qlen = (uint32_t)(a.q_offsets[t + 1] - a.q_offsets[t]);
   // band_for (gapped.rs:27-32)

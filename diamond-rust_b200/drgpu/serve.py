@@ -14,9 +14,11 @@ order the workers reached the GPU): a search fills the GPU by itself, and two
 searches side by side each take about twice as long, which lengthens the tail
 of the latency.  What a worker does on the host (assembling the next batch's
 letters, building Python records of the last one) overlaps the other worker's
-search.  Under a backlog (8 or more requests queued behind a batch) the
-searches overlap instead: each fills the GPU while the other waits on the
-host, which raises throughput when latency is set by the queue anyway.
+search.  On request (overlap_backlog) the searches overlap under a backlog
+instead: each fills the GPU while the other waits on the host.  That raised
+the capacity with every request queued (43-46K against 43K queries/s) but,
+in a burst of a 20 requests/s stream, held p99 near 1 s: it is off by
+default.
 
 Admission protects the oldest request: a batch holds at most max(64k
 letters, the oldest request's letters) (merge_floor, merge_ratio), so small
@@ -120,7 +122,7 @@ class Server:
 
     def __init__(self, db_letters, db_offsets, workers=2, batch=True, budget_letters=1_000_000, device=0,
                  index_chunks=None, index_budget=0, merge_ratio=1.0, merge_floor=64_000, tune_cache=None,
-                 overlap_backlog=8):
+                 overlap_backlog=None):
         self.ctxs = [Context(device) for _ in range(workers)]
         # index_budget > 0: each preset's sorted reference seeds stay resident
         self.db = ResidentDb(self.ctxs[0], db_letters, db_offsets, index_budget=index_budget)
@@ -137,10 +139,10 @@ class Server:
         self.tune_cache = tune_cache
         self.tunings: dict = {}
         self.base_tuning = self.ctxs[0].tuning()
-        # with at least this many requests still queued behind a batch, the
-        # batch does not wait for its turn: under a backlog the searches
-        # overlap on the GPU, filling each other's host phases (throughput);
-        # otherwise they take turns (latency)
+        # overlap_backlog = n: with n or more requests still queued behind a
+        # batch, the batch does not wait for its turn, and the searches overlap
+        # on the GPU, filling each other's host phases (more throughput under
+        # a backlog, at the price of the tail: off by default)
         self.overlap_backlog = overlap_backlog
         self.index_chunks = index_chunks
         self.pending: list[Request] = []
@@ -195,7 +197,8 @@ class Server:
                 if not self.pending and self.closed:
                     return
                 reqs = self._take()
-                backlog = self.batch and len(self.pending) >= self.overlap_backlog
+                backlog = (self.batch and self.overlap_backlog is not None
+                           and len(self.pending) >= self.overlap_backlog)
             try:
                 if self.tunings:
                     ctx.set_tuning(**self.tunings.get(reqs[0].preset, self.base_tuning))

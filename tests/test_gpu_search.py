@@ -144,6 +144,36 @@ def test_search_window_clip(ctx, orc):
         assert any(h[1] == 17 for h in exp[0])
 
 
+def wide_key_workload():
+    """1,100 queries against 1,500 subjects plus one of 4.2M aa holding 40 of
+    the queries: the hit key (target | subject | diagonal | position) needs
+    11 + 11 + 23 + 23 = 68 bits, so the search joins in windows of 128
+    targets (7 bits) while every cap and HSP stays that of the whole batch."""
+    r = np.random.Generator(np.random.PCG64(6464))
+    queries = [synth.random_protein(r, int(x)) for x in r.integers(60, 160, 1100)]
+    db = [synth.random_protein(r, int(x)) for x in r.integers(80, 300, 1500)]
+    for j in range(0, 1500, 7):
+        db[j] = synth.planted_homolog(r, queries[(j * 3) % 1100], 40, 100, 0.5, 0.7, 300)
+    big = synth.random_protein(r, 4_200_000)
+    for k in range(40):
+        q = queries[k * 25]
+        p = 50_000 + 100_000 * k
+        big[p:p + len(q)] = q
+    db.insert(500, big)
+    return queries, db
+
+
+def test_search_wide_hit_key_in_target_windows(ctx, orc):
+    queries, db = wide_key_workload()
+    dl, do = drgpu.concat(db)
+    tl, to = drgpu.concat(queries)
+    got, st = ctx.search(dl, do, tl, to, drgpu.make_config(sensitivity="default"))
+    exp, _ = orc.search(db, queries, sensitivity="default", threads=8)
+    assert st["query_blocks"] >= 9  # 1,100 targets in windows of 128, per index chunk
+    assert as_tuples(got) == exp
+    assert sum(1 for lst in exp for h in lst if h[1] == 500) == 40
+
+
 def cap_workload():
     """60 queries and 80 database sequences that all hold one 24-aa motif, plus
     10 planted homologs.  With one index chunk every motif seed key has 60
