@@ -187,6 +187,15 @@ int drg_ctx_create(int device, drg_ctx** out) {
     delete c;
     return DRG_ERR_CUDA;
   }
+  // the radix sort's error word starts clear: a new allocation may hold a
+  // freed buffer's bytes, which every later check would read as a timeout
+  try {
+    DRG_CUDA(cudaMemsetAsync(c->sort_err.as<uint32_t>(1), 0, sizeof(uint32_t), c->stream));
+    DRG_CUDA(cudaStreamSynchronize(c->stream));
+  } catch (const Error& e) {
+    drg_ctx_destroy(c);
+    return e.code;
+  }
   *out = c;
   return DRG_OK;
 }
