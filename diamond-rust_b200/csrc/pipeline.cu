@@ -1558,35 +1558,45 @@ void Search::finish(drg_result* out) {
     i = j;
   }
   // per target: pairs in subject order, HSPs of a pair by cmp_hsp, pairs by
-  // their best HSP, then --max-target-seqs and --max-hsps (search.rs:256-270)
-  std::vector<std::vector<size_t>> by_target(q->n);
-  for (size_t k = 0; k < kept.size(); ++k) by_target[kept[k].band.target].push_back(k);
-  std::vector<std::vector<size_t>> final_lists(q->n);
-  for (uint64_t t = 0; t < q->n; ++t) {
-    auto& v = by_target[t];
-    std::stable_sort(v.begin(), v.end(), [&](size_t a, size_t b) { return kept[a].band.subject < kept[b].band.subject; });
-    std::vector<std::vector<size_t>> found;
-    for (size_t i = 0; i < v.size();) {
-      size_t j = i;
-      while (j < v.size() && kept[v[j]].band.subject == kept[v[i]].band.subject) ++j;
-      std::vector<size_t> hs(v.begin() + i, v.begin() + j);
-      std::stable_sort(hs.begin(), hs.end(), [&](size_t a, size_t b) { return cmp_cand(kept[a], kept[b]) < 0; });
-      found.push_back(hs);
-      i = j;
+  // their best HSP, then --max-target-seqs and --max-hsps (search.rs:256-270).
+  // One index array, stably ordered by (target, subject); each pair's HSPs
+  // sorted in place by cmp_hsp; each target's pairs then ordered by their
+  // best HSP (stable).  No per-target containers: the culling is linear
+  // after the sorts.
+  std::vector<uint32_t> idx(kept.size());
+  for (size_t k = 0; k < kept.size(); ++k) idx[k] = (uint32_t)k;
+  std::stable_sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) {
+    const Band &x = kept[a].band, &y = kept[b].band;
+    return x.target != y.target ? x.target < y.target : x.subject < y.subject;
+  });
+  std::vector<std::pair<uint32_t, uint32_t>> pairs;  // [begin, end) ranges of idx, one per (target, subject)
+  for (size_t i = 0; i < idx.size();) {
+    size_t j = i;
+    const Band& bi = kept[idx[i]].band;
+    while (j < idx.size() && kept[idx[j]].band.target == bi.target && kept[idx[j]].band.subject == bi.subject) ++j;
+    std::stable_sort(idx.begin() + i, idx.begin() + j,
+                     [&](uint32_t a, uint32_t b) { return cmp_cand(kept[a], kept[b]) < 0; });
+    pairs.push_back({(uint32_t)i, (uint32_t)j});
+    i = j;
+  }
+  std::vector<size_t> order;
+  std::vector<uint64_t> final_off(q->n + 1, 0);
+  for (size_t pp = 0, t = 0; t < q->n; ++t) {
+    size_t p1 = pp;
+    while (p1 < pairs.size() && kept[idx[pairs[p1].first]].band.target == t) ++p1;
+    std::stable_sort(pairs.begin() + pp, pairs.begin() + p1,
+                     [&](const std::pair<uint32_t, uint32_t>& a, const std::pair<uint32_t, uint32_t>& b) {
+                       return cmp_cand(kept[idx[a.first]], kept[idx[b.first]]) < 0;
+                     });
+    const size_t np = std::min<size_t>(p1 - pp, max_targets);
+    for (size_t g = pp; g < pp + np; ++g) {
+      const size_t len = std::min<size_t>(pairs[g].second - pairs[g].first, max_hsps);
+      for (size_t e = 0; e < len; ++e) order.push_back(idx[pairs[g].first + e]);
     }
-    std::stable_sort(found.begin(), found.end(), [&](const std::vector<size_t>& a, const std::vector<size_t>& b) {
-      return cmp_cand(kept[a[0]], kept[b[0]]) < 0;
-    });
-    if (found.size() > max_targets) found.resize(max_targets);
-    for (auto& hs : found) {
-      if (hs.size() > max_hsps) hs.resize(max_hsps);
-      for (size_t k : hs) final_lists[t].push_back(k);
-    }
+    final_off[t + 1] = order.size();
+    pp = p1;
   }
   // traceback for the survivors
-  std::vector<size_t> order;
-  for (uint64_t t = 0; t < q->n; ++t)
-    for (size_t k : final_lists[t]) order.push_back(k);
   const uint64_t nj = order.size();
   std::vector<Band> sb(nj);
   std::vector<uint64_t> ops_off(nj + 1, 0);
@@ -1647,7 +1657,7 @@ void Search::finish(drg_result* out) {
   uint64_t h = 0, ko = 0, k = 0;
   out->target_offsets[0] = 0;
   for (uint64_t t = 0; t < q->n; ++t) {
-    for (size_t kk = 0; kk < final_lists[t].size(); ++kk, ++k) {
+    for (uint64_t kk = final_off[t]; kk < final_off[t + 1]; ++kk, ++k) {
       const Candidate& cd = kept[order[k]];
       const ExactOut& r = eo[k];
       if (r.score != cd.score)
