@@ -41,6 +41,7 @@ struct drg_ctx {
       x_query, x_frame;
   drg::DevBuf pass_counts, sw_counts;             // device-side counts of one pass of the stages after the join
   drg::SortScratch sort_tmp;
+  drg::SortScratch sort_tmp_side;  // a sort on the side stream beside one on the main stream
   drg::DevBuf sort_err;  // radix sort scratch; its wait-timeout word (checked after the work)
   drg_tuning tuning{273, 17, 1, 0};  // tile and routing choices (include/drgpu.h)
   drg::HostBuf h_stage;

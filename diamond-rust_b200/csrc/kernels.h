@@ -34,6 +34,9 @@ void launch_seed_enum(const uint8_t* letters, const uint64_t* offsets, const uin
 // hash(run_keys[u] & key_mask) of 2^log2_bits is set (filter zeroed first).
 void launch_key_filter(const uint64_t* run_keys, uint64_t n, uint64_t key_mask, uint32_t* filter, int log2_bits,
                        cudaStream_t st);
+// The same from the unsorted 32-bit seed keys of a batch without request ids
+// (one bit per valid key; "no seed" keys set none).
+void launch_key_filter_keys32(const uint32_t* keys, uint64_t n, uint32_t* filter, int log2_bits, cudaStream_t st);
 // Reference seeds of letters [letter_lo, letter_hi) whose key's bit is set
 // in the filter, appended in no fixed order: counts[0] += kept, counts[1] +=
 // valid seeds (kept or not).  keys / vals need room for every seed of the

@@ -1004,6 +1004,20 @@ struct Search {
   uint32_t* key_filter = nullptr;
   int key_filter_log2 = 0;
   void build_key_filter(uint64_t n_runs);
+  // The first index chunk's reference side (key bitmap, filtered reference
+  // seeds, their sort) on the side stream while the query seeds sort: no
+  // index cache, no request ids, 32-bit seed keys.  ev_filter: the bitmap is
+  // built (the query sort may then overwrite the unsorted keys it read);
+  // ev_ref: the chunk's sorted reference seeds are ready.
+  bool early_possible() const;
+  void start_early_ref(const uint32_t* q_keys, uint64_t n_q);
+  bool early_ref = false;
+  uint64_t early_c0 = 0, early_c1 = 0;
+  const uint32_t* early_keys32_s = nullptr;
+  const uint32_t* early_vals_s = nullptr;
+  int64_t early_nr = 0;
+  const uint64_t* early_d_nr = nullptr;
+  cudaEvent_t ev_filter = nullptr, ev_ref = nullptr, ev_qkeys = nullptr;
   // X-drop, bands, score pass and gate over the accumulated hits.
   void process_hits(uint64_t pass_id);
   // Hits of the chunks joined since the last process_hits (device, from the
@@ -1012,7 +1026,11 @@ struct Search {
   uint64_t acc_n = 0, acc_cap = 0;
   void acc_reserve(uint64_t n);
   ~Search() {
+    if (early_ref) cudaStreamSynchronize(c->side);  // unconsumed side-stream work (a search that stopped early)
     if (acc) cudaFreeAsync(acc, c->stream);
+    if (ev_filter) cudaEventDestroy(ev_filter);
+    if (ev_ref) cudaEventDestroy(ev_ref);
+    if (ev_qkeys) cudaEventDestroy(ev_qkeys);
   }
   void finish(drg_result* out);
 };
@@ -1034,6 +1052,7 @@ void Search::query_seeds(uint64_t* n_runs_out) {
     uint32_t* keys = c->q_keys.as<uint32_t>(N);
     uint32_t* keys_s = c->q_keys_s.as<uint32_t>(N);
     launch_seed_enum(q->letters, q->offsets, q->owner, 0, q->total, S, keys, vals, c->slot, c->stream);
+    if (early_possible()) start_early_ref(keys, N);
     const SortResult<uint32_t> r = dsort(c, keys, keys_s, vals, vals_s, N, 0, seed_key_bits);
     if (r.vals != vals_s) c->q_vals.swap(c->q_vals_s);
     if (N > 0) {
@@ -1103,6 +1122,65 @@ void Search::acc_reserve(uint64_t n) {
 // At least 32 bits per query run up to 2^29 bits (64 MB): then at most 3.1 %
 // of the keys that no query holds pass, and the bitmap stays resident in L2
 // while the reference seeds probe it.
+bool Search::early_possible() const {
+  const bool cached = db->cache && db->cache->budget() > 0;
+  if (cached || q->request || seed_key_bits > 32 || db->n == 0) return false;
+  const auto ch = split_chunks(db->n, index_chunks);
+  if (ch.empty()) return false;
+  const uint64_t n_pos = (db->h_offsets[ch[0].second] - db->h_offsets[ch[0].first]) * (uint64_t)shapes.size();
+  return n_pos < (1ull << 32);
+}
+
+void Search::start_early_ref(const uint32_t* q_keys, uint64_t n_q) {
+  if (!ev_filter) {
+    DRG_CUDA(cudaEventCreateWithFlags(&ev_qkeys, cudaEventDisableTiming));
+    DRG_CUDA(cudaEventCreateWithFlags(&ev_filter, cudaEventDisableTiming));
+    DRG_CUDA(cudaEventCreateWithFlags(&ev_ref, cudaEventDisableTiming));
+  }
+  const auto ch = split_chunks(db->n, index_chunks);
+  early_c0 = ch[0].first;
+  early_c1 = ch[0].second;
+  const int S = (int)shapes.size();
+  const uint64_t lo = db->h_offsets[early_c0], hi = db->h_offsets[early_c1];
+  const uint64_t N = (hi - lo) * (uint64_t)S;
+  // every buffer first, on the host (a reallocation would wait for the device)
+  int lg = 20;
+  while (lg < 29 && (1ull << lg) < 24 * n_q) ++lg;
+  const uint64_t words = (1ull << lg) / 32;
+  key_filter = c->seed_filter.as<uint32_t>(words);
+  key_filter_log2 = lg;
+  unsigned long long* cnt = c->seed_counts.as<unsigned long long>(2);
+  uint32_t* vals = c->r_vals.as<uint32_t>(N);
+  uint32_t* vs = c->r_vals_s.as<uint32_t>(N);
+  uint32_t* k32 = c->r_keys.as<uint32_t>(N);
+  uint32_t* ks32 = c->r_keys_s.as<uint32_t>(N);
+  uint32_t* err = c->sort_err.as<uint32_t>(1);
+  // the query keys are enumerated: the side stream builds the bitmap from
+  // them, and the query sort waits for that before its passes rewrite them
+  DRG_CUDA(cudaEventRecord(ev_qkeys, c->stream));
+  DRG_CUDA(cudaStreamWaitEvent(c->side, ev_qkeys, 0));
+  DRG_CUDA(cudaMemsetAsync(key_filter, 0, words * sizeof(uint32_t), c->side));
+  launch_key_filter_keys32(q_keys, n_q, key_filter, lg, c->side);
+  DRG_CUDA(cudaEventRecord(ev_filter, c->side));
+  DRG_CUDA(cudaStreamWaitEvent(c->stream, ev_filter, 0));
+  // the first chunk's reference seeds the queries can join, sorted on their
+  // device-side count with the side stream's sort scratch
+  DRG_CUDA(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned long long), c->side));
+  launch_seed_enum_filtered(db->letters, db->offsets, db->owner + lo, lo, hi, S, key_filter, key_filter_log2, k32, vals,
+                            cnt, c->slot, c->side);
+  count_launch();
+  k_add_u64<<<1, 1, 0, c->side>>>(d_counters + 7, cnt + 1);
+  const uint64_t* d_nr = reinterpret_cast<const uint64_t*>(cnt);
+  const SortResult<uint32_t> r = radix_sort<uint32_t>(k32, ks32, vals, vs, N, d_nr, 0, seed_key_bits, c->sort_tmp_side,
+                                                      err, c->side, c->tuning.sort_small_tiles != 0);
+  DRG_CUDA(cudaEventRecord(ev_ref, c->side));
+  early_keys32_s = r.keys;
+  early_vals_s = r.vals;
+  early_nr = (int64_t)N;  // capacity; the count is d_nr
+  early_d_nr = d_nr;
+  early_ref = true;
+}
+
 void Search::build_key_filter(uint64_t n_runs) {
   int lg = 20;
   while (lg < 29 && (1ull << lg) < 32 * n_runs) ++lg;
@@ -1139,6 +1217,14 @@ void Search::join_chunk(uint64_t c0, uint64_t c1, uint64_t n_runs) {
     nr = (int64_t)held->n;
     n_valid = held->n;
     st.index_hits += 1;
+  } else if (!cache && early_ref && c0 == early_c0 && c1 == early_c1) {
+    // sorted on the side stream while the query seeds sorted
+    DRG_CUDA(cudaStreamWaitEvent(c->stream, ev_ref, 0));
+    early_ref = false;
+    keys32_s = early_keys32_s;
+    vals_s = early_vals_s;
+    nr = early_nr;
+    d_nr = early_d_nr;
   } else if (!cache) {
     // Nothing is kept for later searches, so only the seeds whose key the
     // query holds are sorted: the join pairs equal keys only (seed.rs:110-140),
@@ -1724,6 +1810,10 @@ void Search::run(drg_result* out) {
   if (n_runs > 0) {
     for (auto [c0, c1] : split_chunks(db->n, index_chunks)) join_chunk(c0, c1, n_runs);
     process_hits(pass++);
+  }
+  if (early_ref) {  // no join read it: its buffers must not outlive this search's use of them
+    DRG_CUDA(cudaStreamWaitEvent(c->stream, ev_ref, 0));
+    early_ref = false;
   }
   finish(out);
   total.stop(&st.ms_total);

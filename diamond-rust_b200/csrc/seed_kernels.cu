@@ -255,6 +255,26 @@ __global__ void k_key_filter(const uint64_t* __restrict__ run_keys, uint64_t n, 
   if (!(filter[h >> 5] & bit)) atomicOr(filter + (h >> 5), bit);
 }
 
+// The same bitmap from unsorted 32-bit query seed keys (no request ids):
+// every valid key sets its bit, "no seed" keys none.
+__global__ void k_key_filter_keys32(const uint32_t* __restrict__ keys, uint64_t n, uint32_t* __restrict__ filter,
+                                    int log2_bits) {
+  const uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (u >= n) return;
+  const uint32_t k = keys[u];
+  if (k == 0xFFFFFFFFu) return;
+  const uint32_t h = seed_key_hash(k, log2_bits);
+  const uint32_t bit = 1u << (h & 31);
+  if (!(filter[h >> 5] & bit)) atomicOr(filter + (h >> 5), bit);
+}
+
+void launch_key_filter_keys32(const uint32_t* keys, uint64_t n, uint32_t* filter, int log2_bits, cudaStream_t st) {
+  if (n == 0) return;
+  count_launch();
+  k_key_filter_keys32<<<ceil_div(n, 256), 256, 0, st>>>(keys, n, filter, log2_bits);
+  DRG_CUDA(cudaGetLastError());
+}
+
 void launch_key_filter(const uint64_t* run_keys, uint64_t n, uint64_t key_mask, uint32_t* filter, int log2_bits,
                        cudaStream_t st) {
   if (n == 0) return;
