@@ -27,16 +27,15 @@ void launch_seed_enum(const uint8_t* letters, const uint64_t* offsets, const uin
                       uint64_t letter_hi, int n_shapes, uint64_t* keys, uint32_t* vals, int slot, cudaStream_t st,
                       const uint32_t* request = nullptr);
 // The same with 32-bit keys, for a seed key of at most 32 bits and no
-// request; "no seed" is 0xFFFFFFFF.
+// request; "no seed" is 0xFFFFFFFF.  filter (optional, zeroed by the caller):
+// each valid key's bit of the query-key bitmap (launch_key_filter's) is set.
 void launch_seed_enum(const uint8_t* letters, const uint64_t* offsets, const uint32_t* owner, uint64_t letter_lo,
-                      uint64_t letter_hi, int n_shapes, uint32_t* keys, uint32_t* vals, int slot, cudaStream_t st);
+                      uint64_t letter_hi, int n_shapes, uint32_t* keys, uint32_t* vals, int slot, cudaStream_t st,
+                      uint32_t* filter = nullptr, int filter_log2 = 0);
 // Bitmap of the query's seed keys for the filtered enumeration: bit
 // hash(run_keys[u] & key_mask) of 2^log2_bits is set (filter zeroed first).
 void launch_key_filter(const uint64_t* run_keys, uint64_t n, uint64_t key_mask, uint32_t* filter, int log2_bits,
                        cudaStream_t st);
-// The same from the unsorted 32-bit seed keys of a batch without request ids
-// (one bit per valid key; "no seed" keys set none).
-void launch_key_filter_keys32(const uint32_t* keys, uint64_t n, uint32_t* filter, int log2_bits, cudaStream_t st);
 // Reference seeds of letters [letter_lo, letter_hi) whose key's bit is set
 // in the filter, appended in no fixed order: counts[0] += kept, counts[1] +=
 // valid seeds (kept or not).  keys / vals need room for every seed of the

@@ -1006,18 +1006,18 @@ struct Search {
   void build_key_filter(uint64_t n_runs);
   // The first index chunk's reference side (key bitmap, filtered reference
   // seeds, their sort) on the side stream while the query seeds sort: no
-  // index cache, no request ids, 32-bit seed keys.  ev_filter: the bitmap is
-  // built (the query sort may then overwrite the unsorted keys it read);
-  // ev_ref: the chunk's sorted reference seeds are ready.
+  // index cache, no request ids, 32-bit seed keys.  The query enumeration
+  // sets the bitmap; ev_qkeys: it is done; ev_ref: the chunk's sorted
+  // reference seeds are ready.
   bool early_possible() const;
-  void start_early_ref(const uint32_t* q_keys, uint64_t n_q);
+  void start_early_ref();
   bool early_ref = false;
   uint64_t early_c0 = 0, early_c1 = 0;
   const uint32_t* early_keys32_s = nullptr;
   const uint32_t* early_vals_s = nullptr;
   int64_t early_nr = 0;
   const uint64_t* early_d_nr = nullptr;
-  cudaEvent_t ev_filter = nullptr, ev_ref = nullptr, ev_qkeys = nullptr;
+  cudaEvent_t ev_ref = nullptr, ev_qkeys = nullptr;
   // X-drop, bands, score pass and gate over the accumulated hits.
   void process_hits(uint64_t pass_id);
   // Hits of the chunks joined since the last process_hits (device, from the
@@ -1028,7 +1028,6 @@ struct Search {
   ~Search() {
     if (early_ref) cudaStreamSynchronize(c->side);  // unconsumed side-stream work (a search that stopped early)
     if (acc) cudaFreeAsync(acc, c->stream);
-    if (ev_filter) cudaEventDestroy(ev_filter);
     if (ev_ref) cudaEventDestroy(ev_ref);
     if (ev_qkeys) cudaEventDestroy(ev_qkeys);
   }
@@ -1051,8 +1050,20 @@ void Search::query_seeds(uint64_t* n_runs_out) {
   if (!q->request && seed_key_bits <= 32) {
     uint32_t* keys = c->q_keys.as<uint32_t>(N);
     uint32_t* keys_s = c->q_keys_s.as<uint32_t>(N);
-    launch_seed_enum(q->letters, q->offsets, q->owner, 0, q->total, S, keys, vals, c->slot, c->stream);
-    if (early_possible()) start_early_ref(keys, N);
+    // with the early reference side, the enumeration also sets the query-key
+    // bitmap (the same key set as the sorted runs)
+    const bool early = early_possible();
+    if (early) {
+      int lg = 20;
+      while (lg < 29 && (1ull << lg) < 24 * N) ++lg;
+      const uint64_t words = (1ull << lg) / 32;
+      key_filter = c->seed_filter.as<uint32_t>(words);
+      key_filter_log2 = lg;
+      DRG_CUDA(cudaMemsetAsync(key_filter, 0, words * sizeof(uint32_t), c->stream));
+    }
+    launch_seed_enum(q->letters, q->offsets, q->owner, 0, q->total, S, keys, vals, c->slot, c->stream,
+                     early ? key_filter : nullptr, key_filter_log2);
+    if (early) start_early_ref();
     const SortResult<uint32_t> r = dsort(c, keys, keys_s, vals, vals_s, N, 0, seed_key_bits);
     if (r.vals != vals_s) c->q_vals.swap(c->q_vals_s);
     if (N > 0) {
@@ -1131,10 +1142,9 @@ bool Search::early_possible() const {
   return n_pos < (1ull << 32);
 }
 
-void Search::start_early_ref(const uint32_t* q_keys, uint64_t n_q) {
-  if (!ev_filter) {
+void Search::start_early_ref() {
+  if (!ev_qkeys) {
     DRG_CUDA(cudaEventCreateWithFlags(&ev_qkeys, cudaEventDisableTiming));
-    DRG_CUDA(cudaEventCreateWithFlags(&ev_filter, cudaEventDisableTiming));
     DRG_CUDA(cudaEventCreateWithFlags(&ev_ref, cudaEventDisableTiming));
   }
   const auto ch = split_chunks(db->n, index_chunks);
@@ -1144,25 +1154,15 @@ void Search::start_early_ref(const uint32_t* q_keys, uint64_t n_q) {
   const uint64_t lo = db->h_offsets[early_c0], hi = db->h_offsets[early_c1];
   const uint64_t N = (hi - lo) * (uint64_t)S;
   // every buffer first, on the host (a reallocation would wait for the device)
-  int lg = 20;
-  while (lg < 29 && (1ull << lg) < 24 * n_q) ++lg;
-  const uint64_t words = (1ull << lg) / 32;
-  key_filter = c->seed_filter.as<uint32_t>(words);
-  key_filter_log2 = lg;
   unsigned long long* cnt = c->seed_counts.as<unsigned long long>(2);
   uint32_t* vals = c->r_vals.as<uint32_t>(N);
   uint32_t* vs = c->r_vals_s.as<uint32_t>(N);
   uint32_t* k32 = c->r_keys.as<uint32_t>(N);
   uint32_t* ks32 = c->r_keys_s.as<uint32_t>(N);
   uint32_t* err = c->sort_err.as<uint32_t>(1);
-  // the query keys are enumerated: the side stream builds the bitmap from
-  // them, and the query sort waits for that before its passes rewrite them
+  // the query seeds are enumerated and the bitmap set
   DRG_CUDA(cudaEventRecord(ev_qkeys, c->stream));
   DRG_CUDA(cudaStreamWaitEvent(c->side, ev_qkeys, 0));
-  DRG_CUDA(cudaMemsetAsync(key_filter, 0, words * sizeof(uint32_t), c->side));
-  launch_key_filter_keys32(q_keys, n_q, key_filter, lg, c->side);
-  DRG_CUDA(cudaEventRecord(ev_filter, c->side));
-  DRG_CUDA(cudaStreamWaitEvent(c->stream, ev_filter, 0));
   // the first chunk's reference seeds the queries can join, sorted on their
   // device-side count with the side stream's sort scratch
   DRG_CUDA(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned long long), c->side));

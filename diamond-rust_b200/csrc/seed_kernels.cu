@@ -192,13 +192,21 @@ __device__ __forceinline__ bool seed_at(const uint8_t* rb, int s, int slot, uint
   return seed_at_t<uint64_t, uint64_t>(rb, s, slot, key_out);
 }
 
+// Hash of a seed key (shape | key) into a bitmap of 2^log2_bits bits.
+__device__ __forceinline__ uint32_t seed_key_hash(uint64_t k, int log2_bits) {
+  return (uint32_t)((k * 0x9E3779B97F4A7C15ull) >> (64 - log2_bits));  // Fibonacci hashing
+}
+
 // K = uint32_t: the caller guarantees that the seed key (with the request,
 // if any) fits 32 bits; "no seed" is then 0xFFFFFFFF.
+// filter (optional): the bit of every valid seed's key (without the request)
+// is set in it, the query-key bitmap of the filtered reference enumeration.
 template <typename K>
 __global__ void k_seed_enum(const uint8_t* __restrict__ letters, const uint64_t* __restrict__ offsets,
                             const uint32_t* __restrict__ owner, uint64_t lo, uint64_t hi, int n_shapes,
                             K* __restrict__ keys, uint32_t* __restrict__ vals,
-                            const uint32_t* __restrict__ request, int slot) {
+                            const uint32_t* __restrict__ request, int slot, uint32_t* __restrict__ filter = nullptr,
+                            int filter_log2 = 0) {
   __shared__ EnumTables tab;
   const uint64_t L = hi - lo;
   const uint64_t i = blockIdx.x * (uint64_t)kEnumBlock + threadIdx.x;
@@ -214,6 +222,11 @@ __global__ void k_seed_enum(const uint8_t* __restrict__ letters, const uint64_t*
     const bool ok = g + c_shapes[slot].span[s] <= end && seed_at(tab.rb + threadIdx.x, s, slot, &key);
     keys[s * L + i] = ok ? (K)(req | ((uint64_t)s << sp.shape_shift) | key) : (K)kNoSeed;
     vals[s * L + i] = (uint32_t)g;
+    if (filter && ok) {
+      const uint32_t h = seed_key_hash(((uint64_t)s << sp.shape_shift) | key, filter_log2);
+      const uint32_t bit = 1u << (h & 31);
+      if (!(filter[h >> 5] & bit)) atomicOr(filter + (h >> 5), bit);
+    }
   }
 }
 
@@ -228,11 +241,12 @@ void launch_seed_enum(const uint8_t* letters, const uint64_t* offsets, const uin
 }
 
 void launch_seed_enum(const uint8_t* letters, const uint64_t* offsets, const uint32_t* owner, uint64_t lo,
-                      uint64_t hi, int n_shapes, uint32_t* keys, uint32_t* vals, int slot, cudaStream_t st) {
+                      uint64_t hi, int n_shapes, uint32_t* keys, uint32_t* vals, int slot, cudaStream_t st,
+                      uint32_t* filter, int filter_log2) {
   if (hi <= lo || n_shapes == 0) return;
   count_launch();
-  k_seed_enum<uint32_t><<<ceil_div(hi - lo, kEnumBlock), kEnumBlock, 0, st>>>(letters, offsets, owner, lo, hi,
-                                                                             n_shapes, keys, vals, nullptr, slot);
+  k_seed_enum<uint32_t><<<ceil_div(hi - lo, kEnumBlock), kEnumBlock, 0, st>>>(
+      letters, offsets, owner, lo, hi, n_shapes, keys, vals, nullptr, slot, filter, filter_log2);
   DRG_CUDA(cudaGetLastError());
 }
 
@@ -242,9 +256,6 @@ void launch_seed_enum(const uint8_t* letters, const uint64_t* offsets, const uin
 // of the query keys.  The bitmap is hashed: a false positive only keeps a
 // seed that then matches no query run, and no key of the query is missed.
 
-__device__ __forceinline__ uint32_t seed_key_hash(uint64_t k, int log2_bits) {
-  return (uint32_t)((k * 0x9E3779B97F4A7C15ull) >> (64 - log2_bits));  // Fibonacci hashing
-}
 
 __global__ void k_key_filter(const uint64_t* __restrict__ run_keys, uint64_t n, uint64_t key_mask,
                              uint32_t* __restrict__ filter, int log2_bits) {
@@ -253,26 +264,6 @@ __global__ void k_key_filter(const uint64_t* __restrict__ run_keys, uint64_t n, 
   const uint32_t h = seed_key_hash(run_keys[u] & key_mask, log2_bits);
   const uint32_t bit = 1u << (h & 31);
   if (!(filter[h >> 5] & bit)) atomicOr(filter + (h >> 5), bit);
-}
-
-// The same bitmap from unsorted 32-bit query seed keys (no request ids):
-// every valid key sets its bit, "no seed" keys none.
-__global__ void k_key_filter_keys32(const uint32_t* __restrict__ keys, uint64_t n, uint32_t* __restrict__ filter,
-                                    int log2_bits) {
-  const uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (u >= n) return;
-  const uint32_t k = keys[u];
-  if (k == 0xFFFFFFFFu) return;
-  const uint32_t h = seed_key_hash(k, log2_bits);
-  const uint32_t bit = 1u << (h & 31);
-  if (!(filter[h >> 5] & bit)) atomicOr(filter + (h >> 5), bit);
-}
-
-void launch_key_filter_keys32(const uint32_t* keys, uint64_t n, uint32_t* filter, int log2_bits, cudaStream_t st) {
-  if (n == 0) return;
-  count_launch();
-  k_key_filter_keys32<<<ceil_div(n, 256), 256, 0, st>>>(keys, n, filter, log2_bits);
-  DRG_CUDA(cudaGetLastError());
 }
 
 void launch_key_filter(const uint64_t* run_keys, uint64_t n, uint64_t key_mask, uint32_t* filter, int log2_bits,
